@@ -1,0 +1,260 @@
+/* rawengine_b200 -- C ABI of the B200 tiled-render hot path of RawEngine.
+ *
+ * Plain C: fixed-width integers, pointers and sizes; no C++ or torch types.
+ * Every function returns an re_status; on failure re_last_error() holds a
+ * thread-local message.  Status codes map one-to-one onto the exception types
+ * the reference throws on the same condition (RawEngine.hpp, SpatialOps.hpp,
+ * GeometryOps.hpp, TileScheduler.hpp of tylermcm/librawops):
+ *   RE_INVALID_ARGUMENT <-> std::invalid_argument, RE_OUT_OF_RANGE <-> std::out_of_range,
+ *   RE_DOMAIN_ERROR <-> std::domain_error, RE_LENGTH_ERROR <-> std::length_error,
+ *   RE_OVERFLOW_ERROR <-> std::overflow_error, RE_CANCELLED <-> RenderCancelled.
+ *
+ * Each entry point names the reference interface it replaces.  Images are
+ * device-resident once created; outputs may be host or device memory.
+ * Calls are reentrant: state is per handle, streams are caller-supplied
+ * (cudaStream_t passed as void*, NULL = the legacy default stream).
+ */
+#ifndef RAWENGINE_B200_H
+#define RAWENGINE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RE_API __attribute__((visibility("default")))
+#else
+#define RE_API
+#endif
+
+typedef enum re_status {
+    RE_OK = 0,
+    RE_INVALID_ARGUMENT = 1,
+    RE_OUT_OF_RANGE = 2,
+    RE_DOMAIN_ERROR = 3,
+    RE_LENGTH_ERROR = 4,
+    RE_OVERFLOW_ERROR = 5,
+    RE_CANCELLED = 6,
+    RE_CUDA_ERROR = 7,
+    RE_TIMEOUT = 8,
+} re_status;
+
+/* Rect (RawEngine.hpp:29-31). */
+typedef struct re_rect { uint32_t x, y, width, height; } re_rect;
+
+/* RawMetadata (RawEngine.hpp:57-65).  pattern: 0 RGGB, 1 BGGR, 2 GRBG, 3 GBRG. */
+typedef struct re_raw_metadata {
+    uint32_t width, height, row_stride_samples;
+    uint32_t pattern;
+    uint32_t cfa_phase_x, cfa_phase_y;
+    re_rect active_area;
+    uint16_t black_levels[4];
+    uint16_t white_levels[4];
+} re_raw_metadata;
+
+/* ------------------------------------------------------------------ errors */
+
+/* Thread-local text of the last failure on this thread. */
+RE_API const char* re_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+RE_API int re_version(void);
+/* CUDA device count visible to the library (0 without a GPU; never fails). */
+RE_API int re_device_count(void);
+
+/* ------------------------------------------------------------ RAW sources */
+
+typedef struct re_image re_image;
+
+/* RawImage::RawImage(RawMetadata, std::vector<uint16_t>) (RawEngine.cpp:223-250):
+ * validates and normalizes `meta` in place (stride 0 -> width, empty active area
+ * -> full sensor), then uploads the samples to the current device.  `samples`
+ * is HOST memory of `count` uint16 values (count == stride * height). */
+RE_API re_status re_image_create(re_raw_metadata* meta, const uint16_t* samples, size_t count,
+                                 re_image** out);
+/* Same, but `device_samples` is already device memory; it is NOT copied and must
+ * outlive the handle. */
+RE_API re_status re_image_wrap_device(re_raw_metadata* meta, const uint16_t* device_samples,
+                                      size_t count, re_image** out);
+RE_API re_status re_image_destroy(re_image* image);
+RE_API re_status re_image_metadata(const re_image* image, re_raw_metadata* out);
+
+/* Metadata normalization/validation only (no device work): RawEngine.cpp:223-250. */
+RE_API re_status re_raw_metadata_normalize(re_raw_metadata* meta, size_t count);
+/* RawEngine.cpp:74-87: photosite index and CFA colour (R=0, G=1, B=2). */
+RE_API int re_site_index(const re_raw_metadata* meta, uint32_t x, uint32_t y);
+RE_API int re_cfa_color(const re_raw_metadata* meta, uint32_t x, uint32_t y);
+
+/* ------------------------------------------------------ host-side planning */
+
+/* RawEngine.cpp:31-43 request_bounds: extent of a render level. */
+RE_API re_status re_request_bounds(re_rect source_bounds, uint32_t mip, uint32_t quality,
+                                   re_rect* out);
+/* RawEngine.cpp:290-297 RawUnpackNode::input_region: the clipped demosaic halo
+ * (1 for bilinear, 6 for Menon unless an active-area axis is a singleton). */
+RE_API re_status re_raw_input_region(const re_raw_metadata* meta, uint32_t demosaic,
+                                     re_rect output, re_rect* region);
+/* RawEngine.cpp:563-578 CameraToWorkingNode::input_region_level: native
+ * footprint of a reduced (mip 1/2) request. */
+RE_API re_status re_mip_native_region(re_rect native_bounds, uint32_t mip, re_rect output,
+                                      re_rect* native);
+/* RawEngine.cpp:1399-1411 render_tiles tile order: writes up to `capacity`
+ * tiles and returns the total count in *count. */
+RE_API re_status re_plan_tiles(re_rect viewport, uint32_t tile_size, re_rect* tiles,
+                               size_t capacity, size_t* count);
+
+/* RawEngine.cpp:116-219, 502-530: camera->XYZ(D50) composed with XYZ->working
+ * space in double, cast to float32.  target: 0 LinearProPhotoD50, 1 LinearRec2020D65. */
+RE_API re_status re_camera_to_working_matrix(const double camera_to_xyz_d50[9], uint32_t target,
+                                             float out[9]);
+/* RawEngine.cpp:198-214, 658-672 WorkingToSrgbNode matrix. */
+RE_API re_status re_working_to_srgb_matrix(uint32_t source, float out[9]);
+/* RawEngine.cpp:216-219, 603-623 WorkingSpaceConvertNode matrix. */
+RE_API re_status re_working_to_working_matrix(uint32_t source, uint32_t target, float out[9]);
+/* RawEngine.cpp:465-468 ExposureNode multiplier (exp2 of stops, stops in [-32,32]). */
+RE_API re_status re_exposure_multiplier(float stops, float* out);
+
+/* ------------------------------------------------------- point programs */
+
+/* The per-pixel stages of a render chain, fused into the demosaic kernel.
+ * Each kind restates one reference node's pixel arithmetic:
+ *   RE_STAGE_GAIN3   WhiteBalanceNode::render        RawEngine.cpp:417-431  f[0..2] gains
+ *   RE_STAGE_SCALE   ExposureNode::render_level      RawEngine.cpp:488-500  f[0] multiplier
+ *   RE_STAGE_MATRIX  CameraToWorking / WorkingToSrgb / WorkingSpaceConvert
+ *                    RawEngine.cpp:539-545, 646-652, 694-700             f[0..8] row-major
+ *   RE_STAGE_TONE    ToneCurveNode::render_level     RawEngine.cpp:738-758  f[0] shoulder, f[1] 1/gamma
+ *   RE_STAGE_CLIP    OutputClipNode::render          RawEngine.cpp:1223-1233
+ *   RE_STAGE_SRGB    SrgbEncodeNode::render_level    RawEngine.cpp:1254-1277
+ *   RE_STAGE_CURVES  ExtendedCurvesNode::render_level ToneOps.cpp:833-844   arg = curve set
+ */
+typedef enum re_stage_kind {
+    RE_STAGE_GAIN3 = 1,
+    RE_STAGE_SCALE = 2,
+    RE_STAGE_MATRIX = 3,
+    RE_STAGE_TONE = 4,
+    RE_STAGE_CLIP = 5,
+    RE_STAGE_SRGB = 6,
+    RE_STAGE_CURVES = 7,
+} re_stage_kind;
+
+#define RE_MAX_STAGES 16
+
+typedef struct re_stage {
+    uint32_t kind;
+    uint32_t arg;
+    float f[12];
+} re_stage;
+
+typedef struct re_curve_set re_curve_set;
+
+/* ExtendedCurvesSettings (ToneOps.hpp:19-25) -> a device curve set.
+ * knots: x0,y0,x1,y1,... for the master, R, G, B curves concatenated;
+ * counts[4] knot counts (2..256 each); interpolation 0 Linear, 1
+ * ShapePreservingCubic.  Validation follows ToneOps.cpp:17-31, 117-122. */
+RE_API re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4],
+                                     const double* knots, re_curve_set** out);
+RE_API re_status re_curve_set_destroy(re_curve_set* curves);
+
+/* A render description: demosaic policy (0 rawengine.bilinear v1, 1
+ * rawengine.menon_base v1; RawEngine.cpp:276-280), then `count` stages.  Stages
+ * [0, anchor] run at native resolution; when a reduced level is requested the
+ * result is averaged over each output pixel's native footprint after stage
+ * `anchor` (the CameraToWorking mip anchor, RawEngine.cpp:580-601), and stages
+ * after the anchor run on the reduced pixels.  anchor = -1: no reduced levels. */
+typedef struct re_render_desc {
+    uint32_t demosaic;
+    int32_t anchor;
+    uint32_t count;
+    re_stage stages[RE_MAX_STAGES];
+    const re_curve_set* curves[4];
+} re_render_desc;
+
+/* Statistics of one render (Menon near-tie and guard counters). */
+typedef struct re_render_stats {
+    uint64_t pixels;             /* output pixels written */
+    uint64_t native_pixels;      /* demosaiced native pixels */
+    uint64_t menon_decisions;    /* directional decisions evaluated */
+    uint64_t menon_near_ties;    /* decisions within the exact-recheck band */
+    uint32_t launches;           /* kernels launched */
+    float device_ms;             /* device time of the render (CUDA events) */
+} re_render_stats;
+
+/* Renderer::render_image(node, source_bounds, RenderRequest) for a RAW chain
+ * (RawEngine.cpp:1426-1447) fused into one pass per render: demosaic + stages
+ * (+ mip reduction).  `viewport` is in level coordinates (the active-area
+ * origin at mip 0, zero-based at mip 1/2; RawEngine.hpp:35-40).  quality: 0
+ * Preview, 1 Final.  `out` receives viewport.height rows of
+ * `out_row_stride` floats (>= 3*viewport.width); out_on_device selects device
+ * vs host memory (host output is copied back inside this call).  stats may be
+ * NULL.  The call returns after the render completed on `stream`. */
+RE_API re_status re_render_raw(const re_image* image, const re_render_desc* desc,
+                               re_rect viewport, uint32_t mip, uint32_t quality, float* out,
+                               size_t out_row_stride, int out_on_device, void* stream,
+                               re_render_stats* stats);
+
+/* Asynchronous device-only form: enqueues the render on `stream` and returns.
+ * Non-finite/overflow guards are OR-ed into *device_status (a device word the
+ * caller zeroes and later reads; re_status_from_device maps it).  No host sync.
+ * `scratch` must be device memory of at least re_render_scratch_bytes() bytes
+ * when mip > 0 (NULL otherwise). */
+RE_API re_status re_render_raw_async(const re_image* image, const re_render_desc* desc,
+                                     re_rect viewport, uint32_t mip, uint32_t quality, float* out,
+                                     size_t out_row_stride, uint32_t* device_status,
+                                     void* scratch, void* stream);
+RE_API size_t re_render_scratch_bytes(const re_image* image, const re_render_desc* desc,
+                                      re_rect viewport, uint32_t mip);
+RE_API re_status re_status_from_device(uint32_t device_status_word);
+
+/* Renderer::render_tiles (RawEngine.cpp:1390-1412): the reference's per-tile
+ * loop, one fused launch per tile, each tile copied to the host callback in
+ * tile order.  The callback may return nonzero to cancel (RE_CANCELLED). */
+typedef int (*re_tile_callback)(const re_rect* bounds, const float* rgb, void* user);
+RE_API re_status re_render_tiles(const re_image* image, const re_render_desc* desc,
+                                 re_rect viewport, uint32_t tile_size, uint32_t mip,
+                                 uint32_t quality, re_tile_callback callback, void* user,
+                                 void* stream);
+
+/* ------------------------------------------------------------- raster I/O */
+
+/* float32 interleaved RGB device buffers for spatial/geometry stages. */
+
+/* working_y_guided_filter_rgb (SpatialOps.cpp:168-287) over a whole image:
+ * `in` is a device image of width*height RGB pixels (row stride in floats),
+ * `out` a device buffer of the same shape.  working_space selects the Y weights
+ * (0 ProPhoto, 1 Rec2020, SpatialOps.cpp:191-192).  Radius 0..64, epsilon in
+ * [2^-24, 65536].  Windows clip at the image edge with actual counts. */
+RE_API re_status re_guided_filter(const float* in, size_t in_row_stride, float* out,
+                                  size_t out_row_stride, uint32_t width, uint32_t height,
+                                  uint32_t radius, double epsilon, uint32_t working_space,
+                                  void* stream);
+/* local_statistics_rgb (SpatialOps.cpp:79-121) over a whole image: per channel
+ * box mean and population variance over the clipped (2r+1)^2 window, excluding
+ * non-finite samples (count_out gets the finite count; mean/variance NaN when
+ * it is 0).  Outputs are float32 interleaved RGB; count_out may be NULL. */
+RE_API re_status re_local_statistics(const float* in, size_t in_row_stride, uint32_t width,
+                                     uint32_t height, uint32_t radius, float* mean_out,
+                                     float* variance_out, uint32_t* count_out, void* stream);
+
+/* CubicResizeNode (GeometryOps.cpp:346-513): scale-aware Catmull-Rom from an
+ * in_w x in_h device image to the `output` rect of an out_w x out_h canvas at
+ * `mip` (0..2, footprint-averaged like the reference). */
+RE_API re_status re_cubic_resize(const float* in, size_t in_row_stride, uint32_t in_w,
+                                 uint32_t in_h, uint32_t out_w, uint32_t out_h, re_rect output,
+                                 uint32_t mip, float* out, size_t out_row_stride, void* stream);
+/* RotateNode (GeometryOps.cpp:42-174): fixed-canvas clockwise rotation about
+ * the pixel-centre pivot, clamped bilinear taps, mip 0..2 footprint average. */
+RE_API re_status re_rotate(const float* in, size_t in_row_stride, uint32_t width, uint32_t height,
+                           double angle_degrees, re_rect output, uint32_t mip, float* out,
+                           size_t out_row_stride, void* stream);
+/* GeometryOps.cpp:362-389 one Catmull-Rom axis (host): returns taps in *count. */
+RE_API re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, uint32_t* center,
+                               uint32_t tap_index[18], double tap_weight[18], uint32_t* count);
+/* GeometryOps.cpp:46-67 rotation constants (host). */
+RE_API re_status re_rotation_coefficients(double angle_degrees, double* cosine, double* sine);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,129 @@
+"""ctypes binding of the C ABI declared in include/rawengine_b200.h.
+
+The shared library is built in tree (librawops_b200/_lib/librawengine_b200.so,
+see build.py).  There is no fallback: if the library is missing, importing the
+render API raises, and on a machine without a GPU every device entry point
+reports RE_CUDA_ERROR.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "librawengine_b200.so")
+
+RE_OK, RE_INVALID_ARGUMENT, RE_OUT_OF_RANGE, RE_DOMAIN_ERROR = 0, 1, 2, 3
+RE_LENGTH_ERROR, RE_OVERFLOW_ERROR, RE_CANCELLED, RE_CUDA_ERROR, RE_TIMEOUT = 4, 5, 6, 7, 8
+
+STAGE_GAIN3, STAGE_SCALE, STAGE_MATRIX, STAGE_TONE, STAGE_CLIP, STAGE_SRGB, STAGE_CURVES = range(1, 8)
+MAX_STAGES = 16
+
+# Every exported symbol of include/rawengine_b200.h (checked by the CPU tests).
+EXPORTS = [
+    "re_last_error", "re_version", "re_device_count",
+    "re_image_create", "re_image_wrap_device", "re_image_destroy", "re_image_metadata",
+    "re_raw_metadata_normalize", "re_site_index", "re_cfa_color",
+    "re_request_bounds", "re_raw_input_region", "re_mip_native_region", "re_plan_tiles",
+    "re_camera_to_working_matrix", "re_working_to_srgb_matrix", "re_working_to_working_matrix",
+    "re_exposure_multiplier", "re_curve_set_create", "re_curve_set_destroy",
+    "re_render_raw", "re_render_raw_async", "re_render_scratch_bytes", "re_status_from_device",
+    "re_render_tiles", "re_guided_filter", "re_local_statistics", "re_cubic_resize", "re_rotate",
+    "re_cubic_axis", "re_rotation_coefficients",
+]
+
+
+class ReError(RuntimeError):
+    """Raised for a non-zero re_status; `kind` names the reference exception."""
+    KINDS = {1: "invalid_argument", 2: "out_of_range", 3: "domain_error", 4: "length_error",
+             5: "overflow_error", 6: "cancelled", 7: "cuda_error", 8: "timeout"}
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{self.KINDS.get(code, code)}: {message}")
+        self.code = code
+        self.kind = self.KINDS.get(code, str(code))
+
+
+class Rect(C.Structure):
+    _fields_ = [("x", C.c_uint32), ("y", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+    def tuple(self):
+        return (self.x, self.y, self.width, self.height)
+
+
+class RawMetadata(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("row_stride_samples", C.c_uint32),
+                ("pattern", C.c_uint32), ("cfa_phase_x", C.c_uint32), ("cfa_phase_y", C.c_uint32),
+                ("active_area", Rect), ("black_levels", C.c_uint16 * 4),
+                ("white_levels", C.c_uint16 * 4)]
+
+
+class Stage(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("arg", C.c_uint32), ("f", C.c_float * 12)]
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [("demosaic", C.c_uint32), ("anchor", C.c_int32), ("count", C.c_uint32),
+                ("stages", Stage * MAX_STAGES), ("curves", C.c_void_p * 4)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("pixels", C.c_uint64), ("native_pixels", C.c_uint64), ("menon_decisions", C.c_uint64),
+                ("menon_near_ties", C.c_uint64), ("launches", C.c_uint32), ("device_ms", C.c_float)]
+
+
+TILE_CALLBACK = C.CFUNCTYPE(C.c_int, C.POINTER(Rect), C.POINTER(C.c_float), C.c_void_p)
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError(f"{_LIB_PATH} is missing: run `python -m librawops_b200.build`")
+        L = C.CDLL(_LIB_PATH)
+        vp, u32, f32p, f64p = C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_double)
+        sz = C.c_size_t
+        L.re_last_error.restype = C.c_char_p
+        L.re_image_create.argtypes = [C.POINTER(RawMetadata), C.POINTER(C.c_uint16), sz, C.POINTER(vp)]
+        L.re_image_wrap_device.argtypes = [C.POINTER(RawMetadata), vp, sz, C.POINTER(vp)]
+        L.re_image_destroy.argtypes = [vp]
+        L.re_image_metadata.argtypes = [vp, C.POINTER(RawMetadata)]
+        L.re_raw_metadata_normalize.argtypes = [C.POINTER(RawMetadata), sz]
+        L.re_site_index.argtypes = [C.POINTER(RawMetadata), u32, u32]
+        L.re_cfa_color.argtypes = [C.POINTER(RawMetadata), u32, u32]
+        L.re_request_bounds.argtypes = [Rect, u32, u32, C.POINTER(Rect)]
+        L.re_raw_input_region.argtypes = [C.POINTER(RawMetadata), u32, Rect, C.POINTER(Rect)]
+        L.re_mip_native_region.argtypes = [Rect, u32, Rect, C.POINTER(Rect)]
+        L.re_plan_tiles.argtypes = [Rect, u32, C.POINTER(Rect), sz, C.POINTER(sz)]
+        L.re_camera_to_working_matrix.argtypes = [f64p, u32, f32p]
+        L.re_working_to_srgb_matrix.argtypes = [u32, f32p]
+        L.re_working_to_working_matrix.argtypes = [u32, u32, f32p]
+        L.re_exposure_multiplier.argtypes = [C.c_float, f32p]
+        L.re_curve_set_create.argtypes = [u32, C.POINTER(C.c_uint32), f64p, C.POINTER(vp)]
+        L.re_curve_set_destroy.argtypes = [vp]
+        L.re_render_raw.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, C.c_int, vp,
+                                    C.POINTER(RenderStats)]
+        L.re_render_raw_async.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, vp, vp, vp]
+        L.re_render_scratch_bytes.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32]
+        L.re_render_scratch_bytes.restype = sz
+        L.re_status_from_device.argtypes = [u32]
+        L.re_render_tiles.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, u32, TILE_CALLBACK, vp, vp]
+        L.re_guided_filter.argtypes = [vp, sz, vp, sz, u32, u32, u32, C.c_double, u32, vp]
+        L.re_local_statistics.argtypes = [vp, sz, u32, u32, u32, vp, vp, vp, vp]
+        L.re_cubic_resize.argtypes = [vp, sz, u32, u32, u32, u32, Rect, u32, vp, sz, vp]
+        L.re_rotate.argtypes = [vp, sz, u32, u32, C.c_double, Rect, u32, vp, sz, vp]
+        L.re_cubic_axis.argtypes = [u32, u32, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), f64p,
+                                    C.POINTER(C.c_uint32)]
+        L.re_rotation_coefficients.argtypes = [C.c_double, f64p, f64p]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status:
+        raise ReError(status, lib().re_last_error().decode(errors="replace"))
+
+
+def library_path() -> str:
+    return _LIB_PATH

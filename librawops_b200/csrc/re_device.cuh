@@ -1,0 +1,102 @@
+// Device-side data layout shared by the render kernels.
+//
+// HBM layout: a RAW image is its uint16 sensor plane exactly as the caller
+// supplied it (row stride in samples, active area inside it); renders write
+// interleaved float32 RGB rows (3 floats per pixel, caller row stride).  All
+// per-image constants the kernels need travel by value in DevRaw; the per-pixel
+// stage program travels by value in DevProgram (kernel parameter space), so a
+// launch reads nothing but the sensor samples and writes nothing but pixels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rawengine_b200.h"
+
+namespace re {
+
+// Device status word: zero = ok.  A failure stores key = (priority << 8) | kind
+// with atomicMax, so the highest-priority failure survives: internal guards
+// and timeouts (priority 511) first, then the earliest failing chain stage
+// (priority 255 - stage index).  The low byte is the failure kind.
+enum : uint32_t {
+    ST_DOMAIN = 1u << 0,     // non-finite at an output boundary (domain_error)
+    ST_INVALID = 1u << 1,    // non-finite curve input / float32 overflow (invalid_argument)
+    ST_OVERFLOW = 1u << 2,   // guided filter intermediate overflow (overflow_error)
+    ST_GUARD = 1u << 3,      // internal bounds guard tripped (logic error)
+    ST_TIMEOUT = 1u << 4,    // bounded wait expired
+};
+
+struct DevRaw {
+    const uint16_t* samples;
+    uint32_t stride;          // samples per row
+    int32_t ax, ay, aw, ah;   // active area (sensor coordinates)
+    uint32_t phase_x, phase_y;
+    int32_t site_color[4];    // colour of each photosite index (pattern applied)
+    float black[4];           // per-site black level as float
+    float span[4];            // per-site (white - black) as float
+};
+
+// Photosite index of RawEngine.cpp:74-77 for any integer position.
+__host__ __device__ __forceinline__ int site_of(const DevRaw& r, int x, int y) {
+    return (int)((((unsigned)(y & 1) + r.phase_y) & 1u) * 2u + (((unsigned)(x & 1) + r.phase_x) & 1u));
+}
+
+__host__ __device__ __forceinline__ int color_of(const DevRaw& r, int x, int y) {
+    return r.site_color[site_of(r, x, y)];
+}
+
+// RawEngine.cpp:89-97: (float(raw) - black) / (white - black), IEEE division.
+__device__ __forceinline__ float normalize_sample(const DevRaw& r, int x, int y) {
+    const int s = site_of(r, x, y);
+    const float code = (float)__ldg(r.samples + (size_t)y * r.stride + x);
+    return __fdiv_rn(__fsub_rn(code, r.black[s]), r.span[s]);
+}
+
+// MenonDemosaic.cpp:60-66 whole-sample mirror about [origin, origin+size).
+__host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size) {
+    if (v >= origin && v < origin + size) return v;
+    if (size == 1) return origin;
+    const int period = 2 * (size - 1);
+    int folded = (v - origin) % period;
+    if (folded < 0) folded += period;
+    return origin + (folded < size ? folded : period - folded);
+}
+
+// ---------------------------------------------------------------- curves
+
+// One ExtendedCurves curve prepared for float32 evaluation (ToneOps.cpp:795-832).
+// Knot x are rounded UP to float so that `v < xf` equals the reference's
+// double comparison `v < x` for every float v; xeq holds x only when x is a
+// float (else NaN) so that `v == xeq` equals the double equality test.
+struct DevCurve {
+    uint32_t n;               // knots
+    uint32_t identity;        // every knot has x == y
+    uint32_t cubic;           // ShapePreservingCubic
+    uint32_t pad;
+    float xf[256];
+    float xeq[256];
+    float xn[256];            // x rounded to nearest (arithmetic anchor)
+    float y[256];
+    float slope[256];         // segment slopes (linear segments and extrapolation)
+    float4 coef[256];         // power-basis cubic per segment: c0 + t(c1 + t(c2 + t c3))
+    float inv_h[256];         // 1 / (x[i+1] - x[i])
+};
+
+struct DevCurveSet {
+    DevCurve c[4];            // master, R, G, B
+};
+
+// --------------------------------------------------------------- program
+
+struct DevProgram {
+    uint32_t count;
+    int32_t anchor;
+    re_stage st[RE_MAX_STAGES];
+    const DevCurveSet* curves[4];
+};
+
+constexpr uint32_t KEY_GUARD = (511u << 8) | ST_GUARD;
+constexpr uint32_t KEY_TIMEOUT = (511u << 8) | ST_TIMEOUT;
+
+}  // namespace re

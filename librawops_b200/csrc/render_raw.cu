@@ -1,0 +1,380 @@
+// Fused RAW render kernels: demosaic (bilinear v1 or menon_base v1) + the
+// per-pixel stage program, one CTA per output tile, whole viewport per launch.
+//
+// Reference path replaced: Renderer::render_tiles -> Node::render_level chain
+// -> RawUnpackNode::render (RawEngine.cpp:299-344) / detail::render_menon_base
+// (MenonDemosaic.cpp:89-218), then one full-tile pass per point node.  Here the
+// sensor tile plus its halo is staged once in shared memory, every stage runs
+// on chip, and only the final float32 RGB leaves the SM.
+//
+// Both demosaics are pure functions of the pixel position (the reference's
+// tiling/blocking never changes a value), so one launch over the viewport with
+// the CTA grid as the tile grid gives the reference's result for any tile size.
+#include "re_program.cuh"
+
+namespace re {
+
+// ------------------------------------------------------------- bilinear v1
+
+constexpr int BL_TW = 64, BL_TH = 16, BL_THREADS = 256;
+constexpr int BL_SW = BL_TW + 2, BL_SH = BL_TH + 2;
+
+// RawEngine.cpp:299-344.  The normalized samples of the tile and its one-pixel
+// halo are computed once into shared memory (positions outside the active area
+// are never read: the reference skips them and counts only present neighbours).
+__global__ void __launch_bounds__(BL_THREADS)
+bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int stage_end,
+                const __grid_constant__ DevProgram P, float* __restrict__ out,
+                size_t out_stride, uint32_t* status) {
+    __shared__ float tile[BL_SH][BL_SW];
+    const int x0 = ox + blockIdx.x * BL_TW, y0 = oy + blockIdx.y * BL_TH;
+    for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
+        const int sx = i % BL_SW, sy = i / BL_SW;
+        const int x = x0 - 1 + sx, y = y0 - 1 + sy;
+        float v = 0.0f;
+        if (x >= raw.ax && x < raw.ax + raw.aw && y >= raw.ay && y < raw.ay + raw.ah)
+            v = normalize_sample(raw, x, y);
+        tile[sy][sx] = v;
+    }
+    __syncthreads();
+    uint32_t err = 0;
+    for (int i = threadIdx.x; i < BL_TW * BL_TH; i += BL_THREADS) {
+        const int tx = i % BL_TW, ty = i / BL_TW;
+        const int x = x0 + tx, y = y0 + ty;
+        if (x >= ox + ow || y >= oy + oh) continue;
+        const int own = color_of(raw, x, y);
+        float rgb[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            if (own == ch) {
+                rgb[ch] = tile[ty + 1][tx + 1];
+                continue;
+            }
+            float sum = 0.0f;
+            int count = 0;
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int yy = y + dy;
+                if (yy < raw.ay || yy >= raw.ay + raw.ah) continue;
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int xx = x + dx;
+                    if (xx < raw.ax || xx >= raw.ax + raw.aw) continue;
+                    if (color_of(raw, xx, yy) != ch) continue;
+                    sum = __fadd_rn(sum, tile[ty + 1 + dy][tx + 1 + dx]);
+                    ++count;
+                }
+            }
+            rgb[ch] = count ? __fdiv_rn(sum, (float)count) : 0.0f;
+        }
+        apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err);
+        float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+        o[0] = rgb[0];
+        o[1] = rgb[1];
+        o[2] = rgb[2];
+    }
+    report(status, err);
+}
+
+// ------------------------------------------------------------- menon_base v1
+
+// Output tile and the virtual extents of each on-chip plane (MenonDemosaic.cpp:96-105):
+// raw r=6, directional chroma r=4, forward gradients [-4,+2]x[-4,+4] (and its
+// transpose), green/direction r=2, red/blue r=1.  A plane entry at a virtual
+// position outside the active area holds the plane's value at the mirrored
+// position (MenonDemosaic.cpp:67-72), so every mirrored read is a plain
+// shared-memory read; gradients are zero outside (MenonDemosaic.cpp:126-129).
+constexpr int MN_TW = 32, MN_TH = 16, MN_THREADS = 256;
+constexpr int RAW_W = MN_TW + 12, RAW_H = MN_TH + 12;   // origin (-6,-6)
+constexpr int CH_W = MN_TW + 8, CH_H = MN_TH + 8;       // origin (-4,-4)
+constexpr int DH_W = MN_TW + 6, DH_H = MN_TH + 8;       // origin (-4,-4), x to +2
+constexpr int DV_W = MN_TW + 8, DV_H = MN_TH + 6;       // origin (-4,-4), y to +2
+constexpr int GR_W = MN_TW + 4, GR_H = MN_TH + 4;       // origin (-2,-2)
+constexpr int CO_W = MN_TW + 2, CO_H = MN_TH + 2;       // origin (-1,-1)
+
+struct MenonSmem {
+    double ch[CH_H][CH_W];
+    double cv[CH_H][CH_W];
+    double dh[DH_H][DH_W];
+    double dv[DV_H][DV_W];
+    double green[GR_H][GR_W];
+    double red[CO_H][CO_W];
+    double blue[CO_H][CO_W];
+    float raw[RAW_H][RAW_W];
+    uint8_t horiz[GR_H][GR_W];
+};
+
+struct MenonCtx {
+    int x0, y0;                  // tile origin (sensor coordinates)
+    int xe, ye;                  // end of this tile's output pixels (exclusive)
+    int ax, ay, aw, ah;
+    // A plane of radius r is needed only at virtual positions within r of the
+    // tile's output pixels; positions of a partial tile further out are skipped,
+    // which keeps every mirrored read inside its shared-memory plane.
+    __device__ __forceinline__ bool needed(int x, int y, int rx, int ry) const {
+        return x < xe + rx && y < ye + ry;
+    }
+    __device__ __forceinline__ int mx(int x) const { return mirror_coord(x, ax, aw); }
+    __device__ __forceinline__ int my(int y) const { return mirror_coord(y, ay, ah); }
+    __device__ __forceinline__ bool inside(int x, int y) const {
+        return x >= ax && x < ax + aw && y >= ay && y < ay + ah;
+    }
+};
+
+// MenonDemosaic.cpp:112-115 directional five-tap green estimate along one axis.
+__device__ __forceinline__ double five_tap(double m2, double m1, double own, double p1, double p2) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(0.5, __dadd_rn(m1, p1)), __dmul_rn(0.5, own)),
+                     -__dmul_rn(0.25, __dadd_rn(m2, p2)));
+}
+
+__device__ __forceinline__ double raw_at(const MenonSmem& S, const MenonCtx& c, int x, int y) {
+    return (double)S.raw[y - (c.y0 - 6)][x - (c.x0 - 6)];
+}
+
+__device__ __forceinline__ double green_h(const MenonSmem& S, const MenonCtx& c, int x, int y) {
+    return five_tap(raw_at(S, c, x - 2, y), raw_at(S, c, x - 1, y), raw_at(S, c, x, y),
+                    raw_at(S, c, x + 1, y), raw_at(S, c, x + 2, y));
+}
+__device__ __forceinline__ double green_v(const MenonSmem& S, const MenonCtx& c, int x, int y) {
+    return five_tap(raw_at(S, c, x, y - 2), raw_at(S, c, x, y - 1), raw_at(S, c, x, y),
+                    raw_at(S, c, x, y + 1), raw_at(S, c, x, y + 2));
+}
+
+// MenonDemosaic.cpp:148-150 pair mean of a mirrored plane.
+template <int W, int OX, int OY>
+__device__ __forceinline__ double pair_mean(const double (*p)[W], const MenonCtx& c, int x, int y,
+                                            int dx, int dy) {
+    return __dmul_rn(0.5, __dadd_rn(p[y - dy - (c.y0 + OY)][x - dx - (c.x0 + OX)],
+                                    p[y + dy - (c.y0 + OY)][x + dx - (c.x0 + OX)]));
+}
+
+__device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, const MenonCtx& c,
+                                           unsigned long long* ties) {
+    const int t = threadIdx.x;
+    // 1. normalized raw over r=6 at mirrored positions (MenonDemosaic.cpp:106).
+    for (int i = t; i < RAW_W * RAW_H; i += MN_THREADS) {
+        const int sx = i % RAW_W, sy = i / RAW_W;
+        if (!c.needed(c.x0 - 6 + sx, c.y0 - 6 + sy, 6, 6)) continue;
+        S.raw[sy][sx] = normalize_sample(raw, c.mx(c.x0 - 6 + sx), c.my(c.y0 - 6 + sy));
+    }
+    __syncthreads();
+    // 2. directional chroma (MenonDemosaic.cpp:107-119), evaluated at the
+    //    mirrored position; green sites keep zero chroma.
+    for (int i = t; i < CH_W * CH_H; i += MN_THREADS) {
+        const int sx = i % CH_W, sy = i / CH_W;
+        if (!c.needed(c.x0 - 4 + sx, c.y0 - 4 + sy, 4, 4)) continue;
+        const int x = c.mx(c.x0 - 4 + sx), y = c.my(c.y0 - 4 + sy);
+        double h = 0.0, v = 0.0;
+        if (color_of(raw, x, y) != 1) {
+            const double own = raw_at(S, c, x, y);
+            h = __dadd_rn(own, -green_h(S, c, x, y));
+            v = __dadd_rn(own, -green_v(S, c, x, y));
+        }
+        S.ch[sy][sx] = h;
+        S.cv[sy][sx] = v;
+    }
+    __syncthreads();
+    // 3. forward chroma gradients, zero outside the active area (MenonDemosaic.cpp:120-129).
+    for (int i = t; i < DH_W * DH_H; i += MN_THREADS) {
+        const int sx = i % DH_W, sy = i / DH_W;
+        const int x = c.x0 - 4 + sx, y = c.y0 - 4 + sy;
+        if (!c.needed(x, y, 2, 4)) continue;
+        double d = 0.0;
+        if (c.inside(x, y)) d = fabs(__dadd_rn(S.ch[sy][sx], -S.ch[sy][sx + 2]));
+        S.dh[sy][sx] = d;
+    }
+    for (int i = t; i < DV_W * DV_H; i += MN_THREADS) {
+        const int sx = i % DV_W, sy = i / DV_W;
+        const int x = c.x0 - 4 + sx, y = c.y0 - 4 + sy;
+        if (!c.needed(x, y, 4, 2)) continue;
+        double d = 0.0;
+        if (c.inside(x, y)) d = fabs(__dadd_rn(S.cv[sy][sx], -S.cv[sy + 2][sx]));
+        S.dv[sy][sx] = d;
+    }
+    __syncthreads();
+    // 4. classifier and green (MenonDemosaic.cpp:130-147): terms in the
+    //    reference's order, horizontal wins ties (v >= h).
+    unsigned long long local_ties = 0;
+    for (int i = t; i < GR_W * GR_H; i += MN_THREADS) {
+        const int sx = i % GR_W, sy = i / GR_W;
+        if (!c.needed(c.x0 - 2 + sx, c.y0 - 2 + sy, 2, 2)) continue;
+        const int x = c.mx(c.x0 - 2 + sx), y = c.my(c.y0 - 2 + sy);
+        if (color_of(raw, x, y) == 1) {
+            S.horiz[sy][sx] = 1;
+            S.green[sy][sx] = raw_at(S, c, x, y);
+            continue;
+        }
+        // dh index of (x+a, y+b): [y+b-(y0-4)][x+a-(x0-4)]
+        const int hx = x - (c.x0 - 4), hy = y - (c.y0 - 4);
+        const double (*dh)[DH_W] = S.dh;
+        const double (*dv)[DV_W] = S.dv;
+        double h = 0.0, v = 0.0;
+        h = __dadd_rn(h, dh[hy + 2][hx + 0]);
+        v = __dadd_rn(v, dv[hy + 0][hx + 2]);
+        h = __dadd_rn(h, dh[hy + 2][hx - 2]);
+        v = __dadd_rn(v, dv[hy - 2][hx + 2]);
+        h = __dadd_rn(h, dh[hy + 1][hx - 1]);
+        v = __dadd_rn(v, dv[hy - 1][hx + 1]);
+        h = __dadd_rn(h, __dmul_rn(3.0, dh[hy + 0][hx + 0]));
+        v = __dadd_rn(v, __dmul_rn(3.0, dv[hy + 0][hx + 0]));
+        h = __dadd_rn(h, __dmul_rn(3.0, dh[hy + 0][hx - 2]));
+        v = __dadd_rn(v, __dmul_rn(3.0, dv[hy - 2][hx + 0]));
+        h = __dadd_rn(h, dh[hy - 1][hx - 1]);
+        v = __dadd_rn(v, dv[hy - 1][hx - 1]);
+        h = __dadd_rn(h, dh[hy - 2][hx + 0]);
+        v = __dadd_rn(v, dv[hy + 0][hx - 2]);
+        h = __dadd_rn(h, dh[hy - 2][hx - 2]);
+        v = __dadd_rn(v, dv[hy - 2][hx - 2]);
+        const bool horizontal = v >= h;
+        if (ties && v == h && sx >= 2 && sx < GR_W - 2 && sy >= 2 && sy < GR_H - 2) ++local_ties;
+        S.horiz[sy][sx] = horizontal;
+        S.green[sy][sx] = horizontal ? green_h(S, c, x, y) : green_v(S, c, x, y);
+    }
+    if (ties && local_ties) atomicAdd(ties, local_ties);
+    __syncthreads();
+    // 5. red and blue at every colour-support site (MenonDemosaic.cpp:151-161).
+    for (int i = t; i < CO_W * CO_H; i += MN_THREADS) {
+        const int sx = i % CO_W, sy = i / CO_W;
+        if (!c.needed(c.x0 - 1 + sx, c.y0 - 1 + sy, 1, 1)) continue;
+        const int x = c.mx(c.x0 - 1 + sx), y = c.my(c.y0 - 1 + sy);
+        const int own = color_of(raw, x, y);
+        double rr = 0.0, bb = 0.0;
+        if (own == 0) rr = raw_at(S, c, x, y);
+        if (own == 2) bb = raw_at(S, c, x, y);
+        if (own == 1) {
+            const bool red_h = color_of(raw, x + 1, y) == 0;
+            const int dx = red_h ? 1 : 0, dy = red_h ? 0 : 1;
+            const double g = S.green[y - (c.y0 - 2)][x - (c.x0 - 2)];
+            const double rm = __dmul_rn(0.5, __dadd_rn(raw_at(S, c, x - dx, y - dy), raw_at(S, c, x + dx, y + dy)));
+            const double bm = __dmul_rn(0.5, __dadd_rn(raw_at(S, c, x - dy, y - dx), raw_at(S, c, x + dy, y + dx)));
+            const double gr = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dx, dy);
+            const double gb = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dy, dx);
+            rr = __dadd_rn(__dadd_rn(g, rm), -gr);
+            bb = __dadd_rn(__dadd_rn(g, bm), -gb);
+        }
+        S.red[sy][sx] = rr;
+        S.blue[sy][sx] = bb;
+    }
+    __syncthreads();
+}
+
+// One CTA per MN_TW x MN_TH tile of `region` (sensor coordinates).  Writes
+// float32 RGB after stages [0, stage_end) to `out` (row stride in floats).
+__global__ void __launch_bounds__(MN_THREADS)
+menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int stage_end,
+             const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
+             uint32_t* status, unsigned long long* ties) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MenonSmem& S = *reinterpret_cast<MenonSmem*>(smem_raw);
+    MenonCtx c;
+    c.x0 = ox + blockIdx.x * MN_TW;
+    c.y0 = oy + blockIdx.y * MN_TH;
+    c.xe = min(c.x0 + MN_TW, ox + ow);
+    c.ye = min(c.y0 + MN_TH, oy + oh);
+    c.ax = raw.ax; c.ay = raw.ay; c.aw = raw.aw; c.ah = raw.ah;
+    menon_tile(S, raw, c, ties);
+    // 6. final opposite colour at R/B sites, float cast, stage program
+    //    (MenonDemosaic.cpp:162-173).
+    uint32_t err = 0;
+    for (int i = threadIdx.x; i < MN_TW * MN_TH; i += MN_THREADS) {
+        const int tx = i % MN_TW, ty = i / MN_TW;
+        const int x = c.x0 + tx, y = c.y0 + ty;
+        if (x >= ox + ow || y >= oy + oh) continue;
+        const int own = color_of(raw, x, y);
+        const bool horizontal = S.horiz[ty + 2][tx + 2];
+        const int dx = horizontal ? 1 : 0, dy = horizontal ? 0 : 1;
+        double rr = S.red[ty + 1][tx + 1], bb = S.blue[ty + 1][tx + 1];
+        if (own == 2)
+            rr = __dadd_rn(__dadd_rn(bb, pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy)),
+                           -pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy));
+        if (own == 0)
+            bb = __dadd_rn(__dadd_rn(rr, pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy)),
+                           -pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy));
+        float r = (float)rr, g = (float)S.green[ty + 2][tx + 2], b = (float)bb;
+        apply_stages(P, 0, stage_end, r, g, b, err);
+        float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+        o[0] = r;
+        o[1] = g;
+        o[2] = b;
+    }
+    report(status, err);
+}
+
+// ------------------------------------------------------------ mip reduction
+
+// RawEngine.cpp:585-600: each reduced pixel averages its native footprint
+// (clipped at the native region's edge, actual count) in double, row-major
+// footprint order; then the stages after the anchor run on the reduced pixel.
+__global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int nh,
+                                  size_t native_stride, int scale, int ow, int oh, int stage_begin,
+                                  int stage_end, const __grid_constant__ DevProgram P,
+                                  float* __restrict__ out, size_t out_stride, uint32_t* status) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= ow || y >= oh) return;
+    double s0 = 0, s1 = 0, s2 = 0;
+    int count = 0;
+    const int y1 = min((y + 1) * scale, nh), x1 = min((x + 1) * scale, nw);
+    for (int sy = y * scale; sy < y1; ++sy)
+        for (int sx = x * scale; sx < x1; ++sx) {
+            const float* p = native + (size_t)sy * native_stride + (size_t)sx * 3;
+            s0 = __dadd_rn(s0, (double)p[0]);
+            s1 = __dadd_rn(s1, (double)p[1]);
+            s2 = __dadd_rn(s2, (double)p[2]);
+            ++count;
+        }
+    const double n = (double)count;
+    float r = (float)__ddiv_rn(s0, n), g = (float)__ddiv_rn(s1, n), b = (float)__ddiv_rn(s2, n);
+    uint32_t err = 0;
+    apply_stages(P, stage_begin, stage_end, r, g, b, err);
+    float* o = out + (size_t)y * out_stride + (size_t)x * 3;
+    o[0] = r;
+    o[1] = g;
+    o[2] = b;
+    report(status, err);
+}
+
+// ------------------------------------------------------------------- launch
+
+size_t menon_smem_bytes() { return sizeof(MenonSmem); }
+
+cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
+                            int stage_end, const DevProgram& P, float* out, size_t out_stride,
+                            uint32_t* status, unsigned long long* ties, cudaStream_t stream,
+                            uint32_t* launches) {
+    if (ow <= 0 || oh <= 0) return cudaSuccess;
+    // Menon with a singleton active-area axis is bilinear (RawEngine.cpp:303).
+    if (demosaic == 1 && raw.aw > 1 && raw.ah > 1) {
+        static bool configured = false;
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)sizeof(MenonSmem));
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        dim3 grid((ow + MN_TW - 1) / MN_TW, (oh + MN_TH - 1) / MN_TH);
+        menon_kernel<<<grid, MN_THREADS, sizeof(MenonSmem), stream>>>(raw, ox, oy, ow, oh, stage_end, P,
+                                                                       out, out_stride, status, ties);
+    } else {
+        dim3 grid((ow + BL_TW - 1) / BL_TW, (oh + BL_TH - 1) / BL_TH);
+        bilinear_kernel<<<grid, BL_THREADS, 0, stream>>>(raw, ox, oy, ow, oh, stage_end, P, out,
+                                                         out_stride, status);
+    }
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mip_reduce(const float* native, int nw, int nh, size_t native_stride, int mip,
+                              int ow, int oh, int stage_begin, int stage_end, const DevProgram& P,
+                              float* out, size_t out_stride, uint32_t* status, cudaStream_t stream,
+                              uint32_t* launches) {
+    if (ow <= 0 || oh <= 0) return cudaSuccess;
+    dim3 block(32, 8);
+    dim3 grid((ow + 31) / 32, (oh + 7) / 8);
+    mip_reduce_kernel<<<grid, block, 0, stream>>>(native, nw, nh, native_stride, 1 << mip, ow, oh,
+                                                  stage_begin, stage_end, P, out, out_stride, status);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+}  // namespace re
