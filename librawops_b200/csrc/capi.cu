@@ -45,6 +45,14 @@ re_status cuda_fail(cudaError_t e, const char* where) {
     return fail(RE_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
+}  // namespace
+
+namespace re {
+void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace re
+
+namespace {
+
 #define RE_CUDA(call)                                       \
     do {                                                    \
         cudaError_t e_ = (call);                            \
