@@ -66,21 +66,36 @@ class ClockSampler:
         self.proc = None
         self.lines = []
 
-    def __enter__(self):
+    def start(self):
+        """Starts sampling and waits for the first sample, so that the tool's
+        start-up never overlaps the timed region."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
 
+    def mark(self):
+        self.first = len(self.lines)
+
+    def stop(self):
+        self.last = len(self.lines)
+        self.__exit__()
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def __enter__(self):
+        return self.start()
 
     def __exit__(self, *a):
         if self.proc:
@@ -93,7 +108,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        window = self.lines[getattr(self, "first", 0):getattr(self, "last", len(self.lines)) + 1]
+        for line in window:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -111,67 +127,72 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_rate(workload, rows: int, repeats: int):
-    """Reference CPU implementation (oracle/_ref through its TileScheduler with one
-    worker per host core, else the C oracle port) on a horizontal strip of the
-    same frame: returns (Mpix/s, kind, cores, sample)."""
-    from oracle.oracle import (OP_CAMERA_TO_WORKING, OP_CURVES_EXT, OP_DISPLAY_TAG, OP_SRGB_ENCODE, OP_WB,
-                               OP_WORKING_TO_SRGB, Op, Oracle, RawSpec, Reference, curves_params,
-                               reference_available)
-    w = workload
-    samples = w.samples().reshape(-1)
-    raw = RawSpec(w.width, w.height, samples, w.stride, w.pattern, *w.phase, w.active, w.black, (w.white,) * 4)
-    ops = [Op(OP_WB, list(w.wb)), Op(OP_CAMERA_TO_WORKING, list(w.camera_to_xyz.reshape(9)) + [0]),
-           Op(OP_CURVES_EXT, curves_params(1, w.curve)), Op(OP_WORKING_TO_SRGB), Op(OP_DISPLAY_TAG),
-           Op(OP_SRGB_ENCODE)]
-    ax, ay, aw, ah = w.active
-    strip = (ax, ay + ah // 2 - rows // 2, aw, rows)
-    cores = os.cpu_count() or 1
-    times = []
-    if reference_available():
-        ref = Reference()
-        ref.render_raw(raw, True, ops, (ax, ay, 64, 64), tile=w.tile)
-        for _ in range(repeats):
-            t0 = time.perf_counter()
-            ref.render_raw(raw, True, ops, strip, tile=w.tile, scheduled_workers=min(cores, 64))
-            times.append(time.perf_counter() - t0)
-        kind = "reference"
-        threads = min(cores, 64)
-    else:
-        orc = Oracle()
-        ops_port = [o for o in ops if o.code != OP_DISPLAY_TAG]
-        for _ in range(repeats):
-            t0 = time.perf_counter()
-            orc.render_raw(raw, True, ops_port, strip)
-            times.append(time.perf_counter() - t0)
-        kind = "port"
-        threads = 1
-    px = strip[2] * strip[3]
-    rate = px / statistics.median(times) / 1e6
-    return rate, kind, threads, f"{strip[2]}x{strip[3]} strip of the frame, tile {w.tile}, median of {repeats}"
+class CpuReference:
+    """The reference's own CPU implementation of the workload: the reference
+    library built from its sources (oracle/_ref), driven through its
+    TileScheduler with one worker per host core; the C oracle port (one thread)
+    when that library is absent."""
+
+    def __init__(self, workload):
+        from oracle.oracle import (OP_CAMERA_TO_WORKING, OP_CURVES_EXT, OP_DISPLAY_TAG, OP_SRGB_ENCODE,
+                                   OP_WB, OP_WORKING_TO_SRGB, Op, Oracle, RawSpec, Reference, curves_params,
+                                   reference_available)
+        w = self.w = workload
+        samples = w.samples().reshape(-1)
+        self.raw = RawSpec(w.width, w.height, samples, w.stride, w.pattern, *w.phase, w.active, w.black,
+                           (w.white,) * 4)
+        self.ops = [Op(OP_WB, list(w.wb)), Op(OP_CAMERA_TO_WORKING, list(w.camera_to_xyz.reshape(9)) + [0]),
+                    Op(OP_CURVES_EXT, curves_params(1, w.curve)), Op(OP_WORKING_TO_SRGB), Op(OP_DISPLAY_TAG),
+                    Op(OP_SRGB_ENCODE)]
+        self.cores = os.cpu_count() or 1
+        if reference_available():
+            self.impl, self.kind, self.threads = Reference(), "reference", min(self.cores, 64)
+        else:
+            self.impl, self.kind, self.threads = Oracle(), "port", 1
+            self.ops = [o for o in self.ops if o.code != OP_DISPLAY_TAG]
+
+    def strip(self, rows):
+        ax, ay, aw, ah = self.w.active
+        return (ax, ay + ah // 2 - rows // 2, aw, rows)
+
+    def render_seconds(self, rows):
+        s = self.strip(rows)
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            self.impl.render_raw(self.raw, True, self.ops, s, tile=self.w.tile, scheduled_workers=self.threads)
+        else:
+            self.impl.render_raw(self.raw, True, self.ops, s)
+        return time.perf_counter() - t0
+
+    def rate(self, rows, repeats):
+        self.render_seconds(8)
+        times = [self.render_seconds(rows) for _ in range(repeats)]
+        return rows * self.w.active[2] / statistics.median(times) / 1e6
+
+    def sample_text(self, rows, repeats):
+        s = self.strip(rows)
+        return f"{s[2]}x{s[3]} strip of the frame, tile {self.w.tile}, median of {repeats}"
 
 
 def run_reference(args, rank):
     from librawops_b200 import workloads
     if rank != 0:
         return
-    w = workloads.menon_24mp()
-    steps = []
-    rows = 400
+    ref = CpuReference(workloads.menon_24mp())
+    # each step is a bounded strip of the frame, sized so that the whole run
+    # stays near a minute of host time
+    rows = max(2, min(400, int(40000 / max(1, args.steps + args.warmup))))
     for _ in range(args.warmup):
-        cpu_reference_rate(w, rows, 1)
-    for _ in range(args.steps):
-        rate, kind, cores, sample = cpu_reference_rate(w, rows, 1)
-        steps.append(rate)
-    value = statistics.median(steps)
+        ref.render_seconds(rows)
+    t = [ref.render_seconds(rows) for _ in range(args.steps)]
+    value = rows * ref.w.active[2] * len(t) / sum(t) / 1e6
     line = {"metric": METRIC, "value": round(value, 3), "unit": "Mpix/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(rows * w.active[2] / value / 1e3, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": w.name, "sample_rows": rows, "tile": w.tile},
-            "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": cores, "kind": kind,
-                             "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(t) / len(t), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": ref.w.name, "sample_rows_per_step": rows, "tile": ref.w.tile},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": ref.threads, "kind": ref.kind,
+                             "sample": ref.sample_text(rows, args.steps)},
             "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -207,19 +228,21 @@ def run_ours(args, rank, world, local_rank):
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank).start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t_begin = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clocks:
-        t_begin.record(stream)
-        for i in range(args.steps):
-            starts[i].record(stream)
-            step()
-            ends[i].record(stream)
-        t_end.record(stream)
-        torch.cuda.synchronize()
+    clocks.mark()
+    t_begin.record(stream)
+    for i in range(args.steps):
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clocks.stop()
     if world > 1:
         dist.barrier()
     total_ms = t_begin.elapsed_time(t_end)
@@ -263,8 +286,9 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = _peaks()
     traffic = _traffic_from_profile()
     try:
-        cpu_rate, kind, cores, sample = cpu_reference_rate(w, 200, 3)
-        cpu = {"value": round(cpu_rate, 3), "unit": "Mpix/s", "cores": cores, "kind": kind, "sample": sample}
+        ref = CpuReference(w)
+        cpu = {"value": round(ref.rate(200, 3), 3), "unit": "Mpix/s", "cores": ref.threads, "kind": ref.kind,
+               "sample": ref.sample_text(200, 3)}
     except Exception as e:  # the checker libraries are missing
         cpu = {"value": None, "unit": "Mpix/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
     line = {
@@ -292,8 +316,8 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

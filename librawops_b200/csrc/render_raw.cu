@@ -258,28 +258,221 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
     __syncthreads();
 }
 
-// One CTA per MN_TW x MN_TH tile of `region` (sensor coordinates).  Writes
-// float32 RGB after stages [0, stage_end) to `out` (row stride in floats).
-__global__ void __launch_bounds__(MN_THREADS)
-menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int stage_end,
+// ------------------------------------------------- menon fast interior path
+//
+// Tiles whose r=6 raw footprint lies inside the active area need no mirroring
+// and no zero extension, and with an even tile origin the CFA colour of each
+// position of a 2x2 quad is a compile-time constant (template L = the Bayer
+// layout seen from the quad's top-left).  Each thread then works on whole
+// quads with constant shared-memory offsets: chroma/gradients only at the two
+// non-green sites, greens copied, every neighbour a single shared load.  The
+// arithmetic is the reference's, in binary64, in the reference's order.
+
+// Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
+__host__ __device__ constexpr int pat(int l, int k) {
+    return l == 0   ? (k == 0 ? 0 : k == 3 ? 2 : 1)
+           : l == 1 ? (k == 0 ? 2 : k == 3 ? 0 : 1)
+           : l == 2 ? (k == 1 ? 0 : k == 2 ? 2 : 1)
+                    : (k == 1 ? 2 : k == 2 ? 0 : 1);
+}
+constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, origin (-6,-6)
+constexpr int FC_W = MN_TW + 8, FC_H = MN_TH + 8;     // gh gv ch cv dh dv, origin (-4,-4)
+constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, origin (-2,-2)
+
+struct FastSmem {
+    double raw[FR_H * FR_W];
+    double gh[FC_H * FC_W];
+    double gv[FC_H * FC_W];
+    double ch[FC_H * FC_W];      // reused as red after the gradients
+    double cv[FC_H * FC_W];      // reused as blue after the gradients
+    double dh[FC_H * FC_W];
+    double dv[FC_H * FC_W];
+    double green[FG_H * FG_W];
+    uint8_t horiz[FG_H * FG_W];
+};
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double half_sum(double a, double b) { return __dmul_rn(0.5, __dadd_rn(a, b)); }
+
+template <int L>
+__device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
+                                           int ow, int oh, int stage_end, const DevProgram& P,
+                                           float* __restrict__ out, size_t out_stride, uint32_t& err) {
+    const int t = threadIdx.x;
+    // 1. normalized raw (RawEngine.cpp:89-97) as binary64, r = 6 around the tile
+    for (int i = t; i < FR_W * FR_H; i += MN_THREADS) {
+        const int sx = i % FR_W, sy = i / FR_W;
+        S.raw[i] = (double)normalize_sample(raw, x0 - 6 + sx, y0 - 6 + sy);
+    }
+    __syncthreads();
+    // 2. directional green and chroma at non-green sites (MenonDemosaic.cpp:107-119)
+    for (int q = t; q < (FC_W / 2) * (FC_H / 2); q += MN_THREADS) {
+        const int qx = q % (FC_W / 2), qy = q / (FC_W / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            if (pat(L, k) == 1) continue;
+            const int pc = (2 * qy + j) * FC_W + 2 * qx + i;
+            const int pr = (2 * qy + j + 2) * FR_W + 2 * qx + i + 2;
+            const double* r = S.raw + pr;
+            const double own = r[0];
+            const double h = dsub(dadd(half_sum(r[-1], r[1]), __dmul_rn(0.5, own)),
+                                  __dmul_rn(0.25, dadd(r[-2], r[2])));
+            const double v = dsub(dadd(half_sum(r[-FR_W], r[FR_W]), __dmul_rn(0.5, own)),
+                                  __dmul_rn(0.25, dadd(r[-2 * FR_W], r[2 * FR_W])));
+            S.gh[pc] = h;
+            S.gv[pc] = v;
+            S.ch[pc] = dsub(own, h);
+            S.cv[pc] = dsub(own, v);
+        }
+    }
+    __syncthreads();
+    // 3. forward chroma gradients at non-green sites (MenonDemosaic.cpp:120-125)
+    for (int q = t; q < (FC_W / 2) * (FC_H / 2); q += MN_THREADS) {
+        const int qx = q % (FC_W / 2), qy = q / (FC_W / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            if (pat(L, k) == 1) continue;
+            const int x = 2 * qx + i, y = 2 * qy + j;
+            const int p = y * FC_W + x;
+            if (x < FC_W - 2) S.dh[p] = fabs(dsub(S.ch[p], S.ch[p + 2]));
+            if (y < FC_H - 2) S.dv[p] = fabs(dsub(S.cv[p], S.cv[p + 2 * FC_W]));
+        }
+    }
+    __syncthreads();
+    // 4. classifier and green (MenonDemosaic.cpp:130-147), terms in reference order
+    for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
+        const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            const int gx = 2 * qx + i, gy = 2 * qy + j;
+            const int pg = gy * FG_W + gx;
+            if (pat(L, k) == 1) {
+                S.green[pg] = S.raw[(gy + 4) * FR_W + gx + 4];
+                S.horiz[pg] = 1;
+                continue;
+            }
+            const int p = (gy + 2) * FC_W + gx + 2;
+            const double* dh = S.dh + p;
+            const double* dv = S.dv + p;
+            double h = 0.0, v = 0.0;
+            h = dadd(h, dh[2 * FC_W]);                       v = dadd(v, dv[2]);
+            h = dadd(h, dh[2 * FC_W - 2]);                   v = dadd(v, dv[-2 * FC_W + 2]);
+            h = dadd(h, dh[FC_W - 1]);                       v = dadd(v, dv[-FC_W + 1]);
+            h = dadd(h, __dmul_rn(3.0, dh[0]));              v = dadd(v, __dmul_rn(3.0, dv[0]));
+            h = dadd(h, __dmul_rn(3.0, dh[-2]));             v = dadd(v, __dmul_rn(3.0, dv[-2 * FC_W]));
+            h = dadd(h, dh[-FC_W - 1]);                      v = dadd(v, dv[-FC_W - 1]);
+            h = dadd(h, dh[-2 * FC_W]);                      v = dadd(v, dv[-2]);
+            h = dadd(h, dh[-2 * FC_W - 2]);                  v = dadd(v, dv[-2 * FC_W - 2]);
+            const bool horizontal = v >= h;
+            S.horiz[pg] = horizontal;
+            S.green[pg] = horizontal ? S.gh[p] : S.gv[p];
+        }
+    }
+    __syncthreads();
+    // 5. red and blue on the r=1 ring (MenonDemosaic.cpp:151-161); chroma planes are dead
+    double* red = S.ch;
+    double* blue = S.cv;
+    for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
+        const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            const int gx = 2 * qx + i, gy = 2 * qy + j;
+            if (gx == 0 || gx == FG_W - 1 || gy == 0 || gy == FG_H - 1) continue;
+            const int pg = gy * FG_W + gx;
+            const int pr = (gy + 4) * FR_W + gx + 4;
+            const int own = pat(L, k);
+            double rr = 0.0, bb = 0.0;
+            if (own == 0) rr = S.raw[pr];
+            if (own == 2) bb = S.raw[pr];
+            if (own == 1) {
+                // colour of the horizontal neighbour (same row, other column of the quad)
+                const bool red_h = pat(L, (j << 1) | (i ^ 1)) == 0;
+                const int dr = red_h ? 1 : FR_W, dg = red_h ? 1 : FG_W;      // red axis
+                const int br = red_h ? FR_W : 1, bg = red_h ? FG_W : 1;      // blue axis
+                const double g = S.green[pg];
+                rr = dsub(dadd(g, half_sum(S.raw[pr - dr], S.raw[pr + dr])),
+                          half_sum(S.green[pg - dg], S.green[pg + dg]));
+                bb = dsub(dadd(g, half_sum(S.raw[pr - br], S.raw[pr + br])),
+                          half_sum(S.green[pg - bg], S.green[pg + bg]));
+            }
+            red[pg] = rr;
+            blue[pg] = bb;
+        }
+    }
+    __syncthreads();
+    // 6. opposite colour at R/B sites, float cast, fused stages (MenonDemosaic.cpp:162-173)
+    for (int q = t; q < (MN_TW / 2) * (MN_TH / 2); q += MN_THREADS) {
+        const int qx = q % (MN_TW / 2), qy = q / (MN_TW / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
+            const int pg = (2 * qy + j + 2) * FG_W + 2 * qx + i + 2;
+            const int own = pat(L, k);
+            const int d = S.horiz[pg] ? 1 : FG_W;
+            double rr = red[pg], bb = blue[pg];
+            if (own == 2) rr = dsub(dadd(bb, half_sum(red[pg - d], red[pg + d])), half_sum(blue[pg - d], blue[pg + d]));
+            if (own == 0) bb = dsub(dadd(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
+            float r = (float)rr, g = (float)S.green[pg], b = (float)bb;
+            if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
+            apply_stages(P, 0, stage_end, r, g, b, err);
+            float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+            o[0] = r;
+            o[1] = g;
+            o[2] = b;
+        }
+    }
+}
+
+union MenonShared {
+    MenonSmem generic;
+    FastSmem fast;
+};
+
+// One CTA per MN_TW x MN_TH tile of the viewport, tiles anchored at an even
+// sensor coordinate.  Interior tiles take the fast quad path; tiles whose
+// footprint meets the active-area edge take the general mirrored path.
+// Writes float32 RGB after stages [0, stage_end) (row stride in floats).
+__global__ void __launch_bounds__(MN_THREADS, 2)
+menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
              const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
              uint32_t* status, unsigned long long* ties) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MenonSmem& S = *reinterpret_cast<MenonSmem*>(smem_raw);
+    const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
+    const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
+    uint32_t err = 0;
+    const bool interior = !ties && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay && x0 + MN_TW + 6 <= raw.ax + raw.aw &&
+                          y0 + MN_TH + 6 <= raw.ay + raw.ah;
+    if (interior) {
+        FastSmem& F = reinterpret_cast<MenonShared*>(smem_raw)->fast;
+        switch (layout) {
+        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        }
+        report(status, err);
+        return;
+    }
+    MenonSmem& S = reinterpret_cast<MenonShared*>(smem_raw)->generic;
     MenonCtx c;
-    c.x0 = ox + blockIdx.x * MN_TW;
-    c.y0 = oy + blockIdx.y * MN_TH;
+    c.x0 = x0;
+    c.y0 = y0;
     c.xe = min(c.x0 + MN_TW, ox + ow);
     c.ye = min(c.y0 + MN_TH, oy + oh);
     c.ax = raw.ax; c.ay = raw.ay; c.aw = raw.aw; c.ah = raw.ah;
     menon_tile(S, raw, c, ties);
     // 6. final opposite colour at R/B sites, float cast, stage program
     //    (MenonDemosaic.cpp:162-173).
-    uint32_t err = 0;
     for (int i = threadIdx.x; i < MN_TW * MN_TH; i += MN_THREADS) {
         const int tx = i % MN_TW, ty = i / MN_TW;
         const int x = c.x0 + tx, y = c.y0 + ty;
-        if (x >= ox + ow || y >= oy + oh) continue;
+        if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
         const int own = color_of(raw, x, y);
         const bool horizontal = S.horiz[ty + 2][tx + 2];
         const int dx = horizontal ? 1 : 0, dy = horizontal ? 0 : 1;
@@ -336,7 +529,19 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
 
 // ------------------------------------------------------------------- launch
 
-size_t menon_smem_bytes() { return sizeof(MenonSmem); }
+size_t menon_smem_bytes() { return sizeof(MenonShared); }
+
+// Bayer layout seen from an even sensor coordinate (the fast path's template).
+static int quad_layout(const DevRaw& raw) {
+    int e[4];
+    for (int k = 0; k < 4; ++k) {
+        const int i = k & 1, j = k >> 1;
+        e[k] = raw.site_color[((j + (int)raw.phase_y) & 1) * 2 + ((i + (int)raw.phase_x) & 1)];
+    }
+    for (int l = 0; l < 4; ++l)
+        if (pat(l, 0) == e[0] && pat(l, 1) == e[1] && pat(l, 2) == e[2] && pat(l, 3) == e[3]) return l;
+    return 0;
+}
 
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
                             int stage_end, const DevProgram& P, float* out, size_t out_stride,
@@ -345,16 +550,14 @@ cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy
     if (ow <= 0 || oh <= 0) return cudaSuccess;
     // Menon with a singleton active-area axis is bilinear (RawEngine.cpp:303).
     if (demosaic == 1 && raw.aw > 1 && raw.ah > 1) {
-        static bool configured = false;
-        if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)sizeof(MenonSmem));
-            if (e != cudaSuccess) return e;
-            configured = true;
-        }
-        dim3 grid((ow + MN_TW - 1) / MN_TW, (oh + MN_TH - 1) / MN_TH);
-        menon_kernel<<<grid, MN_THREADS, sizeof(MenonSmem), stream>>>(raw, ox, oy, ow, oh, stage_end, P,
-                                                                       out, out_stride, status, ties);
+        cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(MenonShared));
+        if (e != cudaSuccess) return e;
+        const int gx0 = ox & ~1, gy0 = oy & ~1;
+        dim3 grid((ox + ow - gx0 + MN_TW - 1) / MN_TW, (oy + oh - gy0 + MN_TH - 1) / MN_TH);
+        menon_kernel<<<grid, MN_THREADS, sizeof(MenonShared), stream>>>(raw, ox, oy, ow, oh, quad_layout(raw),
+                                                                         stage_end, P, out, out_stride, status,
+                                                                         ties);
     } else {
         dim3 grid((ow + BL_TW - 1) / BL_TW, (oh + BL_TH - 1) / BL_TH);
         bilinear_kernel<<<grid, BL_THREADS, 0, stream>>>(raw, ox, oy, ow, oh, stage_end, P, out,

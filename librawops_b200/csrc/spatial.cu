@@ -91,7 +91,7 @@ __global__ void gf_hbox_moments(const float* __restrict__ in, size_t in_stride, 
 #pragma unroll
         for (int q = 0; q < 8; ++q) h[q] = s[q];
     }
-    if (bad && status) atomicMax(status, (uint32_t)((400u << 8) | ST_INVALID));
+    if (bad && status) atomicMax(status, (uint32_t)((401u << 8) | ST_INVALID));
 }
 
 // Vertical box sums of H, then the per-centre regression a, b (float AB: 6 per px).

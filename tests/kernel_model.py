@@ -53,7 +53,7 @@ def mirror(v, origin, size):
     return origin + (folded if folded < size else period - folded)
 
 
-def model_render(meta, samples, viewport):
+def model_render(meta, samples, viewport, fast=True):
     """meta: dict(width,height,stride,pattern,phase_x,phase_y,active,black,white)."""
     ax, ay, aw, ah = meta["active"]
     stride = meta["stride"]
@@ -76,10 +76,15 @@ def model_render(meta, samples, viewport):
     ox, oy, ow, oh = viewport
     out = np.zeros((oh, ow, 3), np.float32)
     inside = lambda x, y: ax <= x < ax + aw and ay <= y < ay + ah
-    for by in range((oh + TH - 1) // TH):
-        for bx in range((ow + TW - 1) // TW):
-            x0, y0 = ox + bx * TW, oy + by * TH
+    gx0, gy0 = ox & ~1, oy & ~1
+    for by in range((oy + oh - gy0 + TH - 1) // TH):
+        for bx in range((ox + ow - gx0 + TW - 1) // TW):
+            x0, y0 = gx0 + bx * TW, gy0 + by * TH
             xe, ye = min(x0 + TW, ox + ow), min(y0 + TH, oy + oh)
+            if (fast and x0 - 6 >= ax and y0 - 6 >= ay and x0 + TW + 6 <= ax + aw
+                    and y0 + TH + 6 <= ay + ah):
+                _fast_tile(meta, sample, color, x0, y0, viewport, out)
+                continue
             needed = lambda x, y, rx, ry: x < xe + rx and y < ye + ry
             mx = lambda x: mirror(x, ax, aw)
             my = lambda y: mirror(y, ay, ah)
@@ -166,8 +171,8 @@ def model_render(meta, samples, viewport):
                         bb = (g + pm(raw, x, y, dy, dx)) - pm(green, x, y, dy, dx)
                     red.set(vx, vy, rr)
                     blue.set(vx, vy, bb)
-            for y in range(y0, ye):
-                for x in range(x0, xe):
+            for y in range(max(y0, oy), ye):
+                for x in range(max(x0, ox), xe):
                     own = color(x, y)
                     hz = horiz.get(x, y) != 0
                     dx, dy = (1, 0) if hz else (0, 1)
@@ -178,3 +183,104 @@ def model_render(meta, samples, viewport):
                         bb = (rr + pm(blue, x, y, dx, dy)) - pm(red, x, y, dx, dy)
                     out[y - oy, x - ox] = (rr, green.get(x, y), bb)
     return out
+
+
+def _fast_tile(meta, sample, color, x0, y0, viewport, out):
+    """The interior quad path (menon_fast in render_raw.cu): flat planes with the
+    kernel's strides, colours from the even-origin quad layout."""
+    ox, oy, ow, oh = viewport
+    RW, RH, CW, CH, GW, GH = TW + 12, TH + 12, TW + 8, TH + 8, TW + 4, TH + 4
+    lay = [color(x0 + (k & 1), y0 + (k >> 1)) for k in range(4)]
+
+    def flat(n):
+        return Plane(n, 1, 0, 0)
+
+    raw, gh, gv, ch, cv, dh, dv = flat(RW * RH), flat(CW * CH), flat(CW * CH), flat(CW * CH), \
+        flat(CW * CH), flat(CW * CH), flat(CW * CH)
+    green, horiz = flat(GW * GH), flat(GW * GH)
+    for i in range(RW * RH):
+        raw.set(i, 0, sample(x0 - 6 + i % RW, y0 - 6 + i // RW))
+    half = lambda a, b: 0.5 * (a + b)
+    for q in range((CW // 2) * (CH // 2)):
+        qx, qy = q % (CW // 2), q // (CW // 2)
+        for k in range(4):
+            i, j = k & 1, k >> 1
+            if lay[k] == 1:
+                continue
+            pc = (2 * qy + j) * CW + 2 * qx + i
+            pr = (2 * qy + j + 2) * RW + 2 * qx + i + 2
+            r = lambda o: raw.get(pr + o, 0)
+            own = r(0)
+            h = (half(r(-1), r(1)) + 0.5 * own) - 0.25 * (r(-2) + r(2))
+            v = (half(r(-RW), r(RW)) + 0.5 * own) - 0.25 * (r(-2 * RW) + r(2 * RW))
+            gh.set(pc, 0, h); gv.set(pc, 0, v); ch.set(pc, 0, own - h); cv.set(pc, 0, own - v)
+    for q in range((CW // 2) * (CH // 2)):
+        qx, qy = q % (CW // 2), q // (CW // 2)
+        for k in range(4):
+            i, j = k & 1, k >> 1
+            if lay[k] == 1:
+                continue
+            x, y = 2 * qx + i, 2 * qy + j
+            p = y * CW + x
+            if x < CW - 2:
+                dh.set(p, 0, abs(ch.get(p, 0) - ch.get(p + 2, 0)))
+            if y < CH - 2:
+                dv.set(p, 0, abs(cv.get(p, 0) - cv.get(p + 2 * CW, 0)))
+    for q in range((GW // 2) * (GH // 2)):
+        qx, qy = q % (GW // 2), q // (GW // 2)
+        for k in range(4):
+            i, j = k & 1, k >> 1
+            gx, gy = 2 * qx + i, 2 * qy + j
+            pg = gy * GW + gx
+            if lay[k] == 1:
+                green.set(pg, 0, raw.get((gy + 4) * RW + gx + 4, 0)); horiz.set(pg, 0, 1.0)
+                continue
+            p = (gy + 2) * CW + gx + 2
+            H = lambda o: dh.get(p + o, 0)
+            V = lambda o: dv.get(p + o, 0)
+            h = v = 0.0
+            for oh_, ov_, w in ((2 * CW, 2, 1), (2 * CW - 2, -2 * CW + 2, 1), (CW - 1, -CW + 1, 1),
+                                (0, 0, 3), (-2, -2 * CW, 3), (-CW - 1, -CW - 1, 1), (-2 * CW, -2, 1),
+                                (-2 * CW - 2, -2 * CW - 2, 1)):
+                h += w * H(oh_)
+                v += w * V(ov_)
+            hz = v >= h
+            horiz.set(pg, 0, 1.0 if hz else 0.0)
+            green.set(pg, 0, gh.get(p, 0) if hz else gv.get(p, 0))
+    red, blue = flat(CW * CH), flat(CW * CH)
+    for q in range((GW // 2) * (GH // 2)):
+        qx, qy = q % (GW // 2), q // (GW // 2)
+        for k in range(4):
+            i, j = k & 1, k >> 1
+            gx, gy = 2 * qx + i, 2 * qy + j
+            if gx == 0 or gx == GW - 1 or gy == 0 or gy == GH - 1:
+                continue
+            pg = gy * GW + gx
+            pr = (gy + 4) * RW + gx + 4
+            rr = bb = 0.0
+            if lay[k] == 0:
+                rr = raw.get(pr, 0)
+            if lay[k] == 2:
+                bb = raw.get(pr, 0)
+            if lay[k] == 1:
+                red_h = lay[(j << 1) | (i ^ 1)] == 0
+                dr, dg = (1, 1) if red_h else (RW, GW)
+                br, bg = (RW, GW) if red_h else (1, 1)
+                g = green.get(pg, 0)
+                rr = (g + half(raw.get(pr - dr, 0), raw.get(pr + dr, 0))) - half(green.get(pg - dg, 0), green.get(pg + dg, 0))
+                bb = (g + half(raw.get(pr - br, 0), raw.get(pr + br, 0))) - half(green.get(pg - bg, 0), green.get(pg + bg, 0))
+            red.set(pg, 0, rr); blue.set(pg, 0, bb)
+    for q in range((TW // 2) * (TH // 2)):
+        qx, qy = q % (TW // 2), q // (TW // 2)
+        for k in range(4):
+            i, j = k & 1, k >> 1
+            x, y = x0 + 2 * qx + i, y0 + 2 * qy + j
+            pg = (2 * qy + j + 2) * GW + 2 * qx + i + 2
+            d = 1 if horiz.get(pg, 0) else GW
+            rr, bb = red.get(pg, 0), blue.get(pg, 0)
+            if lay[k] == 2:
+                rr = (bb + half(red.get(pg - d, 0), red.get(pg + d, 0))) - half(blue.get(pg - d, 0), blue.get(pg + d, 0))
+            if lay[k] == 0:
+                bb = (rr + half(blue.get(pg - d, 0), blue.get(pg + d, 0))) - half(red.get(pg - d, 0), red.get(pg + d, 0))
+            if ox <= x < ox + ow and oy <= y < oy + oh:
+                out[y - oy, x - ox] = (rr, green.get(pg, 0), bb)

@@ -9,7 +9,7 @@ from kernel_model import model_render
 from oracle.oracle import RawSpec
 
 CASES = [(2, 2, None), (3, 5, None), (5, 3, None), (2, 9, None), (33, 17, None), (40, 20, (1, 1, 37, 17)),
-         (64, 34, None), (37, 19, (2, 1, 33, 17))]
+         (64, 34, None), (37, 19, (2, 1, 33, 17)), (90, 50, (1, 0, 87, 49))]
 
 
 @pytest.mark.parametrize("w,h,act", CASES)
@@ -25,5 +25,5 @@ def test_menon_kernel_model(oracle, w, h, act):
         meta = dict(width=W, height=H, stride=stride, pattern=pattern, phase_x=px, phase_y=py, active=a,
                     black=raw.black, white=raw.white)
         for vp in (a, (a[0] + a[2] // 3, a[1] + a[3] // 3, max(1, a[2] // 3), max(1, a[3] // 3)),
-                   (a[0] + a[2] - 1, a[1] + a[3] - 1, 1, 1)):
+                   (a[0] + a[2] - 1, a[1] + a[3] - 1, 1, 1), (a[0] + 1, a[1] + 1, a[2] - 1, a[3] - 1)):
             assert bits_equal(model_render(meta, s, vp), oracle.demosaic(raw, vp, True)), (pattern, vp)
