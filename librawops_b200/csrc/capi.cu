@@ -161,10 +161,25 @@ DevRaw make_dev_raw(const re_raw_metadata& m, const uint16_t* dev) {
     r.ah = (int32_t)m.active_area.height;
     r.phase_x = m.cfa_phase_x;
     r.phase_y = m.cfa_phase_y;
+    r.rcp_exact = 0;
     for (int s = 0; s < 4; ++s) {
         r.site_color[s] = k_pattern_colors[m.pattern][s];
         r.black[s] = (float)m.black_levels[s];
         r.span[s] = (float)((int)m.white_levels[s] - (int)m.black_levels[s]);
+        // Exhaustive check of the reciprocal quotient against IEEE division for
+        // every numerator a 16-bit code can produce at this site.
+        const float d = r.span[s], rc = 1.0f / d;
+        bool exact = true;
+        for (int code = 0; code <= 65535 && exact; ++code) {
+            const float n = (float)code - r.black[s];
+            const float q0 = n * rc;
+            const float res = std::fma(-q0, d, n);
+            const float q = std::fma(res, rc, q0);
+            const float want = n / d;
+            exact = std::memcmp(&q, &want, sizeof(float)) == 0;
+        }
+        r.rcp[s] = rc;
+        if (exact) r.rcp_exact |= 1u << s;
     }
     return r;
 }

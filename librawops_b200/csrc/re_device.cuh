@@ -35,6 +35,8 @@ struct DevRaw {
     int32_t site_color[4];    // colour of each photosite index (pattern applied)
     float black[4];           // per-site black level as float
     float span[4];            // per-site (white - black) as float
+    float rcp[4];             // 1/span, used only where rcp_exact says it is exact
+    uint32_t rcp_exact;       // bit s: the reciprocal form equals IEEE division for every code
 };
 
 // Photosite index of RawEngine.cpp:74-77 for any integer position.
@@ -47,10 +49,23 @@ __host__ __device__ __forceinline__ int color_of(const DevRaw& r, int x, int y) 
 }
 
 // RawEngine.cpp:89-97: (float(raw) - black) / (white - black), IEEE division.
+// The numerator is an integer in [-65535, 65535]; for a site whose span passed
+// the host's exhaustive check (every numerator gives the same float as IEEE
+// division) the quotient is formed as q = n*rcp refined by one fused residual
+// step, which is three instructions instead of the division sequence.
+__device__ __forceinline__ float normalize_code(const DevRaw& r, int s, float code) {
+    const float n = __fsub_rn(code, r.black[s]);
+    if ((r.rcp_exact >> s) & 1u) {
+        const float q0 = __fmul_rn(n, r.rcp[s]);
+        const float res = __fmaf_rn(-q0, r.span[s], n);
+        return __fmaf_rn(res, r.rcp[s], q0);
+    }
+    return __fdiv_rn(n, r.span[s]);
+}
+
 __device__ __forceinline__ float normalize_sample(const DevRaw& r, int x, int y) {
     const int s = site_of(r, x, y);
-    const float code = (float)__ldg(r.samples + (size_t)y * r.stride + x);
-    return __fdiv_rn(__fsub_rn(code, r.black[s]), r.span[s]);
+    return normalize_code(r, s, (float)__ldg(r.samples + (size_t)y * r.stride + x));
 }
 
 // MenonDemosaic.cpp:60-66 whole-sample mirror about [origin, origin+size).
@@ -85,6 +100,24 @@ struct DevCurve {
 
 struct DevCurveSet {
     DevCurve c[4];            // master, R, G, B
+};
+
+// Shared-memory copy of a curve set whose curves have at most SC_MAX knots
+// (each CTA loads it once; the per-sample segment search then reads only
+// shared memory).
+constexpr int SC_MAX = 64;
+struct SmemCurve {
+    uint32_t n, identity, cubic, pad;
+    float xf[SC_MAX];
+    float xeq[SC_MAX];
+    float xn[SC_MAX];
+    float y[SC_MAX];
+    float slope[SC_MAX];
+    float inv_h[SC_MAX];
+    float4 coef[SC_MAX];
+};
+struct SmemCurveSet {
+    SmemCurve c[4];
 };
 
 // --------------------------------------------------------------- program

@@ -4,7 +4,8 @@
 // Bit-exactness: WhiteBalance, Exposure and the 3x3 matrices use explicitly
 // rounded float ops in the reference's evaluation order (no contraction), so
 // they reproduce the reference's float32 results exactly.  ToneCurve and
-// SrgbEncode call powf (a few ulp from the host libm); ExtendedCurves are
+// SrgbEncode take their power through exp2(e*log2(x)) on the hardware
+// approximations (a few 1e-7 from the host libm's powf); ExtendedCurves are
 // evaluated in float32 from host-prepared per-segment polynomials instead of
 // the reference's binary64 de Casteljau blend -- both stay far inside the
 // 1e-5 full-scale tolerance of the float outputs.
@@ -14,27 +15,66 @@
 
 namespace re {
 
-__device__ __forceinline__ float curve_map(const DevCurve* __restrict__ c, float v) {
+template <class Curve>
+__device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v) {
     if (c->identity) return v;
     const int n = (int)c->n;
     int lo = 0, hi = n;  // upper_bound over the RU-rounded knots
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (v < __ldg(&c->xf[mid])) hi = mid; else lo = mid + 1;
+        if (v < c->xf[mid]) hi = mid; else lo = mid + 1;
     }
     const int left = lo == 0 ? 0 : lo - 1;
     const int seg = left < n - 2 ? left : n - 2;
-    if (v == __ldg(&c->xeq[left])) return __ldg(&c->y[left]);
-    const float xl = __ldg(&c->xf[n - 1]);
-    const bool above = v > xl || (v == xl && isnan(__ldg(&c->xeq[n - 1])));
-    if (!c->cubic || v < __ldg(&c->xf[0]) || above) {
-        const float s = __ldg(&c->slope[seg]);
-        const float yl = __ldg(&c->y[left]);
-        return s == 0.0f ? yl : yl + (v - __ldg(&c->xn[left])) * s;
+    if (v == c->xeq[left]) return c->y[left];
+    const float xl = c->xf[n - 1];
+    const bool above = v > xl || (v == xl && isnan(c->xeq[n - 1]));
+    if (!c->cubic || v < c->xf[0] || above) {
+        const float s = c->slope[seg];
+        const float yl = c->y[left];
+        return s == 0.0f ? yl : yl + (v - c->xn[left]) * s;
     }
-    const float t = (v - __ldg(&c->xn[seg])) * __ldg(&c->inv_h[seg]);
-    const float4 k = __ldg(&c->coef[seg]);
+    const float t = (v - c->xn[seg]) * c->inv_h[seg];
+    const float4 k = c->coef[seg];
     return k.x + t * (k.y + t * (k.z + t * k.w));
+}
+
+// Loads curve set 0 of P into shared memory when every curve fits; returns it
+// (or null, in which case curves are read from global memory).  All threads
+// of the block must call it; it ends with a barrier.
+__device__ __forceinline__ const SmemCurveSet* load_curves(const DevProgram& P, SmemCurveSet* sc) {
+    const DevCurveSet* g = P.curves[0];
+    bool fits = g != nullptr;
+    if (fits)
+        for (int k = 0; k < 4; ++k) fits &= g->c[k].n <= (uint32_t)SC_MAX;
+    if (!fits) return nullptr;
+    for (int k = 0; k < 4; ++k) {
+        const DevCurve& src = g->c[k];
+        SmemCurve& dst = sc->c[k];
+        const int n = (int)src.n;
+        if (threadIdx.x == 0) {
+            dst.n = src.n;
+            dst.identity = src.identity;
+            dst.cubic = src.cubic;
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            dst.xf[i] = src.xf[i];
+            dst.xeq[i] = src.xeq[i];
+            dst.xn[i] = src.xn[i];
+            dst.y[i] = src.y[i];
+            dst.slope[i] = src.slope[i];
+            dst.inv_h[i] = src.inv_h[i];
+            dst.coef[i] = src.coef[i];
+        }
+    }
+    __syncthreads();
+    return sc;
+}
+
+// x^e for x in [0, 1] through the hardware log2/exp2 approximations: a few
+// 1e-7 relative, inside the float tolerance of the tone and sRGB stages.
+__device__ __forceinline__ float unit_pow(float x, float e) {
+    return x > 0.0f ? exp2f(e * __log2f(x)) : (e == 0.0f ? 1.0f : 0.0f);
 }
 
 // Error key of a failing stage: the earliest stage in chain order wins when
@@ -47,7 +87,8 @@ __device__ __forceinline__ uint32_t stage_key(int s, uint32_t kind) {
 
 // Applies stages [begin, end) of P to one pixel; `err` keeps the max key.
 __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int end, float& r,
-                                             float& g, float& b, uint32_t& err) {
+                                             float& g, float& b, uint32_t& err,
+                                             const SmemCurveSet* sc = nullptr) {
     float v[3] = {r, g, b};
     for (int s = begin; s < end; ++s) {
         const re_stage& st = P.st[s];
@@ -75,7 +116,7 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
                 const float lin = v[c];
                 const float mag = fabsf(lin);
                 const float comp = __fdiv_rn(mag, __fadd_rn(mag, shoulder));
-                const float mapped = inv_gamma == 1.0f ? comp : powf(comp, inv_gamma);
+                const float mapped = inv_gamma == 1.0f ? comp : unit_pow(comp, inv_gamma);
                 v[c] = copysignf(mapped, lin);
             }
             break;
@@ -93,21 +134,33 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
                 const float lin = fminf(fmaxf(v[c], 0.0f), 1.0f);
                 v[c] = lin <= 0.0031308f
                            ? __fmul_rn(12.92f, lin)
-                           : __fsub_rn(__fmul_rn(1.055f, powf(lin, 1.0f / 2.4f)), 0.055f);
+                           : __fsub_rn(__fmul_rn(1.055f, unit_pow(lin, 1.0f / 2.4f)), 0.055f);
             }
             break;
         }
         case RE_STAGE_CURVES: {
-            const DevCurveSet* cs = P.curves[st.arg];
             bool bad = !(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]));
+            if (sc && st.arg == 0) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const DevCurve* ch = &cs->c[c + 1];
-                if (cs->c[0].identity && ch->identity) continue;
-                const float master = curve_map(&cs->c[0], v[c]);
-                const float mapped = curve_map(ch, master);
-                if (!isfinite(master) || !isfinite(mapped)) bad = true;
-                v[c] = mapped;
+                for (int c = 0; c < 3; ++c) {
+                    const SmemCurve* ch = &sc->c[c + 1];
+                    if (sc->c[0].identity && ch->identity) continue;
+                    const float master = curve_map(&sc->c[0], v[c]);
+                    const float mapped = curve_map(ch, master);
+                    if (!isfinite(master) || !isfinite(mapped)) bad = true;
+                    v[c] = mapped;
+                }
+            } else {
+                const DevCurveSet* cs = P.curves[st.arg];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const DevCurve* ch = &cs->c[c + 1];
+                    if (cs->c[0].identity && ch->identity) continue;
+                    const float master = curve_map(&cs->c[0], v[c]);
+                    const float mapped = curve_map(ch, master);
+                    if (!isfinite(master) || !isfinite(mapped)) bad = true;
+                    v[c] = mapped;
+                }
             }
             if (bad) {
                 err = max(err, stage_key(s, ST_INVALID));

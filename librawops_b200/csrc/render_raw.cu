@@ -19,15 +19,71 @@ namespace re {
 constexpr int BL_TW = 64, BL_TH = 16, BL_THREADS = 256;
 constexpr int BL_SW = BL_TW + 2, BL_SH = BL_TH + 2;
 
+// Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
+__host__ __device__ constexpr int pat(int l, int k) {
+    return l == 0   ? (k == 0 ? 0 : k == 3 ? 2 : 1)
+           : l == 1 ? (k == 0 ? 2 : k == 3 ? 0 : 1)
+           : l == 2 ? (k == 1 ? 0 : k == 2 ? 2 : 1)
+                    : (k == 1 ? 2 : k == 2 ? 0 : 1);
+}
+
+// Interior tiles of RawEngine.cpp:299-344: every 3x3 neighbourhood is present,
+// so each colour's neighbours and their row-major order are fixed by the
+// quad position -- four edge neighbours (N, W, E, S) or four diagonals at R/B
+// sites, a horizontal or vertical pair at G sites -- and the division by the
+// count (4 or 2, a power of two) is an exact multiply.
+template <int L>
+__device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0, int y0, int ox, int oy,
+                                              int ow, int oh, int stage_end, const DevProgram& P,
+                                              const SmemCurveSet* sc, float* __restrict__ out,
+                                              size_t out_stride, uint32_t& err) {
+    for (int q = threadIdx.x; q < (BL_TW / 2) * (BL_TH / 2); q += BL_THREADS) {
+        const int qx = q % (BL_TW / 2), qy = q / (BL_TW / 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = k & 1, j = k >> 1;
+            const int tx = 2 * qx + i + 1, ty = 2 * qy + j + 1;
+            const int x = x0 + tx - 1, y = y0 + ty - 1;
+            const int own = pat(L, k);
+            float rgb[3];
+            rgb[own] = tile[ty][tx];
+            if (own == 1) {
+                const int row_colour = pat(L, (j << 1) | (i ^ 1));       // colour of the W/E neighbours
+                const float hsum = __fadd_rn(tile[ty][tx - 1], tile[ty][tx + 1]);
+                const float vsum = __fadd_rn(tile[ty - 1][tx], tile[ty + 1][tx]);
+                rgb[row_colour] = __fmul_rn(hsum, 0.5f);
+                rgb[2 - row_colour] = __fmul_rn(vsum, 0.5f);
+            } else {
+                const float edge = __fadd_rn(__fadd_rn(__fadd_rn(tile[ty - 1][tx], tile[ty][tx - 1]), tile[ty][tx + 1]),
+                                             tile[ty + 1][tx]);
+                const float diag = __fadd_rn(__fadd_rn(__fadd_rn(tile[ty - 1][tx - 1], tile[ty - 1][tx + 1]),
+                                                       tile[ty + 1][tx - 1]),
+                                             tile[ty + 1][tx + 1]);
+                rgb[1] = __fmul_rn(edge, 0.25f);
+                rgb[2 - own] = __fmul_rn(diag, 0.25f);
+            }
+            if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
+            apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err, sc);
+            float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+            o[0] = rgb[0];
+            o[1] = rgb[1];
+            o[2] = rgb[2];
+        }
+    }
+}
+
 // RawEngine.cpp:299-344.  The normalized samples of the tile and its one-pixel
 // halo are computed once into shared memory (positions outside the active area
 // are never read: the reference skips them and counts only present neighbours).
-__global__ void __launch_bounds__(BL_THREADS)
-bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int stage_end,
+// Tiles are anchored at even sensor coordinates; interior tiles take the quad
+// path, tiles meeting the active-area edge the general neighbour scan.
+__global__ void __launch_bounds__(BL_THREADS, 4)
+bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
     __shared__ float tile[BL_SH][BL_SW];
-    const int x0 = ox + blockIdx.x * BL_TW, y0 = oy + blockIdx.y * BL_TH;
+    __shared__ SmemCurveSet curves;
+    const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
     for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
         const int sx = i % BL_SW, sy = i / BL_SW;
         const int x = x0 - 1 + sx, y = y0 - 1 + sy;
@@ -36,12 +92,25 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
             v = normalize_sample(raw, x, y);
         tile[sy][sx] = v;
     }
+    const SmemCurveSet* sc = load_curves(P, &curves);
     __syncthreads();
     uint32_t err = 0;
+    const bool interior = x0 - 1 >= raw.ax && y0 - 1 >= raw.ay && x0 + BL_TW + 1 <= raw.ax + raw.aw &&
+                          y0 + BL_TH + 1 <= raw.ay + raw.ah;
+    if (interior) {
+        switch (layout) {
+        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        }
+        report(status, err);
+        return;
+    }
     for (int i = threadIdx.x; i < BL_TW * BL_TH; i += BL_THREADS) {
         const int tx = i % BL_TW, ty = i / BL_TW;
         const int x = x0 + tx, y = y0 + ty;
-        if (x >= ox + ow || y >= oy + oh) continue;
+        if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
         const int own = color_of(raw, x, y);
         float rgb[3];
 #pragma unroll
@@ -67,7 +136,7 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
             }
             rgb[ch] = count ? __fdiv_rn(sum, (float)count) : 0.0f;
         }
-        apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err);
+        apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err, sc);
         float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
         o[0] = rgb[0];
         o[1] = rgb[1];
@@ -268,13 +337,6 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
 // non-green sites, greens copied, every neighbour a single shared load.  The
 // arithmetic is the reference's, in binary64, in the reference's order.
 
-// Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
-__host__ __device__ constexpr int pat(int l, int k) {
-    return l == 0   ? (k == 0 ? 0 : k == 3 ? 2 : 1)
-           : l == 1 ? (k == 0 ? 2 : k == 3 ? 0 : 1)
-           : l == 2 ? (k == 1 ? 0 : k == 2 ? 2 : 1)
-                    : (k == 1 ? 2 : k == 2 ? 0 : 1);
-}
 constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, origin (-6,-6)
 constexpr int FC_W = MN_TW + 8, FC_H = MN_TH + 8;     // gh gv ch cv dh dv, origin (-4,-4)
 constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, origin (-2,-2)
@@ -298,7 +360,8 @@ __device__ __forceinline__ double half_sum(double a, double b) { return __dmul_r
 template <int L>
 __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
                                            int ow, int oh, int stage_end, const DevProgram& P,
-                                           float* __restrict__ out, size_t out_stride, uint32_t& err) {
+                                           const SmemCurveSet* sc, float* __restrict__ out, size_t out_stride,
+                                           uint32_t& err) {
     const int t = threadIdx.x;
     // 1. normalized raw (RawEngine.cpp:89-97) as binary64, r = 6 around the tile
     for (int i = t; i < FR_W * FR_H; i += MN_THREADS) {
@@ -420,7 +483,7 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
             if (own == 0) bb = dsub(dadd(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
             float r = (float)rr, g = (float)S.green[pg], b = (float)bb;
             if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
-            apply_stages(P, 0, stage_end, r, g, b, err);
+            apply_stages(P, 0, stage_end, r, g, b, err, sc);
             float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
             o[0] = r;
             o[1] = g;
@@ -433,6 +496,7 @@ union MenonShared {
     MenonSmem generic;
     FastSmem fast;
 };
+constexpr size_t kCurveOffset = (sizeof(MenonShared) + 15) & ~size_t(15);
 
 // One CTA per MN_TW x MN_TH tile of the viewport, tiles anchored at an even
 // sensor coordinate.  Interior tiles take the fast quad path; tiles whose
@@ -446,15 +510,16 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
     const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
     const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
     uint32_t err = 0;
+    const SmemCurveSet* sc = load_curves(P, reinterpret_cast<SmemCurveSet*>(smem_raw + kCurveOffset));
     const bool interior = !ties && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay && x0 + MN_TW + 6 <= raw.ax + raw.aw &&
                           y0 + MN_TH + 6 <= raw.ay + raw.ah;
     if (interior) {
         FastSmem& F = reinterpret_cast<MenonShared*>(smem_raw)->fast;
         switch (layout) {
-        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
         }
         report(status, err);
         return;
@@ -484,7 +549,7 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
             bb = __dadd_rn(__dadd_rn(rr, pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy)),
                            -pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy));
         float r = (float)rr, g = (float)S.green[ty + 2][tx + 2], b = (float)bb;
-        apply_stages(P, 0, stage_end, r, g, b, err);
+        apply_stages(P, 0, stage_end, r, g, b, err, sc);
         float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
         o[0] = r;
         o[1] = g;
@@ -502,6 +567,8 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
                                   size_t native_stride, int scale, int ow, int oh, int stage_begin,
                                   int stage_end, const __grid_constant__ DevProgram P,
                                   float* __restrict__ out, size_t out_stride, uint32_t* status) {
+    __shared__ SmemCurveSet curves;
+    const SmemCurveSet* sc = load_curves(P, &curves);
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= ow || y >= oh) return;
@@ -519,7 +586,7 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
     const double n = (double)count;
     float r = (float)__ddiv_rn(s0, n), g = (float)__ddiv_rn(s1, n), b = (float)__ddiv_rn(s2, n);
     uint32_t err = 0;
-    apply_stages(P, stage_begin, stage_end, r, g, b, err);
+    apply_stages(P, stage_begin, stage_end, r, g, b, err, sc);
     float* o = out + (size_t)y * out_stride + (size_t)x * 3;
     o[0] = r;
     o[1] = g;
@@ -550,17 +617,17 @@ cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy
     if (ow <= 0 || oh <= 0) return cudaSuccess;
     // Menon with a singleton active-area axis is bilinear (RawEngine.cpp:303).
     if (demosaic == 1 && raw.aw > 1 && raw.ah > 1) {
-        cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(MenonShared));
+        const size_t smem = kCurveOffset + sizeof(SmemCurveSet);
+        cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const int gx0 = ox & ~1, gy0 = oy & ~1;
         dim3 grid((ox + ow - gx0 + MN_TW - 1) / MN_TW, (oy + oh - gy0 + MN_TH - 1) / MN_TH);
-        menon_kernel<<<grid, MN_THREADS, sizeof(MenonShared), stream>>>(raw, ox, oy, ow, oh, quad_layout(raw),
-                                                                         stage_end, P, out, out_stride, status,
-                                                                         ties);
+        menon_kernel<<<grid, MN_THREADS, smem, stream>>>(raw, ox, oy, ow, oh, quad_layout(raw), stage_end, P, out,
+                                                         out_stride, status, ties);
     } else {
-        dim3 grid((ow + BL_TW - 1) / BL_TW, (oh + BL_TH - 1) / BL_TH);
-        bilinear_kernel<<<grid, BL_THREADS, 0, stream>>>(raw, ox, oy, ow, oh, stage_end, P, out,
+        const int gx0 = ox & ~1, gy0 = oy & ~1;
+        dim3 grid((ox + ow - gx0 + BL_TW - 1) / BL_TW, (oy + oh - gy0 + BL_TH - 1) / BL_TH);
+        bilinear_kernel<<<grid, BL_THREADS, 0, stream>>>(raw, ox, oy, ow, oh, quad_layout(raw), stage_end, P, out,
                                                          out_stride, status);
     }
     if (launches) ++*launches;
