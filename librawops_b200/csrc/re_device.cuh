@@ -105,9 +105,9 @@ struct DevCurveSet {
 // Shared-memory copy of a curve set whose curves have at most SC_MAX knots
 // (each CTA loads it once; the per-sample segment search then reads only
 // shared memory).
-constexpr int SC_MAX = 64;
+constexpr int SC_MAX = 32;
 struct SmemCurve {
-    uint32_t n, identity, cubic, pad;
+    uint32_t n, identity, cubic, pad;    // pad: largest power of two <= n (search span)
     float xf[SC_MAX];
     float xeq[SC_MAX];
     float xn[SC_MAX];

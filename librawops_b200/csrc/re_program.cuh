@@ -39,6 +39,43 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
     return k.x + t * (k.y + t * (k.z + t * k.w));
 }
 
+// Three samples through one shared-memory curve at once: a fixed-length,
+// branch-free upper_bound (binary lifting over the RU-rounded knots) so that
+// the three searches interleave instead of chaining their loads.
+__device__ __forceinline__ void curve_map3(const SmemCurve* __restrict__ c, float v[3]) {
+    if (c->identity) return;
+    const int n = (int)c->n;
+    int lo[3] = {0, 0, 0};
+    for (int step = (int)c->pad; step > 0; step >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int cand = lo[k] + step;
+            if (cand <= n && v[k] >= c->xf[cand - 1]) lo[k] = cand;
+        }
+    }
+    const float xl = c->xf[n - 1], x0 = c->xf[0];
+    const bool tail_nan = isnan(c->xeq[n - 1]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int left = lo[k] == 0 ? 0 : lo[k] - 1;
+        const int seg = left < n - 2 ? left : n - 2;
+        const float x = v[k];
+        float r;
+        if (x == c->xeq[left]) {
+            r = c->y[left];
+        } else if (!c->cubic || x < x0 || x > xl || (x == xl && tail_nan)) {
+            const float s = c->slope[seg];
+            const float yl = c->y[left];
+            r = s == 0.0f ? yl : yl + (x - c->xn[left]) * s;
+        } else {
+            const float t = (x - c->xn[seg]) * c->inv_h[seg];
+            const float4 kf = c->coef[seg];
+            r = kf.x + t * (kf.y + t * (kf.z + t * kf.w));
+        }
+        v[k] = r;
+    }
+}
+
 // Loads curve set 0 of P into shared memory when every curve fits; returns it
 // (or null, in which case curves are read from global memory).  All threads
 // of the block must call it; it ends with a barrier.
@@ -56,6 +93,9 @@ __device__ __forceinline__ const SmemCurveSet* load_curves(const DevProgram& P, 
             dst.n = src.n;
             dst.identity = src.identity;
             dst.cubic = src.cubic;
+            uint32_t p2 = 1;                    // largest power of two <= n (search span)
+            while (p2 * 2 <= src.n) p2 *= 2;
+            dst.pad = p2;
         }
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             dst.xf[i] = src.xf[i];
@@ -141,14 +181,17 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
         case RE_STAGE_CURVES: {
             bool bad = !(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]));
             if (sc && st.arg == 0) {
+                curve_map3(&sc->c[0], v);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
+                    if (!isfinite(v[c])) bad = true;
                     const SmemCurve* ch = &sc->c[c + 1];
-                    if (sc->c[0].identity && ch->identity) continue;
-                    const float master = curve_map(&sc->c[0], v[c]);
-                    const float mapped = curve_map(ch, master);
-                    if (!isfinite(master) || !isfinite(mapped)) bad = true;
-                    v[c] = mapped;
+                    if (!ch->identity) {
+                        float one[3] = {v[c], v[c], v[c]};
+                        curve_map3(ch, one);
+                        v[c] = one[0];
+                    }
+                    if (!isfinite(v[c])) bad = true;
                 }
             } else {
                 const DevCurveSet* cs = P.curves[st.arg];

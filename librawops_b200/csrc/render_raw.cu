@@ -337,108 +337,135 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
 // non-green sites, greens copied, every neighbour a single shared load.  The
 // arithmetic is the reference's, in binary64, in the reference's order.
 
-constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, origin (-6,-6)
-constexpr int FC_W = MN_TW + 8, FC_H = MN_TH + 8;     // gh gv ch cv dh dv, origin (-4,-4)
-constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, origin (-2,-2)
+constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, full resolution, origin (-6,-6)
+constexpr int QW = (MN_TW + 8) / 2, QH = (MN_TH + 8) / 2;  // quad grid of the r=4 planes, origin (-4,-4)
+constexpr int QN = QW * QH;
+constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, full resolution, origin (-2,-2)
+
+// The two non-green sites of a quad: A in the quad's first row at column
+// ax(L), B in its second row at column 1 - ax(L).  Chroma-stage planes keep
+// one value per quad and class (consecutive quads are consecutive doubles, so
+// a warp's accesses are bank-conflict free), halving their footprint.
+__host__ __device__ constexpr int ng_col(int l) { return l < 2 ? 0 : 1; }
+
+enum { GH_A, GH_B, GV_A, GV_B, CH_A, CH_B, CV_A, CV_B, DH_A, DH_B, DV_A, DV_B, NG_PLANES };
 
 struct FastSmem {
     double raw[FR_H * FR_W];
-    double gh[FC_H * FC_W];
-    double gv[FC_H * FC_W];
-    double ch[FC_H * FC_W];      // reused as red after the gradients
-    double cv[FC_H * FC_W];      // reused as blue after the gradients
-    double dh[FC_H * FC_W];
-    double dv[FC_H * FC_W];
+    double ng[NG_PLANES][QN];        // red and blue reuse planes 0..5 in the last stages
     double green[FG_H * FG_W];
     uint8_t horiz[FG_H * FG_W];
 };
+static_assert(2 * FG_W * FG_H <= 6 * QN, "red/blue must fit in the dead chroma planes");
 
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double half_sum(double a, double b) { return __dmul_rn(0.5, __dadd_rn(a, b)); }
+
+// MenonDemosaic.cpp:112-115 five-tap directional green at raw index r (stride d).
+__device__ __forceinline__ double five(const double* r, int d) {
+    return dsub(dadd(half_sum(r[-d], r[d]), __dmul_rn(0.5, r[0])), __dmul_rn(0.25, dadd(r[-2 * d], r[2 * d])));
+}
 
 template <int L>
 __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
                                            int ow, int oh, int stage_end, const DevProgram& P,
                                            const SmemCurveSet* sc, float* __restrict__ out, size_t out_stride,
                                            uint32_t& err) {
+    constexpr int AX = ng_col(L), BX = 1 - AX;
     const int t = threadIdx.x;
     // 1. normalized raw (RawEngine.cpp:89-97) as binary64, r = 6 around the tile
+#pragma unroll 4
     for (int i = t; i < FR_W * FR_H; i += MN_THREADS) {
         const int sx = i % FR_W, sy = i / FR_W;
         S.raw[i] = (double)normalize_sample(raw, x0 - 6 + sx, y0 - 6 + sy);
     }
     __syncthreads();
-    // 2. directional green and chroma at non-green sites (MenonDemosaic.cpp:107-119)
-    for (int q = t; q < (FC_W / 2) * (FC_H / 2); q += MN_THREADS) {
-        const int qx = q % (FC_W / 2), qy = q / (FC_W / 2);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = k & 1, j = k >> 1;
-            if (pat(L, k) == 1) continue;
-            const int pc = (2 * qy + j) * FC_W + 2 * qx + i;
-            const int pr = (2 * qy + j + 2) * FR_W + 2 * qx + i + 2;
-            const double* r = S.raw + pr;
-            const double own = r[0];
-            const double h = dsub(dadd(half_sum(r[-1], r[1]), __dmul_rn(0.5, own)),
-                                  __dmul_rn(0.25, dadd(r[-2], r[2])));
-            const double v = dsub(dadd(half_sum(r[-FR_W], r[FR_W]), __dmul_rn(0.5, own)),
-                                  __dmul_rn(0.25, dadd(r[-2 * FR_W], r[2 * FR_W])));
-            S.gh[pc] = h;
-            S.gv[pc] = v;
-            S.ch[pc] = dsub(own, h);
-            S.cv[pc] = dsub(own, v);
+    // 2. directional green and chroma at the two non-green sites of every quad
+    //    of the r=4 region (MenonDemosaic.cpp:107-119)
+#pragma unroll 2
+    for (int q = t; q < QN; q += MN_THREADS) {
+        const int qx = q % QW, qy = q / QW;
+        const double* ra = S.raw + (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
+        const double* rb = S.raw + (2 * qy + 3) * FR_W + 2 * qx + BX + 2;
+        const double ha = five(ra, 1), va = five(ra, FR_W);
+        const double hb = five(rb, 1), vb = five(rb, FR_W);
+        S.ng[GH_A][q] = ha;
+        S.ng[GV_A][q] = va;
+        S.ng[CH_A][q] = dsub(ra[0], ha);
+        S.ng[CV_A][q] = dsub(ra[0], va);
+        S.ng[GH_B][q] = hb;
+        S.ng[GV_B][q] = vb;
+        S.ng[CH_B][q] = dsub(rb[0], hb);
+        S.ng[CV_B][q] = dsub(rb[0], vb);
+    }
+    __syncthreads();
+    // 3. forward chroma gradients (MenonDemosaic.cpp:120-125): the same-class
+    //    neighbour two pixels right is the next quad, two pixels down the next row
+#pragma unroll 2
+    for (int q = t; q < QN; q += MN_THREADS) {
+        const int qx = q % QW, qy = q / QW;
+        if (qx < QW - 1) {
+            S.ng[DH_A][q] = fabs(dsub(S.ng[CH_A][q], S.ng[CH_A][q + 1]));
+            S.ng[DH_B][q] = fabs(dsub(S.ng[CH_B][q], S.ng[CH_B][q + 1]));
+        }
+        if (qy < QH - 1) {
+            S.ng[DV_A][q] = fabs(dsub(S.ng[CV_A][q], S.ng[CV_A][q + QW]));
+            S.ng[DV_B][q] = fabs(dsub(S.ng[CV_B][q], S.ng[CV_B][q + QW]));
         }
     }
     __syncthreads();
-    // 3. forward chroma gradients at non-green sites (MenonDemosaic.cpp:120-125)
-    for (int q = t; q < (FC_W / 2) * (FC_H / 2); q += MN_THREADS) {
-        const int qx = q % (FC_W / 2), qy = q / (FC_W / 2);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = k & 1, j = k >> 1;
-            if (pat(L, k) == 1) continue;
-            const int x = 2 * qx + i, y = 2 * qy + j;
-            const int p = y * FC_W + x;
-            if (x < FC_W - 2) S.dh[p] = fabs(dsub(S.ch[p], S.ch[p + 2]));
-            if (y < FC_H - 2) S.dv[p] = fabs(dsub(S.cv[p], S.cv[p + 2 * FC_W]));
-        }
-    }
-    __syncthreads();
-    // 4. classifier and green (MenonDemosaic.cpp:130-147), terms in reference order
-    for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
-        const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = k & 1, j = k >> 1;
-            const int gx = 2 * qx + i, gy = 2 * qy + j;
-            const int pg = gy * FG_W + gx;
-            if (pat(L, k) == 1) {
-                S.green[pg] = S.raw[(gy + 4) * FR_W + gx + 4];
-                S.horiz[pg] = 1;
-                continue;
-            }
-            const int p = (gy + 2) * FC_W + gx + 2;
-            const double* dh = S.dh + p;
-            const double* dv = S.dv + p;
-            double h = 0.0, v = 0.0;
-            h = dadd(h, dh[2 * FC_W]);                       v = dadd(v, dv[2]);
-            h = dadd(h, dh[2 * FC_W - 2]);                   v = dadd(v, dv[-2 * FC_W + 2]);
-            h = dadd(h, dh[FC_W - 1]);                       v = dadd(v, dv[-FC_W + 1]);
-            h = dadd(h, __dmul_rn(3.0, dh[0]));              v = dadd(v, __dmul_rn(3.0, dv[0]));
-            h = dadd(h, __dmul_rn(3.0, dh[-2]));             v = dadd(v, __dmul_rn(3.0, dv[-2 * FC_W]));
-            h = dadd(h, dh[-FC_W - 1]);                      v = dadd(v, dv[-FC_W - 1]);
-            h = dadd(h, dh[-2 * FC_W]);                      v = dadd(v, dv[-2]);
-            h = dadd(h, dh[-2 * FC_W - 2]);                  v = dadd(v, dv[-2 * FC_W - 2]);
-            const bool horizontal = v >= h;
-            S.horiz[pg] = horizontal;
-            S.green[pg] = horizontal ? S.gh[p] : S.gv[p];
-        }
+    // 4. classifier and green (MenonDemosaic.cpp:130-147) for the quads of the r=2
+    //    region, terms in the reference's order; (-1,+-1) offsets land on the other class
+#pragma unroll 2
+    for (int k = t; k < (QW - 2) * (QH - 2); k += MN_THREADS) {
+        const int qx = k % (QW - 2) + 1, qy = k / (QW - 2) + 1;
+        const int q = qy * QW + qx;
+        const double* dhA = S.ng[DH_A];
+        const double* dhB = S.ng[DH_B];
+        const double* dvA = S.ng[DV_A];
+        const double* dvB = S.ng[DV_B];
+        // A site: other-class (B) quads at column offsets -(1-AX) / +AX
+        double h = 0.0, v = 0.0;
+        h = dadd(h, dhA[q + QW]);                 v = dadd(v, dvA[q + 1]);
+        h = dadd(h, dhA[q + QW - 1]);             v = dadd(v, dvA[q - QW + 1]);
+        h = dadd(h, dhB[q - BX]);                 v = dadd(v, dvB[q - QW + AX]);
+        h = dadd(h, __dmul_rn(3.0, dhA[q]));      v = dadd(v, __dmul_rn(3.0, dvA[q]));
+        h = dadd(h, __dmul_rn(3.0, dhA[q - 1]));  v = dadd(v, __dmul_rn(3.0, dvA[q - QW]));
+        h = dadd(h, dhB[q - QW - BX]);            v = dadd(v, dvB[q - QW - BX]);
+        h = dadd(h, dhA[q - QW]);                 v = dadd(v, dvA[q - 1]);
+        h = dadd(h, dhA[q - QW - 1]);             v = dadd(v, dvA[q - QW - 1]);
+        const bool hzA = v >= h;
+        // B site: other-class (A) quads at column offsets -AX / +(1-AX)
+        h = 0.0; v = 0.0;
+        h = dadd(h, dhB[q + QW]);                 v = dadd(v, dvB[q + 1]);
+        h = dadd(h, dhB[q + QW - 1]);             v = dadd(v, dvB[q - QW + 1]);
+        h = dadd(h, dhA[q + QW - AX]);            v = dadd(v, dvA[q + BX]);
+        h = dadd(h, __dmul_rn(3.0, dhB[q]));      v = dadd(v, __dmul_rn(3.0, dvB[q]));
+        h = dadd(h, __dmul_rn(3.0, dhB[q - 1]));  v = dadd(v, __dmul_rn(3.0, dvB[q - QW]));
+        h = dadd(h, dhA[q - AX]);                 v = dadd(v, dvA[q - AX]);
+        h = dadd(h, dhB[q - QW]);                 v = dadd(v, dvB[q - 1]);
+        h = dadd(h, dhB[q - QW - 1]);             v = dadd(v, dvB[q - QW - 1]);
+        const bool hzB = v >= h;
+        // full-resolution green/direction on the r=2 grid (origin -2)
+        const int ga = (2 * qy - 2) * FG_W + 2 * qx - 2 + AX;          // A site
+        const int gb = (2 * qy - 1) * FG_W + 2 * qx - 2 + BX;          // B site
+        const int g0 = (2 * qy - 2) * FG_W + 2 * qx - 2 + BX;          // green in row 0
+        const int g1 = (2 * qy - 1) * FG_W + 2 * qx - 2 + AX;          // green in row 1
+        S.horiz[ga] = hzA;
+        S.horiz[gb] = hzB;
+        S.horiz[g0] = 1;
+        S.horiz[g1] = 1;
+        S.green[ga] = hzA ? S.ng[GH_A][q] : S.ng[GV_A][q];
+        S.green[gb] = hzB ? S.ng[GH_B][q] : S.ng[GV_B][q];
+        S.green[g0] = S.raw[(2 * qy + 2) * FR_W + 2 * qx + 2 + BX];
+        S.green[g1] = S.raw[(2 * qy + 3) * FR_W + 2 * qx + 2 + AX];
     }
     __syncthreads();
     // 5. red and blue on the r=1 ring (MenonDemosaic.cpp:151-161); chroma planes are dead
-    double* red = S.ch;
-    double* blue = S.cv;
+    double* red = S.ng[0];
+    double* blue = S.ng[0] + FG_W * FG_H;
+#pragma unroll 2
     for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
         const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
 #pragma unroll
@@ -453,10 +480,9 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
             if (own == 0) rr = S.raw[pr];
             if (own == 2) bb = S.raw[pr];
             if (own == 1) {
-                // colour of the horizontal neighbour (same row, other column of the quad)
-                const bool red_h = pat(L, (j << 1) | (i ^ 1)) == 0;
-                const int dr = red_h ? 1 : FR_W, dg = red_h ? 1 : FG_W;      // red axis
-                const int br = red_h ? FR_W : 1, bg = red_h ? FG_W : 1;      // blue axis
+                const bool red_h = pat(L, (j << 1) | (i ^ 1)) == 0;   // colour of the row's non-green
+                const int dr = red_h ? 1 : FR_W, dg = red_h ? 1 : FG_W;
+                const int br = red_h ? FR_W : 1, bg = red_h ? FG_W : 1;
                 const double g = S.green[pg];
                 rr = dsub(dadd(g, half_sum(S.raw[pr - dr], S.raw[pr + dr])),
                           half_sum(S.green[pg - dg], S.green[pg + dg]));

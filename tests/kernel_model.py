@@ -186,68 +186,79 @@ def model_render(meta, samples, viewport, fast=True):
 
 
 def _fast_tile(meta, sample, color, x0, y0, viewport, out):
-    """The interior quad path (menon_fast in render_raw.cu): flat planes with the
-    kernel's strides, colours from the even-origin quad layout."""
+    """The interior quad path (menon_fast in render_raw.cu): class-packed chroma
+    planes on the quad grid, full-resolution green/red/blue, the kernel's strides
+    and neighbour offsets."""
     ox, oy, ow, oh = viewport
-    RW, RH, CW, CH, GW, GH = TW + 12, TH + 12, TW + 8, TH + 8, TW + 4, TH + 4
+    RW, RH, GW, GH = TW + 12, TH + 12, TW + 4, TH + 4
+    QW, QH = (TW + 8) // 2, (TH + 8) // 2
+    QN = QW * QH
     lay = [color(x0 + (k & 1), y0 + (k >> 1)) for k in range(4)]
+    AX = 0 if lay[0] != 1 else 1          # column of the first row's non-green
+    BX = 1 - AX
 
     def flat(n):
         return Plane(n, 1, 0, 0)
 
-    raw, gh, gv, ch, cv, dh, dv = flat(RW * RH), flat(CW * CH), flat(CW * CH), flat(CW * CH), \
-        flat(CW * CH), flat(CW * CH), flat(CW * CH)
+    raw = flat(RW * RH)
+    ng = {name: flat(QN) for name in ("ghA", "ghB", "gvA", "gvB", "chA", "chB", "cvA", "cvB",
+                                      "dhA", "dhB", "dvA", "dvB")}
     green, horiz = flat(GW * GH), flat(GW * GH)
     for i in range(RW * RH):
         raw.set(i, 0, sample(x0 - 6 + i % RW, y0 - 6 + i // RW))
     half = lambda a, b: 0.5 * (a + b)
-    for q in range((CW // 2) * (CH // 2)):
-        qx, qy = q % (CW // 2), q // (CW // 2)
-        for k in range(4):
-            i, j = k & 1, k >> 1
-            if lay[k] == 1:
-                continue
-            pc = (2 * qy + j) * CW + 2 * qx + i
-            pr = (2 * qy + j + 2) * RW + 2 * qx + i + 2
-            r = lambda o: raw.get(pr + o, 0)
-            own = r(0)
-            h = (half(r(-1), r(1)) + 0.5 * own) - 0.25 * (r(-2) + r(2))
-            v = (half(r(-RW), r(RW)) + 0.5 * own) - 0.25 * (r(-2 * RW) + r(2 * RW))
-            gh.set(pc, 0, h); gv.set(pc, 0, v); ch.set(pc, 0, own - h); cv.set(pc, 0, own - v)
-    for q in range((CW // 2) * (CH // 2)):
-        qx, qy = q % (CW // 2), q // (CW // 2)
-        for k in range(4):
-            i, j = k & 1, k >> 1
-            if lay[k] == 1:
-                continue
-            x, y = 2 * qx + i, 2 * qy + j
-            p = y * CW + x
-            if x < CW - 2:
-                dh.set(p, 0, abs(ch.get(p, 0) - ch.get(p + 2, 0)))
-            if y < CH - 2:
-                dv.set(p, 0, abs(cv.get(p, 0) - cv.get(p + 2 * CW, 0)))
-    for q in range((GW // 2) * (GH // 2)):
-        qx, qy = q % (GW // 2), q // (GW // 2)
-        for k in range(4):
-            i, j = k & 1, k >> 1
-            gx, gy = 2 * qx + i, 2 * qy + j
-            pg = gy * GW + gx
-            if lay[k] == 1:
-                green.set(pg, 0, raw.get((gy + 4) * RW + gx + 4, 0)); horiz.set(pg, 0, 1.0)
-                continue
-            p = (gy + 2) * CW + gx + 2
-            H = lambda o: dh.get(p + o, 0)
-            V = lambda o: dv.get(p + o, 0)
+    R = lambda i: raw.get(i, 0)
+
+    def five(i, d):
+        return (half(R(i - d), R(i + d)) + 0.5 * R(i)) - 0.25 * (R(i - 2 * d) + R(i + 2 * d))
+
+    for q in range(QN):
+        qx, qy = q % QW, q // QW
+        ra = (2 * qy + 2) * RW + 2 * qx + AX + 2
+        rb = (2 * qy + 3) * RW + 2 * qx + BX + 2
+        ha, va, hb, vb = five(ra, 1), five(ra, RW), five(rb, 1), five(rb, RW)
+        ng["ghA"].set(q, 0, ha); ng["gvA"].set(q, 0, va)
+        ng["chA"].set(q, 0, R(ra) - ha); ng["cvA"].set(q, 0, R(ra) - va)
+        ng["ghB"].set(q, 0, hb); ng["gvB"].set(q, 0, vb)
+        ng["chB"].set(q, 0, R(rb) - hb); ng["cvB"].set(q, 0, R(rb) - vb)
+    G = lambda name, i: ng[name].get(i, 0)
+    for q in range(QN):
+        qx, qy = q % QW, q // QW
+        if qx < QW - 1:
+            ng["dhA"].set(q, 0, abs(G("chA", q) - G("chA", q + 1)))
+            ng["dhB"].set(q, 0, abs(G("chB", q) - G("chB", q + 1)))
+        if qy < QH - 1:
+            ng["dvA"].set(q, 0, abs(G("cvA", q) - G("cvA", q + QW)))
+            ng["dvB"].set(q, 0, abs(G("cvB", q) - G("cvB", q + QW)))
+    for k in range((QW - 2) * (QH - 2)):
+        qx, qy = k % (QW - 2) + 1, k // (QW - 2) + 1
+        q = qy * QW + qx
+        termsA = [(("dhA", q + QW), ("dvA", q + 1), 1), (("dhA", q + QW - 1), ("dvA", q - QW + 1), 1),
+                  (("dhB", q - BX), ("dvB", q - QW + AX), 1), (("dhA", q), ("dvA", q), 3),
+                  (("dhA", q - 1), ("dvA", q - QW), 3), (("dhB", q - QW - BX), ("dvB", q - QW - BX), 1),
+                  (("dhA", q - QW), ("dvA", q - 1), 1), (("dhA", q - QW - 1), ("dvA", q - QW - 1), 1)]
+        termsB = [(("dhB", q + QW), ("dvB", q + 1), 1), (("dhB", q + QW - 1), ("dvB", q - QW + 1), 1),
+                  (("dhA", q + QW - AX), ("dvA", q + BX), 1), (("dhB", q), ("dvB", q), 3),
+                  (("dhB", q - 1), ("dvB", q - QW), 3), (("dhA", q - AX), ("dvA", q - AX), 1),
+                  (("dhB", q - QW), ("dvB", q - 1), 1), (("dhB", q - QW - 1), ("dvB", q - QW - 1), 1)]
+        hz = []
+        for terms in (termsA, termsB):
             h = v = 0.0
-            for oh_, ov_, w in ((2 * CW, 2, 1), (2 * CW - 2, -2 * CW + 2, 1), (CW - 1, -CW + 1, 1),
-                                (0, 0, 3), (-2, -2 * CW, 3), (-CW - 1, -CW - 1, 1), (-2 * CW, -2, 1),
-                                (-2 * CW - 2, -2 * CW - 2, 1)):
-                h += w * H(oh_)
-                v += w * V(ov_)
-            hz = v >= h
-            horiz.set(pg, 0, 1.0 if hz else 0.0)
-            green.set(pg, 0, gh.get(p, 0) if hz else gv.get(p, 0))
-    red, blue = flat(CW * CH), flat(CW * CH)
+            for (hn, hi), (vn, vi), w in terms:
+                h += w * G(hn, hi)
+                v += w * G(vn, vi)
+            hz.append(v >= h)
+        ga = (2 * qy - 2) * GW + 2 * qx - 2 + AX
+        gb = (2 * qy - 1) * GW + 2 * qx - 2 + BX
+        g0 = (2 * qy - 2) * GW + 2 * qx - 2 + BX
+        g1 = (2 * qy - 1) * GW + 2 * qx - 2 + AX
+        horiz.set(ga, 0, float(hz[0])); horiz.set(gb, 0, float(hz[1]))
+        horiz.set(g0, 0, 1.0); horiz.set(g1, 0, 1.0)
+        green.set(ga, 0, G("ghA", q) if hz[0] else G("gvA", q))
+        green.set(gb, 0, G("ghB", q) if hz[1] else G("gvB", q))
+        green.set(g0, 0, R((2 * qy + 2) * RW + 2 * qx + 2 + BX))
+        green.set(g1, 0, R((2 * qy + 3) * RW + 2 * qx + 2 + AX))
+    red, blue = flat(GW * GH), flat(GW * GH)
     for q in range((GW // 2) * (GH // 2)):
         qx, qy = q % (GW // 2), q // (GW // 2)
         for k in range(4):
@@ -259,16 +270,16 @@ def _fast_tile(meta, sample, color, x0, y0, viewport, out):
             pr = (gy + 4) * RW + gx + 4
             rr = bb = 0.0
             if lay[k] == 0:
-                rr = raw.get(pr, 0)
+                rr = R(pr)
             if lay[k] == 2:
-                bb = raw.get(pr, 0)
+                bb = R(pr)
             if lay[k] == 1:
                 red_h = lay[(j << 1) | (i ^ 1)] == 0
                 dr, dg = (1, 1) if red_h else (RW, GW)
                 br, bg = (RW, GW) if red_h else (1, 1)
                 g = green.get(pg, 0)
-                rr = (g + half(raw.get(pr - dr, 0), raw.get(pr + dr, 0))) - half(green.get(pg - dg, 0), green.get(pg + dg, 0))
-                bb = (g + half(raw.get(pr - br, 0), raw.get(pr + br, 0))) - half(green.get(pg - bg, 0), green.get(pg + bg, 0))
+                rr = (g + half(R(pr - dr), R(pr + dr))) - half(green.get(pg - dg, 0), green.get(pg + dg, 0))
+                bb = (g + half(R(pr - br), R(pr + br))) - half(green.get(pg - bg, 0), green.get(pg + bg, 0))
             red.set(pg, 0, rr); blue.set(pg, 0, bb)
     for q in range((TW // 2) * (TH // 2)):
         qx, qy = q % (TW // 2), q // (TW // 2)
