@@ -207,6 +207,24 @@ RE_API size_t re_render_scratch_bytes(const re_image* image, const re_render_des
                                       re_rect viewport, uint32_t mip);
 RE_API re_status re_status_from_device(uint32_t device_status_word);
 
+/* Reduced-level (mip 1 or 2, Preview) RAW render that allocates no memory.
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory while rendering -- a plug-in inside a host application whose
+ * device memory is budgeted up front, or a real-time preview thread that must
+ * not take allocator locks or risk running out of memory mid-frame.  Output
+ * goes to caller DEVICE memory (`out`, row stride in floats); the native
+ * footprint is staged in a fixed device array of
+ * re_render_raw_reduced_noalloc_max_native_pixels() pixels (12 MiB, held on
+ * every GPU that loads the library until exit).  Larger footprints return
+ * RE_LENGTH_ERROR.  All calls share that array: calls that overlap on the GPU
+ * race, so order them on one stream or serialize them.  The first call on a
+ * device looks up the array's address with that device current; make it
+ * before any stream capture.  Returns after the render completed on `stream`. */
+RE_API re_status re_render_raw_reduced_noalloc(const re_image* image, const re_render_desc* desc,
+                                               re_rect viewport, uint32_t mip, float* out,
+                                               size_t out_row_stride, void* stream);
+RE_API size_t re_render_raw_reduced_noalloc_max_native_pixels(void);
+
 /* Renderer::render_tiles (RawEngine.cpp:1390-1412): the reference's per-tile
  * loop, one fused launch per tile, each tile copied to the host callback in
  * tile order.  The callback may return nonzero to cancel (RE_CANCELLED). */

@@ -29,6 +29,7 @@ EXPORTS = [
     "re_render_raw", "re_render_raw_async", "re_render_scratch_bytes", "re_status_from_device",
     "re_render_tiles", "re_guided_filter", "re_local_statistics", "re_cubic_resize", "re_rotate",
     "re_cubic_axis", "re_rotation_coefficients",
+    "re_render_raw_reduced_noalloc", "re_render_raw_reduced_noalloc_max_native_pixels",
 ]
 
 
@@ -116,6 +117,8 @@ def lib() -> C.CDLL:
         L.re_cubic_axis.argtypes = [u32, u32, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), f64p,
                                     C.POINTER(C.c_uint32)]
         L.re_rotation_coefficients.argtypes = [C.c_double, f64p, f64p]
+        L.re_render_raw_reduced_noalloc.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, vp, sz, vp]
+        L.re_render_raw_reduced_noalloc_max_native_pixels.restype = sz
         _lib = L
     return _lib
 

@@ -562,6 +562,24 @@ static re_status enqueue_render(const re_image* img, const DevProgram& P, uint32
     return RE_OK;
 }
 
+}  // extern "C"
+
+namespace re {
+// Planning shared with entry points defined in other translation units.
+re_status render_plan(const re_image* img, const re_render_desc* desc, re_rect viewport, uint32_t mip,
+                      uint32_t quality, DevProgram& P, re_rect& native, const DevRaw** raw) {
+    re_status s = build_program(desc, P);
+    if (s) return s;
+    s = plan_render(img, P, viewport, mip, quality, &native);
+    if (s) return s;
+    *raw = &img->raw;
+    return RE_OK;
+}
+re_status status_key_to_error(uint32_t key) { return status_from_key(key); }
+}  // namespace re
+
+extern "C" {
+
 re_status re_render_raw_async(const re_image* img, const re_render_desc* desc, re_rect viewport, uint32_t mip,
                               uint32_t quality, float* out, size_t out_stride, uint32_t* device_status,
                               void* scratch, void* stream) {
