@@ -27,7 +27,7 @@ EXPORTS = [
     "re_camera_to_working_matrix", "re_working_to_srgb_matrix", "re_working_to_working_matrix",
     "re_exposure_multiplier", "re_curve_set_create", "re_curve_set_destroy",
     "re_render_raw", "re_render_raw_async", "re_render_scratch_bytes", "re_status_from_device",
-    "re_render_tiles", "re_guided_filter", "re_local_statistics", "re_cubic_resize", "re_rotate",
+    "re_render_tiles", "re_render_raster", "re_guided_filter", "re_local_statistics", "re_cubic_resize", "re_rotate",
     "re_cubic_axis", "re_rotation_coefficients",
     "re_render_raw_reduced_noalloc", "re_render_raw_reduced_noalloc_max_native_pixels",
 ]
@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         L.re_render_scratch_bytes.restype = sz
         L.re_status_from_device.argtypes = [u32]
         L.re_render_tiles.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, u32, TILE_CALLBACK, vp, vp]
+        L.re_render_raster.argtypes = [vp, sz, u32, u32, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, vp]
         L.re_guided_filter.argtypes = [vp, sz, vp, sz, u32, u32, u32, C.c_double, u32, vp]
         L.re_local_statistics.argtypes = [vp, sz, u32, u32, u32, vp, vp, vp, vp]
         L.re_cubic_resize.argtypes = [vp, sz, u32, u32, u32, u32, Rect, u32, vp, sz, vp]

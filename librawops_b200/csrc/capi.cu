@@ -28,6 +28,9 @@ cudaError_t launch_mip_reduce(const float* native, int nw, int nh, size_t native
                               int ow, int oh, int stage_begin, int stage_end, const DevProgram& P,
                               float* out, size_t out_stride, uint32_t* status, cudaStream_t stream,
                               uint32_t* launches);
+cudaError_t launch_raster(const float* in, size_t in_stride, int width, int height, int ox, int oy, int ow, int oh,
+                          int mip, const DevProgram& P, float* out, size_t out_stride, uint32_t* status,
+                          cudaStream_t stream);
 }  // namespace re
 
 using namespace re;
@@ -488,13 +491,48 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
             d.xeq[i] = (double)rn == x[i] ? rn : NAN;
             d.y[i] = (float)y[i];
         }
+        double min_h = INFINITY;
         for (uint32_t i = 0; i + 1 < n; ++i) {
             const double h = x[i + 1] - x[i];
+            min_h = std::min(min_h, h);
             const double p0 = y[i] + (h * tangent[i]) / 3, p1 = y[i + 1] - (h * tangent[i + 1]) / 3;
             d.slope[i] = (float)slope[i];
             d.inv_h[i] = (float)(1.0 / h);
             d.coef[i] = make_float4((float)y[i], (float)(3 * (p0 - y[i])), (float)(3 * (y[i] - 2 * p0 + p1)),
                                     (float)(y[i + 1] - y[i] + 3 * (p0 - p1)));
+            // cell-lookup records: cubic segments in t = (v - x_i)/h, linear ones
+            // (and the extrapolations) as y_i + (v - x_i)*slope like ToneOps.cpp:826
+            if (interpolation) {
+                d.rec[i] = make_float4(d.xn[i], d.inv_h[i], d.xf[i + 1], 0.0f);
+                d.rcoef[i] = d.coef[i];
+            } else {
+                d.rec[i] = make_float4(d.xn[i], 1.0f, d.xf[i + 1], 0.0f);
+                d.rcoef[i] = make_float4(d.y[i], d.slope[i], 0.0f, 0.0f);
+            }
+        }
+        d.rec[n - 1] = make_float4(d.xn[n - 1], 1.0f, INFINITY, 0.0f);
+        d.rcoef[n - 1] = make_float4(d.y[n - 1], d.slope[n - 2], 0.0f, 0.0f);
+        d.rec[n] = make_float4(d.xn[0], 1.0f, d.xf[0], 0.0f);
+        d.rcoef[n] = make_float4(d.y[0], d.slope[0], 0.0f, 0.0f);
+        // Uniform cells at most half the narrowest segment wide: every cell
+        // names the segment one cell to its left (a safe lower start for the
+        // device's short forward walk).  Curves needing more than 4096 cells
+        // keep the binary search.
+        const double span = x[n - 1] - x[0];
+        const double cells = std::ceil(span / (0.5 * min_h));
+        d.ncells = 0;
+        if (cells >= 1 && cells <= 4096) {
+            const uint32_t nc = (uint32_t)cells;
+            const double dx = span / nc;
+            d.ncells = nc;
+            d.x0c = d.xn[0];
+            d.inv_dx = (float)(1.0 / dx);
+            for (uint32_t c = 0; c < nc; ++c) {
+                const double left = x[0] + (double(c) - 1.0) * dx;
+                uint32_t seg = 0;
+                while (seg + 2 < n && (double)d.xf[seg + 1] <= left) ++seg;
+                d.cell_seg[c] = (uint8_t)seg;
+            }
         }
     }
     cudaError_t e = cudaMalloc(&cs->dev, sizeof(DevCurveSet));
@@ -653,6 +691,35 @@ re_status re_render_raw(const re_image* img, const re_render_desc* desc, re_rect
         stats->launches = launches;
     }
     return status_from_key((uint32_t)head_host[0]);
+}
+
+// RasterSourceNode::render_level (RawEngine.cpp:346-406) + fused stages.
+re_status re_render_raster(const float* in, size_t in_stride, uint32_t width, uint32_t height,
+                           const re_render_desc* desc, re_rect viewport, uint32_t mip, uint32_t quality, float* out,
+                           size_t out_stride, void* stream_) {
+    DevProgram P;
+    re_status s = build_program(desc, P);
+    if (s) return s;
+    if (!width || !height) return fail(RE_INVALID_ARGUMENT, "invalid scene-linear raster metadata");
+    re_rect level;
+    s = re_request_bounds({0, 0, width, height}, mip, quality, &level);
+    if (s) return fail(RE_INVALID_ARGUMENT, "raster source does not support this render level");
+    if (!inside(level, viewport)) return fail(RE_OUT_OF_RANGE, "viewport is outside the active RAW area");
+    if (!viewport.width || !viewport.height) return RE_OK;
+    if (!in || !out || in_stride < (size_t)width * 3 || out_stride < (size_t)viewport.width * 3)
+        return fail(RE_INVALID_ARGUMENT, "invalid raster buffers");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    DeviceScratch scratch;
+    scratch.s = stream;
+    RE_CUDA(cudaMallocAsync(&scratch.p, 256, stream));
+    uint32_t* status = static_cast<uint32_t*>(scratch.p);
+    RE_CUDA(cudaMemsetAsync(status, 0, 4, stream));
+    RE_CUDA(launch_raster(in, in_stride, (int)width, (int)height, (int)viewport.x, (int)viewport.y,
+                          (int)viewport.width, (int)viewport.height, (int)mip, P, out, out_stride, status, stream));
+    uint32_t key = 0;
+    RE_CUDA(cudaMemcpyAsync(&key, status, 4, cudaMemcpyDeviceToHost, stream));
+    RE_CUDA(cudaStreamSynchronize(stream));
+    return status_from_key(key);
 }
 
 // Renderer::render_tiles (RawEngine.cpp:1390-1412): tile loop in the

@@ -96,29 +96,20 @@ struct DevCurve {
     float slope[256];         // segment slopes (linear segments and extrapolation)
     float4 coef[256];         // power-basis cubic per segment: c0 + t(c1 + t(c2 + t c3))
     float inv_h[256];         // 1 / (x[i+1] - x[i])
+    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none),
+    // each naming a segment at or below every sample that falls in it; records
+    // 0..n-2 are the segments, n-1 the right and n the left linear extrapolation.
+    uint32_t ncells;
+    float x0c, inv_dx, pad2;
+    float4 rec[258];          // {x anchor, 1/h (1 for linear records), next knot (RU), 0}
+    float4 rcoef[258];        // power basis in t = (v - anchor) * rec.y
+    uint8_t cell_seg[4096];
 };
 
 struct DevCurveSet {
     DevCurve c[4];            // master, R, G, B
 };
 
-// Shared-memory copy of a curve set whose curves have at most SC_MAX knots
-// (each CTA loads it once; the per-sample segment search then reads only
-// shared memory).
-constexpr int SC_MAX = 32;
-struct SmemCurve {
-    uint32_t n, identity, cubic, pad;    // pad: largest power of two <= n (search span)
-    float xf[SC_MAX];
-    float xeq[SC_MAX];
-    float xn[SC_MAX];
-    float y[SC_MAX];
-    float slope[SC_MAX];
-    float inv_h[SC_MAX];
-    float4 coef[SC_MAX];
-};
-struct SmemCurveSet {
-    SmemCurve c[4];
-};
 
 // --------------------------------------------------------------- program
 

@@ -39,76 +39,31 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
     return k.x + t * (k.y + t * (k.z + t * k.w));
 }
 
-// Three samples through one shared-memory curve at once: a fixed-length,
-// branch-free upper_bound (binary lifting over the RU-rounded knots) so that
-// the three searches interleave instead of chaining their loads.
-__device__ __forceinline__ void curve_map3(const SmemCurve* __restrict__ c, float v[3]) {
-    if (c->identity) return;
+// Cell lookup (DevCurve::ncells > 0): the cell gives a segment at or below
+// the sample, a short walk over the RU-rounded knots (which equals the
+// reference's double comparisons for every float sample) finds the segment,
+// and one power-basis polynomial evaluates it.  Extrapolation and linear
+// curves are records of the same form.
+__device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
     const int n = (int)c->n;
-    int lo[3] = {0, 0, 0};
-    for (int step = (int)c->pad; step > 0; step >>= 1) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int cand = lo[k] + step;
-            if (cand <= n && v[k] >= c->xf[cand - 1]) lo[k] = cand;
-        }
+    int rec;
+    if (v < __ldg(&c->xf[0])) {
+        rec = n;
+    } else {
+        int cell = __float2int_rz((v - c->x0c) * c->inv_dx);
+        cell = min(max(cell, 0), (int)c->ncells - 1);
+        rec = __ldg(&c->cell_seg[cell]);
+        while (rec < n - 1 && v >= __ldg(&c->rec[rec].z)) ++rec;
     }
-    const float xl = c->xf[n - 1], x0 = c->xf[0];
-    const bool tail_nan = isnan(c->xeq[n - 1]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int left = lo[k] == 0 ? 0 : lo[k] - 1;
-        const int seg = left < n - 2 ? left : n - 2;
-        const float x = v[k];
-        float r;
-        if (x == c->xeq[left]) {
-            r = c->y[left];
-        } else if (!c->cubic || x < x0 || x > xl || (x == xl && tail_nan)) {
-            const float s = c->slope[seg];
-            const float yl = c->y[left];
-            r = s == 0.0f ? yl : yl + (x - c->xn[left]) * s;
-        } else {
-            const float t = (x - c->xn[seg]) * c->inv_h[seg];
-            const float4 kf = c->coef[seg];
-            r = kf.x + t * (kf.y + t * (kf.z + t * kf.w));
-        }
-        v[k] = r;
-    }
+    const float4 r = __ldg(&c->rec[rec]);
+    const float4 k = __ldg(&c->rcoef[rec]);
+    const float t = (v - r.x) * r.y;
+    return k.x + t * (k.y + t * (k.z + t * k.w));
 }
 
-// Loads curve set 0 of P into shared memory when every curve fits; returns it
-// (or null, in which case curves are read from global memory).  All threads
-// of the block must call it; it ends with a barrier.
-__device__ __forceinline__ const SmemCurveSet* load_curves(const DevProgram& P, SmemCurveSet* sc) {
-    const DevCurveSet* g = P.curves[0];
-    bool fits = g != nullptr;
-    if (fits)
-        for (int k = 0; k < 4; ++k) fits &= g->c[k].n <= (uint32_t)SC_MAX;
-    if (!fits) return nullptr;
-    for (int k = 0; k < 4; ++k) {
-        const DevCurve& src = g->c[k];
-        SmemCurve& dst = sc->c[k];
-        const int n = (int)src.n;
-        if (threadIdx.x == 0) {
-            dst.n = src.n;
-            dst.identity = src.identity;
-            dst.cubic = src.cubic;
-            uint32_t p2 = 1;                    // largest power of two <= n (search span)
-            while (p2 * 2 <= src.n) p2 *= 2;
-            dst.pad = p2;
-        }
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            dst.xf[i] = src.xf[i];
-            dst.xeq[i] = src.xeq[i];
-            dst.xn[i] = src.xn[i];
-            dst.y[i] = src.y[i];
-            dst.slope[i] = src.slope[i];
-            dst.inv_h[i] = src.inv_h[i];
-            dst.coef[i] = src.coef[i];
-        }
-    }
-    __syncthreads();
-    return sc;
+__device__ __forceinline__ float curve_apply(const DevCurve* __restrict__ c, float v) {
+    if (c->identity) return v;
+    return c->ncells ? curve_cells(c, v) : curve_map(c, v);
 }
 
 // x^e for x in [0, 1] through the hardware log2/exp2 approximations: a few
@@ -127,8 +82,7 @@ __device__ __forceinline__ uint32_t stage_key(int s, uint32_t kind) {
 
 // Applies stages [begin, end) of P to one pixel; `err` keeps the max key.
 __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int end, float& r,
-                                             float& g, float& b, uint32_t& err,
-                                             const SmemCurveSet* sc = nullptr) {
+                                             float& g, float& b, uint32_t& err) {
     float v[3] = {r, g, b};
     for (int s = begin; s < end; ++s) {
         const re_stage& st = P.st[s];
@@ -180,30 +134,15 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
         }
         case RE_STAGE_CURVES: {
             bool bad = !(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]));
-            if (sc && st.arg == 0) {
-                curve_map3(&sc->c[0], v);
+            const DevCurveSet* cs = P.curves[st.arg];
+            const bool master_id = cs->c[0].identity;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (!isfinite(v[c])) bad = true;
-                    const SmemCurve* ch = &sc->c[c + 1];
-                    if (!ch->identity) {
-                        float one[3] = {v[c], v[c], v[c]};
-                        curve_map3(ch, one);
-                        v[c] = one[0];
-                    }
-                    if (!isfinite(v[c])) bad = true;
-                }
-            } else {
-                const DevCurveSet* cs = P.curves[st.arg];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const DevCurve* ch = &cs->c[c + 1];
-                    if (cs->c[0].identity && ch->identity) continue;
-                    const float master = curve_map(&cs->c[0], v[c]);
-                    const float mapped = curve_map(ch, master);
-                    if (!isfinite(master) || !isfinite(mapped)) bad = true;
-                    v[c] = mapped;
-                }
+            for (int c = 0; c < 3; ++c) {
+                const DevCurve* ch = &cs->c[c + 1];
+                const float master = master_id ? v[c] : curve_apply(&cs->c[0], v[c]);
+                const float mapped = curve_apply(ch, master);
+                if (!isfinite(master) || !isfinite(mapped)) bad = true;
+                v[c] = mapped;
             }
             if (bad) {
                 err = max(err, stage_key(s, ST_INVALID));
@@ -217,6 +156,156 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
     r = v[0];
     g = v[1];
     b = v[2];
+}
+
+// Cell-lookup evaluation with the curve's uniform scalars already in registers.
+struct CurveView {
+    const DevCurve* c;
+    int n, ncells;
+    float xf0, x0c, inv_dx;
+    bool identity;
+    __device__ __forceinline__ void load(const DevCurve* curve) {
+        c = curve;
+        identity = curve->identity != 0;
+        n = (int)curve->n;
+        ncells = (int)curve->ncells;
+        xf0 = curve->xf[0];
+        x0c = curve->x0c;
+        inv_dx = curve->inv_dx;
+    }
+    __device__ __forceinline__ float eval(float v) const {
+        if (identity) return v;
+        if (!ncells) return curve_map(c, v);
+        int rec;
+        if (v < xf0) {
+            rec = n;
+        } else {
+            int cell = __float2int_rz((v - x0c) * inv_dx);
+            cell = min(max(cell, 0), ncells - 1);
+            rec = __ldg(&c->cell_seg[cell]);
+            while (rec < n - 1 && v >= __ldg(&c->rec[rec].z)) ++rec;
+        }
+        const float4 r = __ldg(&c->rec[rec]);
+        const float4 k = __ldg(&c->rcoef[rec]);
+        const float t = (v - r.x) * r.y;
+        return k.x + t * (k.y + t * (k.z + t * k.w));
+    }
+};
+
+// The stage program over N pixels held by one thread: the stage loop is
+// outside, so each stage's constants are read once and its arithmetic runs
+// over N independent pixels.  Per pixel the operations and their order are
+// exactly apply_stages'.
+template <int N>
+__device__ __forceinline__ void apply_stages_n(const DevProgram& P, int begin, int end, float (&r)[N],
+                                               float (&g)[N], float (&b)[N], uint32_t& err) {
+    for (int s = begin; s < end; ++s) {
+        const re_stage& st = P.st[s];
+        switch (st.kind) {
+        case RE_STAGE_GAIN3: {
+            const float k0 = st.f[0], k1 = st.f[1], k2 = st.f[2];
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                r[i] = __fmul_rn(r[i], k0);
+                g[i] = __fmul_rn(g[i], k1);
+                b[i] = __fmul_rn(b[i], k2);
+            }
+            break;
+        }
+        case RE_STAGE_SCALE: {
+            const float k = st.f[0];
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                r[i] = __fmul_rn(r[i], k);
+                g[i] = __fmul_rn(g[i], k);
+                b[i] = __fmul_rn(b[i], k);
+            }
+            break;
+        }
+        case RE_STAGE_MATRIX: {
+            const float m0 = st.f[0], m1 = st.f[1], m2 = st.f[2], m3 = st.f[3], m4 = st.f[4], m5 = st.f[5],
+                        m6 = st.f[6], m7 = st.f[7], m8 = st.f[8];
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const float nr = __fadd_rn(__fadd_rn(__fmul_rn(m0, r[i]), __fmul_rn(m1, g[i])), __fmul_rn(m2, b[i]));
+                const float ng = __fadd_rn(__fadd_rn(__fmul_rn(m3, r[i]), __fmul_rn(m4, g[i])), __fmul_rn(m5, b[i]));
+                const float nb = __fadd_rn(__fadd_rn(__fmul_rn(m6, r[i]), __fmul_rn(m7, g[i])), __fmul_rn(m8, b[i]));
+                r[i] = nr;
+                g[i] = ng;
+                b[i] = nb;
+            }
+            break;
+        }
+        case RE_STAGE_TONE: {
+            const float shoulder = st.f[0], inv_gamma = st.f[1];
+            const bool linear = inv_gamma == 1.0f;
+            auto tone = [&](float lin) {
+                const float mag = fabsf(lin);
+                const float comp = __fdiv_rn(mag, __fadd_rn(mag, shoulder));
+                return copysignf(linear ? comp : unit_pow(comp, inv_gamma), lin);
+            };
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                r[i] = tone(r[i]);
+                g[i] = tone(g[i]);
+                b[i] = tone(b[i]);
+            }
+            break;
+        }
+        case RE_STAGE_CLIP: {
+            bool bad = false;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
+                r[i] = fminf(fmaxf(r[i], 0.0f), 1.0f);
+                g[i] = fminf(fmaxf(g[i], 0.0f), 1.0f);
+                b[i] = fminf(fmaxf(b[i], 0.0f), 1.0f);
+            }
+            if (bad) err = max(err, stage_key(s, ST_DOMAIN));
+            break;
+        }
+        case RE_STAGE_SRGB: {
+            bool bad = false;
+            auto enc = [](float v) {
+                const float lin = fminf(fmaxf(v, 0.0f), 1.0f);
+                return lin <= 0.0031308f ? __fmul_rn(12.92f, lin)
+                                         : __fsub_rn(__fmul_rn(1.055f, unit_pow(lin, 1.0f / 2.4f)), 0.055f);
+            };
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
+                r[i] = enc(r[i]);
+                g[i] = enc(g[i]);
+                b[i] = enc(b[i]);
+            }
+            if (bad) err = max(err, stage_key(s, ST_DOMAIN));
+            break;
+        }
+        case RE_STAGE_CURVES: {
+            const DevCurveSet* cs = P.curves[st.arg];
+            CurveView m, cr, cg, cb;
+            m.load(&cs->c[0]);
+            cr.load(&cs->c[1]);
+            cg.load(&cs->c[2]);
+            cb.load(&cs->c[3]);
+            bool bad = false;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
+                const float mr = m.eval(r[i]), mg = m.eval(g[i]), mb = m.eval(b[i]);
+                bad |= !(isfinite(mr) && isfinite(mg) && isfinite(mb));
+                r[i] = cr.eval(mr);
+                g[i] = cg.eval(mg);
+                b[i] = cb.eval(mb);
+                bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
+            }
+            if (bad) err = max(err, stage_key(s, ST_INVALID));
+            break;
+        }
+        default:
+            break;
+        }
+    }
 }
 
 __device__ __forceinline__ void report(uint32_t* status, uint32_t err) {

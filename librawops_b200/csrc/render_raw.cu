@@ -35,10 +35,11 @@ __host__ __device__ constexpr int pat(int l, int k) {
 template <int L>
 __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0, int y0, int ox, int oy,
                                               int ow, int oh, int stage_end, const DevProgram& P,
-                                              const SmemCurveSet* sc, float* __restrict__ out,
-                                              size_t out_stride, uint32_t& err) {
+                                              float* __restrict__ out, size_t out_stride, uint32_t& err) {
     for (int q = threadIdx.x; q < (BL_TW / 2) * (BL_TH / 2); q += BL_THREADS) {
         const int qx = q % (BL_TW / 2), qy = q / (BL_TW / 2);
+        float R[4], G[4], B[4];
+        bool keep[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int i = k & 1, j = k >> 1;
@@ -62,12 +63,20 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
                 rgb[1] = __fmul_rn(edge, 0.25f);
                 rgb[2 - own] = __fmul_rn(diag, 0.25f);
             }
-            if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
-            apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err, sc);
+            keep[k] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
+            R[k] = keep[k] ? rgb[0] : 0.0f;
+            G[k] = keep[k] ? rgb[1] : 0.0f;
+            B[k] = keep[k] ? rgb[2] : 0.0f;
+        }
+        apply_stages_n<4>(P, 0, stage_end, R, G, B, err);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!keep[k]) continue;
+            const int x = x0 + 2 * qx + (k & 1), y = y0 + 2 * qy + (k >> 1);
             float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
-            o[0] = rgb[0];
-            o[1] = rgb[1];
-            o[2] = rgb[2];
+            o[0] = R[k];
+            o[1] = G[k];
+            o[2] = B[k];
         }
     }
 }
@@ -82,7 +91,6 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
     __shared__ float tile[BL_SH][BL_SW];
-    __shared__ SmemCurveSet curves;
     const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
     for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
         const int sx = i % BL_SW, sy = i / BL_SW;
@@ -92,17 +100,16 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
             v = normalize_sample(raw, x, y);
         tile[sy][sx] = v;
     }
-    const SmemCurveSet* sc = load_curves(P, &curves);
     __syncthreads();
     uint32_t err = 0;
     const bool interior = x0 - 1 >= raw.ax && y0 - 1 >= raw.ay && x0 + BL_TW + 1 <= raw.ax + raw.aw &&
                           y0 + BL_TH + 1 <= raw.ay + raw.ah;
     if (interior) {
         switch (layout) {
-        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
         report(status, err);
         return;
@@ -136,7 +143,7 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
             }
             rgb[ch] = count ? __fdiv_rn(sum, (float)count) : 0.0f;
         }
-        apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err, sc);
+        apply_stages(P, 0, stage_end, rgb[0], rgb[1], rgb[2], err);
         float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
         o[0] = rgb[0];
         o[1] = rgb[1];
@@ -370,7 +377,7 @@ __device__ __forceinline__ double five(const double* r, int d) {
 template <int L>
 __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
                                            int ow, int oh, int stage_end, const DevProgram& P,
-                                           const SmemCurveSet* sc, float* __restrict__ out, size_t out_stride,
+                                           float* __restrict__ out, size_t out_stride,
                                            uint32_t& err) {
     constexpr int AX = ng_col(L), BX = 1 - AX;
     const int t = threadIdx.x;
@@ -494,9 +501,12 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
         }
     }
     __syncthreads();
-    // 6. opposite colour at R/B sites, float cast, fused stages (MenonDemosaic.cpp:162-173)
+    // 6. opposite colour at R/B sites, float cast (MenonDemosaic.cpp:162-173), then the
+    //    fused stages over the quad's four pixels at once
     for (int q = t; q < (MN_TW / 2) * (MN_TH / 2); q += MN_THREADS) {
         const int qx = q % (MN_TW / 2), qy = q / (MN_TW / 2);
+        float R[4], G[4], B[4];
+        bool keep[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int i = k & 1, j = k >> 1;
@@ -507,13 +517,21 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
             double rr = red[pg], bb = blue[pg];
             if (own == 2) rr = dsub(dadd(bb, half_sum(red[pg - d], red[pg + d])), half_sum(blue[pg - d], blue[pg + d]));
             if (own == 0) bb = dsub(dadd(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
-            float r = (float)rr, g = (float)S.green[pg], b = (float)bb;
-            if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
-            apply_stages(P, 0, stage_end, r, g, b, err, sc);
+            keep[k] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
+            // pixels outside the viewport enter the stages as zeros (never written)
+            R[k] = keep[k] ? (float)rr : 0.0f;
+            G[k] = keep[k] ? (float)S.green[pg] : 0.0f;
+            B[k] = keep[k] ? (float)bb : 0.0f;
+        }
+        apply_stages_n<4>(P, 0, stage_end, R, G, B, err);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!keep[k]) continue;
+            const int x = x0 + 2 * qx + (k & 1), y = y0 + 2 * qy + (k >> 1);
             float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
-            o[0] = r;
-            o[1] = g;
-            o[2] = b;
+            o[0] = R[k];
+            o[1] = G[k];
+            o[2] = B[k];
         }
     }
 }
@@ -522,13 +540,12 @@ union MenonShared {
     MenonSmem generic;
     FastSmem fast;
 };
-constexpr size_t kCurveOffset = (sizeof(MenonShared) + 15) & ~size_t(15);
 
 // One CTA per MN_TW x MN_TH tile of the viewport, tiles anchored at an even
 // sensor coordinate.  Interior tiles take the fast quad path; tiles whose
 // footprint meets the active-area edge take the general mirrored path.
 // Writes float32 RGB after stages [0, stage_end) (row stride in floats).
-__global__ void __launch_bounds__(MN_THREADS, 2)
+__global__ void __launch_bounds__(MN_THREADS, 4)
 menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
              const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
              uint32_t* status, unsigned long long* ties) {
@@ -536,16 +553,15 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
     const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
     const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
     uint32_t err = 0;
-    const SmemCurveSet* sc = load_curves(P, reinterpret_cast<SmemCurveSet*>(smem_raw + kCurveOffset));
     const bool interior = !ties && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay && x0 + MN_TW + 6 <= raw.ax + raw.aw &&
                           y0 + MN_TH + 6 <= raw.ay + raw.ah;
     if (interior) {
         FastSmem& F = reinterpret_cast<MenonShared*>(smem_raw)->fast;
         switch (layout) {
-        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
-        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, sc, out, out_stride, err); break;
+        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
         report(status, err);
         return;
@@ -575,7 +591,7 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
             bb = __dadd_rn(__dadd_rn(rr, pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy)),
                            -pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy));
         float r = (float)rr, g = (float)S.green[ty + 2][tx + 2], b = (float)bb;
-        apply_stages(P, 0, stage_end, r, g, b, err, sc);
+        apply_stages(P, 0, stage_end, r, g, b, err);
         float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
         o[0] = r;
         o[1] = g;
@@ -593,8 +609,6 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
                                   size_t native_stride, int scale, int ow, int oh, int stage_begin,
                                   int stage_end, const __grid_constant__ DevProgram P,
                                   float* __restrict__ out, size_t out_stride, uint32_t* status) {
-    __shared__ SmemCurveSet curves;
-    const SmemCurveSet* sc = load_curves(P, &curves);
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= ow || y >= oh) return;
@@ -612,12 +626,64 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
     const double n = (double)count;
     float r = (float)__ddiv_rn(s0, n), g = (float)__ddiv_rn(s1, n), b = (float)__ddiv_rn(s2, n);
     uint32_t err = 0;
-    apply_stages(P, stage_begin, stage_end, r, g, b, err, sc);
+    apply_stages(P, stage_begin, stage_end, r, g, b, err);
     float* o = out + (size_t)y * out_stride + (size_t)x * 3;
     o[0] = r;
     o[1] = g;
     o[2] = b;
     report(status, err);
+}
+
+// ----------------------------------------------------------- raster sources
+
+// RasterSourceNode::render_level (RawEngine.cpp:346-406) followed by the stage
+// program: mip 0 copies the pixel, mip 1/2 average the clipped scale x scale
+// footprint in double (row-major, per channel) with the actual count.
+__global__ void raster_render_kernel(const float* __restrict__ in, size_t in_stride, int width, int height,
+                                     int ox, int oy, int ow, int oh, int scale, int stage_end,
+                                     const __grid_constant__ DevProgram P, float* __restrict__ out,
+                                     size_t out_stride, uint32_t* status) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= ow || y >= oh) return;
+    float r, g, b;
+    if (scale == 1) {
+        const float* p = in + (size_t)(oy + y) * in_stride + (size_t)(ox + x) * 3;
+        r = p[0]; g = p[1]; b = p[2];
+    } else {
+        const int sy0 = (oy + y) * scale, sx0 = (ox + x) * scale;
+        const int sy1 = min(sy0 + scale, height), sx1 = min(sx0 + scale, width);
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int sy = sy0; sy < sy1; ++sy)
+            for (int sx = sx0; sx < sx1; ++sx) {
+                const float* p = in + (size_t)sy * in_stride + (size_t)sx * 3;
+                s0 = __dadd_rn(s0, (double)p[0]);
+                s1 = __dadd_rn(s1, (double)p[1]);
+                s2 = __dadd_rn(s2, (double)p[2]);
+            }
+        const double n = (double)((sx1 - sx0) * (sy1 - sy0));
+        r = (float)__ddiv_rn(s0, n);
+        g = (float)__ddiv_rn(s1, n);
+        b = (float)__ddiv_rn(s2, n);
+    }
+    uint32_t err = 0;
+    apply_stages(P, 0, stage_end, r, g, b, err);
+    float* o = out + (size_t)y * out_stride + (size_t)x * 3;
+    o[0] = r;
+    o[1] = g;
+    o[2] = b;
+    report(status, err);
+}
+
+cudaError_t launch_raster(const float* in, size_t in_stride, int width, int height, int ox, int oy, int ow, int oh,
+                          int mip, const DevProgram& P, float* out, size_t out_stride, uint32_t* status,
+                          cudaStream_t stream) {
+    if (ow <= 0 || oh <= 0) return cudaSuccess;
+    dim3 block(32, 8);
+    dim3 grid((ow + 31) / 32, (oh + 7) / 8);
+    raster_render_kernel<<<grid, block, 0, stream>>>(in, in_stride, width, height, ox, oy, ow, oh, 1 << mip,
+                                                     (int)P.count, P, out, out_stride, status);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------- launch
@@ -643,7 +709,7 @@ cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy
     if (ow <= 0 || oh <= 0) return cudaSuccess;
     // Menon with a singleton active-area axis is bilinear (RawEngine.cpp:303).
     if (demosaic == 1 && raw.aw > 1 && raw.ah > 1) {
-        const size_t smem = kCurveOffset + sizeof(SmemCurveSet);
+        const size_t smem = sizeof(MenonShared);
         cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const int gx0 = ox & ~1, gy0 = oy & ~1;

@@ -208,3 +208,33 @@ def test_device_output_and_async_status():
     torch.cuda.synchronize()
     render.status_from_device(int(status.item()))
     assert bits_equal(dev2.cpu().numpy(), host)
+
+
+def test_extended_curves_against_oracle(oracle):
+    """Curve evaluation (cell lookup, binary-search fallback, linear and cubic,
+    extrapolation on both sides, samples exactly at knots) vs the reference's
+    binary64 restatement, through a bilinear chain."""
+    from oracle.oracle import OP_CURVES_EXT, Op, curves_params
+    rng = np.random.default_rng(21)
+    w, h = 96, 64
+    s = rng.integers(300, 16000, w * h).astype(np.uint16)
+    raw = RawSpec(w, h, s, 0, 0, 0, 0, (0, 0, w, h), (512,) * 4, (16383,) * 4)
+    meta = render.Metadata(w, h, 0, 0, 0, 0, (0, 0, w, h), (512,) * 4, (16383,) * 4)
+    img = render.Image(meta, s)
+    cases = []
+    for n in (2, 3, 5, 16, 40):
+        xs = np.sort(rng.uniform(0.05, 0.9, n))
+        ys = np.cumsum(rng.uniform(0.0, 0.3, n))
+        cases.append([(float(a), float(b)) for a, b in zip(xs, ys)])
+    tiny = [(0.0, 0.0), (1e-4, 0.3), (0.5, 0.6), (1.0, 1.0)]        # forces the search fallback
+    cases.append(tiny)
+    exact = [(0.25, 0.3), (0.5, 0.5), (0.75, 0.9)]                   # knots that are floats
+    cases.append(exact)
+    for knots in cases:
+        for cubic in (True, False):
+            chans = [knots, None, [(0.0, 0.0), (0.5, 0.7), (1.5, 1.6)], None]
+            pipe = render.Pipeline().extended_curves(render.CurveSet(*chans, cubic=cubic))
+            ops = [Op(OP_CURVES_EXT, curves_params(int(cubic), *chans))]
+            got = render.render(img, pipe, (0, 0, w, h))
+            want = oracle.render_raw(raw, False, ops, (0, 0, w, h))
+            within_tolerance(got, want, lsb16=False)
