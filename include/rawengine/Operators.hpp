@@ -1,0 +1,174 @@
+// Drop-in spatial, tone and geometry operators of RawEngine's render path
+// (the reference's SpatialOps.hpp, ToneOps.hpp and GeometryOps.hpp entries
+// that the tiled render reaches), executed on the B200 kernels.
+#pragma once
+
+#include "RawEngine.hpp"
+
+namespace rawengine {
+
+// ----------------------------------------------------------------- ToneOps
+
+struct CurvePoint { double x = 0, y = 0; };
+enum class CurveInterpolation { Linear, ShapePreservingCubic };
+struct CurveKnots { std::vector<CurvePoint> knots{{0, 0}, {1, 1}}; };
+struct ExtendedCurvesSettings {
+    CurveKnots master;
+    std::array<CurveKnots, 3> channels;
+    CurveInterpolation interpolation = CurveInterpolation::Linear;
+};
+RAWENGINE_API void validate_extended_curves_settings(const ExtendedCurvesSettings& settings);
+
+struct CurveTables;  // device curve set
+
+// Master then per-channel curve (ToneOps.cpp:795-844); scene-linear working input.
+class RAWENGINE_API ExtendedCurvesNode final : public PointNode {
+public:
+    ExtendedCurvesNode(std::shared_ptr<const Node> input, ExtendedCurvesSettings settings = {});
+    bool supports_level(RenderLevel level) const noexcept override;
+    Rect input_region_level(Rect output, Rect bounds, RenderLevel level) const override;
+    ImageDescriptor output_descriptor() const noexcept override { return input_->output_descriptor(); }
+    const CurveTables& tables() const noexcept { return *tables_; }
+private:
+    ExtendedCurvesSettings settings_;
+    std::shared_ptr<CurveTables> tables_;
+};
+
+// -------------------------------------------------------------- SpatialOps
+
+struct LocalStatisticsTile {
+    Rect bounds;
+    ImageDescriptor descriptor;
+    std::uint32_t radius = 3;
+    std::vector<double> mean, variance;       // interleaved RGB; population variance
+    std::vector<std::uint32_t> finite_count;  // non-finite samples excluded per channel
+};
+
+RAWENGINE_API Rect local_statistics_region(Rect output, Rect image_bounds, std::uint32_t radius);
+RAWENGINE_API LocalStatisticsTile local_statistics_rgb(const Tile& input, Rect output, Rect image_bounds,
+                                                       std::uint32_t radius = 3);
+using LocalStatisticsCallback = std::function<void(const LocalStatisticsTile&)>;
+RAWENGINE_API void analyze_local_rgb(const Node& output, Rect native_bounds, const RenderRequest& request,
+                                     const LocalStatisticsCallback& callback, std::uint32_t radius = 3,
+                                     const CancellationToken* cancellation = nullptr);
+RAWENGINE_API void analyze_local_rgb(const ImageGraph& graph, const RenderRequest& request,
+                                     const LocalStatisticsCallback& callback, std::uint32_t radius = 3,
+                                     const CancellationToken* cancellation = nullptr);
+
+struct WorkingYGuidedFilterSettings {
+    std::uint32_t radius = 3;   // 0..8 (the reference's contract)
+    double epsilon = 0x1p-12;   // finite [2^-24, 65536]
+};
+RAWENGINE_API void validate_working_y_guided_filter_settings(const WorkingYGuidedFilterSettings& settings);
+RAWENGINE_API Rect working_y_guided_filter_region(Rect output, Rect image_bounds, std::uint32_t radius);
+RAWENGINE_API Tile working_y_guided_filter_rgb(const Tile& input, Rect output, Rect image_bounds,
+                                               const WorkingYGuidedFilterSettings& settings = {});
+
+class RAWENGINE_API WorkingYGuidedFilterNode final : public DeviceNode {
+public:
+    WorkingYGuidedFilterNode(std::shared_ptr<const Node> input, Rect native_bounds,
+                             WorkingYGuidedFilterSettings settings = {});
+    bool supports_level(RenderLevel level) const noexcept override;
+    Rect input_region(Rect output, Rect source_bounds) const override;
+    Rect input_region_level(Rect output, Rect source_bounds, RenderLevel level) const override;
+    const Node* input_node() const noexcept override { return input_.get(); }
+    ImageDescriptor output_descriptor() const noexcept override { return descriptor_; }
+    const WorkingYGuidedFilterSettings& settings() const noexcept { return settings_; }
+    Rect native_bounds() const noexcept { return native_bounds_; }
+private:
+    std::shared_ptr<const Node> input_;
+    Rect native_bounds_;
+    WorkingYGuidedFilterSettings settings_;
+    ImageDescriptor descriptor_;
+};
+
+// ------------------------------------------------------------- GeometryOps
+
+struct RAWENGINE_API RotateSettings {
+    double angle_degrees = 0;
+};
+RAWENGINE_API void validate_rotate_settings(const RotateSettings& settings);
+
+class RAWENGINE_API RotateNode final : public DeviceNode {
+public:
+    RotateNode(std::shared_ptr<const Node> input, Rect input_bounds, RotateSettings settings = {});
+    bool supports_level(RenderLevel level) const noexcept override;
+    RenderLevel input_level(RenderLevel level) const override;
+    Rect input_region(Rect output, Rect input_bounds) const override;
+    Rect input_region_level(Rect output, Rect input_bounds, RenderLevel level) const override;
+    const Node* input_node() const noexcept override { return input_.get(); }
+    ImageDescriptor output_descriptor() const noexcept override { return descriptor_; }
+    Rect output_bounds() const noexcept { return {0, 0, input_bounds_.width, input_bounds_.height}; }
+    Rect native_output_region(Rect output, RenderLevel level) const;
+    Rect support(Rect native_output) const;
+    Rect input_bounds() const noexcept { return input_bounds_; }
+    double angle() const noexcept { return settings_.angle_degrees; }
+private:
+    std::shared_ptr<const Node> input_;
+    Rect input_bounds_;
+    RotateSettings settings_;
+    ImageDescriptor descriptor_;
+    double cx_, cy_, cosine_, sine_;
+};
+
+struct RAWENGINE_API CubicResizeSettings {
+    std::uint32_t width = 0, height = 0;
+};
+RAWENGINE_API void validate_cubic_resize_settings(const CubicResizeSettings& settings, Rect native_input_bounds);
+
+class RAWENGINE_API CubicResizeNode final : public DeviceNode {
+public:
+    CubicResizeNode(std::shared_ptr<const Node> input, Rect input_bounds, CubicResizeSettings settings);
+    bool supports_level(RenderLevel level) const noexcept override;
+    RenderLevel input_level(RenderLevel level) const override;
+    Rect input_region(Rect output, Rect input_bounds) const override;
+    Rect input_region_level(Rect output, Rect input_bounds, RenderLevel level) const override;
+    const Node* input_node() const noexcept override { return input_.get(); }
+    ImageDescriptor output_descriptor() const noexcept override { return descriptor_; }
+    Rect output_bounds() const noexcept { return {0, 0, settings_.width, settings_.height}; }
+    Rect native_output_region(Rect output, RenderLevel level) const;
+    Rect support(Rect native_output) const;
+    Rect input_bounds() const noexcept { return input_bounds_; }
+    const CubicResizeSettings& settings() const noexcept { return settings_; }
+private:
+    std::shared_ptr<const Node> input_;
+    Rect input_bounds_;
+    CubicResizeSettings settings_;
+    ImageDescriptor descriptor_;
+};
+
+// ----------------------------------------------------------- TileScheduler
+
+enum class RenderPriority { Background = 0, Normal = 1, Interactive = 2 };
+
+// Queued requests run in priority order, FIFO within a priority; each worker
+// thread renders on its own CUDA stream.  Throws length_error when the pending
+// budget is full; cancellation is checked before and between tiles.
+class RAWENGINE_API TileScheduler final {
+public:
+    TileScheduler(std::size_t workers, std::size_t max_pending);
+    ~TileScheduler();
+    TileScheduler(const TileScheduler&) = delete;
+    TileScheduler& operator=(const TileScheduler&) = delete;
+    std::future<Tile> submit(std::shared_ptr<const Node> output, Rect source_bounds, RenderRequest request,
+                             RenderPriority priority = RenderPriority::Normal,
+                             std::shared_ptr<CancellationToken> cancellation = nullptr);
+    std::future<Tile> submit(std::shared_ptr<const Node> output, Rect source_bounds, Rect viewport,
+                             RenderPriority priority = RenderPriority::Normal, std::uint32_t tile_size = 256,
+                             std::shared_ptr<CancellationToken> cancellation = nullptr);
+    std::future<Tile> submit_latest(std::string group, std::shared_ptr<const Node> output, Rect source_bounds,
+                                    RenderRequest request, RenderPriority priority = RenderPriority::Interactive,
+                                    std::shared_ptr<CancellationToken> cancellation = nullptr);
+    std::future<Tile> submit_latest(std::string group, std::shared_ptr<const Node> output, Rect source_bounds,
+                                    Rect viewport, RenderPriority priority = RenderPriority::Interactive,
+                                    std::uint32_t tile_size = 256,
+                                    std::shared_ptr<CancellationToken> cancellation = nullptr);
+private:
+    std::future<Tile> submit_request(std::string group, std::shared_ptr<const Node> output, Rect source_bounds,
+                                     RenderRequest request, RenderPriority priority,
+                                     std::shared_ptr<CancellationToken> cancellation);
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+}  // namespace rawengine

@@ -1,0 +1,4 @@
+// Same include name as the reference header SpatialOps.hpp; the declarations of the
+// render-path subset live in Operators.hpp.
+#pragma once
+#include "Operators.hpp"

@@ -236,6 +236,15 @@ RE_API re_status re_render_tiles(const re_image* image, const re_render_desc* de
 
 /* ------------------------------------------------------------- raster I/O */
 
+/* RasterSourceNode::render_level (RawEngine.cpp:346-406) followed by the
+ * stages of `desc` (its demosaic and anchor are ignored): `in` is a device
+ * float32 RGB image (width x height, row stride in floats); mip 1/2 Preview
+ * average each output pixel's clipped footprint in double with the actual
+ * count.  `out` is device memory.  Returns after completion on `stream`. */
+RE_API re_status re_render_raster(const float* in, size_t in_row_stride, uint32_t width, uint32_t height,
+                                  const re_render_desc* desc, re_rect viewport, uint32_t mip,
+                                  uint32_t quality, float* out, size_t out_row_stride, void* stream);
+
 /* float32 interleaved RGB device buffers for spatial/geometry stages. */
 
 /* working_y_guided_filter_rgb (SpatialOps.cpp:168-287) over a whole image:
@@ -254,6 +263,11 @@ RE_API re_status re_guided_filter(const float* in, size_t in_row_stride, float* 
 RE_API re_status re_local_statistics(const float* in, size_t in_row_stride, uint32_t width,
                                      uint32_t height, uint32_t radius, float* mean_out,
                                      float* variance_out, uint32_t* count_out, void* stream);
+/* The same with binary64 mean/variance, the precision of the reference's
+ * LocalStatisticsTile (SpatialOps.hpp:7-13). */
+RE_API re_status re_local_statistics_f64(const float* in, size_t in_row_stride, uint32_t width,
+                                         uint32_t height, uint32_t radius, double* mean_out,
+                                         double* variance_out, uint32_t* count_out, void* stream);
 
 /* CubicResizeNode (GeometryOps.cpp:346-513): scale-aware Catmull-Rom from an
  * in_w x in_h device image to the `output` rect of an out_w x out_h canvas at
@@ -266,6 +280,21 @@ RE_API re_status re_cubic_resize(const float* in, size_t in_row_stride, uint32_t
 RE_API re_status re_rotate(const float* in, size_t in_row_stride, uint32_t width, uint32_t height,
                            double angle_degrees, re_rect output, uint32_t mip, float* out,
                            size_t out_row_stride, void* stream);
+/* The same two operators on an input WINDOW: `in` holds only the input
+ * columns [window.x, window.x + window.width) and rows [window.y, ...) of the
+ * full in_w x in_h (width x height) image -- the support a tile needs, as the
+ * reference's nodes request it (GeometryOps.cpp:99-118, 411-430).  The window
+ * must cover the taps of every requested output pixel (checked on the host). */
+RE_API re_status re_cubic_resize_window(const float* in, size_t in_row_stride, re_rect window, uint32_t in_w,
+                                        uint32_t in_h, uint32_t out_w, uint32_t out_h, re_rect output,
+                                        uint32_t mip, float* out, size_t out_row_stride, void* stream);
+RE_API re_status re_rotate_window(const float* in, size_t in_row_stride, re_rect window, uint32_t width,
+                                  uint32_t height, double angle_degrees, re_rect output, uint32_t mip,
+                                  float* out, size_t out_row_stride, void* stream);
+/* GeometryOps.cpp:99-111 support of a native output rectangle (relative to the
+ * rotation's own bounds). */
+RE_API re_status re_rotation_support(uint32_t width, uint32_t height, double angle_degrees,
+                                     re_rect native_output, re_rect* support);
 /* GeometryOps.cpp:362-389 one Catmull-Rom axis (host): returns taps in *count. */
 RE_API re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, uint32_t* center,
                                uint32_t tap_index[18], double tap_weight[18], uint32_t* count);

@@ -3,9 +3,11 @@
     python -m librawops_b200.build            # -> librawops_b200/_lib/librawengine_b200.so
 
 nvcc compiles every csrc/*.cu for sm_100a (no fast-math: the IEEE division,
-rounding and powf semantics are part of the parity contract) and links one
-shared library exporting the C ABI of include/rawengine_b200.h.  Objects are
-rebuilt only when a source or header is newer than the library.
+rounding and powf semantics are part of the parity contract), g++ compiles the
+host-only csrc/*.cpp (the C++ drop-in surface of include/rawengine/, C++20),
+and one shared library is linked that exports the C ABI of
+include/rawengine_b200.h and the rawengine:: classes.  Objects are rebuilt
+only when a source or header is newer than the library.
 """
 from __future__ import annotations
 
@@ -20,6 +22,11 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "librawengine_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+HOST_CXX = "g++"
+CUDA_INCLUDE = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "include")
+CXX_FLAGS = ["-std=c++20", "-O2", "-g", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wextra",
+             "-Wno-unused-parameter", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+             "-I", CUDA_INCLUDE]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
@@ -29,9 +36,14 @@ def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+def _host_sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
 def _deps():
-    return _sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return _sources() + _host_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h")) + \
+        glob.glob(os.path.join(ROOT, "include", "rawengine", "*.hpp"))
 
 
 def stale() -> bool:
@@ -54,10 +66,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
             cmd += ["-Xptxas", "-v"]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
         objs.append(obj)
+    for src in _host_sources():
+        obj = os.path.join(OUT_DIR, os.path.basename(src)[:-4] + ".host.o")
+        cmd = [HOST_CXX, *CXX_FLAGS, "-c", src, "-o", obj]
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
     failed = False
     for src, p in procs:
         out, _ = p.communicate()
-        if verbose or p.returncode:
+        if verbose or p.returncode or (src.endswith(".cpp") and out):
             sys.stderr.write(out.decode())
         failed |= p.returncode != 0
     if failed:

@@ -95,13 +95,14 @@ __device__ __forceinline__ float finite_float(double v, uint32_t& err) {
 
 // Horizontal pass: H[r][x][c] for source rows [row0, row0+rows) and native
 // output columns [0, nw), GeometryOps.cpp:453-465.
-__global__ void cubic_h_kernel(const float* __restrict__ src, size_t src_stride, const Axis* __restrict__ ax,
-                               int nw, int row0, int rows, double* __restrict__ H, uint32_t* status) {
+__global__ void cubic_h_kernel(const float* __restrict__ src, size_t src_stride, int src_x0, int src_y0,
+                               const Axis* __restrict__ ax, int nw, int row0, int rows, double* __restrict__ H,
+                               uint32_t* status) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= nw || r >= rows) return;
     const Axis& a = ax[x];
-    const float* row = src + (size_t)(row0 + r) * src_stride;
+    const float* row = src + (size_t)(row0 + r - src_y0) * src_stride - (ptrdiff_t)src_x0 * 3;
     uint32_t err = 0;
     double* h = H + ((size_t)r * nw + x) * 3;
 #pragma unroll
@@ -157,8 +158,9 @@ struct RotateParams {
 };
 
 // GeometryOps.cpp:68-76 taps and 129-141 sampling, one native output pixel per thread.
-__global__ void rotate_kernel(const float* __restrict__ src, size_t src_stride, RotateParams p, int nx0, int ny0,
-                              int nw, int nh, float* __restrict__ out, size_t out_stride, uint32_t* status) {
+__global__ void rotate_kernel(const float* __restrict__ src, size_t src_stride, int src_x0, int src_y0,
+                              RotateParams p, int nx0, int ny0, int nw, int nh, float* __restrict__ out,
+                              size_t out_stride, uint32_t* status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nw || j >= nh) return;
@@ -172,19 +174,41 @@ __global__ void rotate_kernel(const float* __restrict__ src, size_t src_stride, 
     const double fx = __dsub_rn(sx, (double)x0), fy = __dsub_rn(sy, (double)y0);
     const uint32_t x1 = fx == 0 ? x0 : min(x0 + 1, (uint32_t)p.width - 1);
     const uint32_t y1 = fy == 0 ? y0 : min(y0 + 1, (uint32_t)p.height - 1);
+    const float* base = src - (ptrdiff_t)src_y0 * (ptrdiff_t)src_stride - (ptrdiff_t)src_x0 * 3;
     uint32_t err = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float a00 = src[(size_t)y0 * src_stride + (size_t)x0 * 3 + c];
-        const float a10 = src[(size_t)y0 * src_stride + (size_t)x1 * 3 + c];
-        const float a01 = src[(size_t)y1 * src_stride + (size_t)x0 * 3 + c];
-        const float a11 = src[(size_t)y1 * src_stride + (size_t)x1 * 3 + c];
+        const float a00 = base[(size_t)y0 * src_stride + (size_t)x0 * 3 + c];
+        const float a10 = base[(size_t)y0 * src_stride + (size_t)x1 * 3 + c];
+        const float a01 = base[(size_t)y1 * src_stride + (size_t)x0 * 3 + c];
+        const float a11 = base[(size_t)y1 * src_stride + (size_t)x1 * 3 + c];
         if (!(isfinite(a00) && isfinite(a10) && isfinite(a01) && isfinite(a11))) err = ST_INVALID | (201u << 8);
         const double upper = blend((double)a00, (double)a10, fx);
         const double lower = blend((double)a01, (double)a11, fx);
         out[(size_t)j * out_stride + (size_t)i * 3 + c] = finite_float(blend(upper, lower, fy), err);
     }
     if (err && status) atomicMax(status, err);
+}
+
+// GeometryOps.cpp:68-76 taps and 99-111 support scan, on the host (relative to the rotation bounds).
+re_status rotate_support_host(const RotateParams& p, re_rect out, re_rect& support) {
+    uint32_t left = (uint32_t)p.width, top = (uint32_t)p.height, right = 0, bottom = 0;
+    for (uint64_t y = out.y; y < (uint64_t)out.y + out.height; ++y)
+        for (uint64_t x = out.x; x < (uint64_t)out.x + out.width; ++x) {
+            const double dx = double(x) - p.cx, dy = double(y) - p.cy;
+            const double sx = std::clamp((p.cx + p.cosine * dx) + p.sine * dy, 0., double(p.width) - 1);
+            const double sy = std::clamp((p.cy - p.sine * dx) + p.cosine * dy, 0., double(p.height) - 1);
+            const uint32_t ix = (uint32_t)std::floor(sx), iy = (uint32_t)std::floor(sy);
+            const double fx = sx - ix, fy = sy - iy;
+            const uint32_t x1 = fx == 0 ? ix : std::min(ix + 1, (uint32_t)p.width - 1);
+            const uint32_t y1 = fy == 0 ? iy : std::min(iy + 1, (uint32_t)p.height - 1);
+            left = std::min(left, ix);
+            top = std::min(top, iy);
+            right = std::max(right, x1);
+            bottom = std::max(bottom, y1);
+        }
+    support = {left, top, right - left + 1, bottom - top + 1};
+    return RE_OK;
 }
 
 // native footprint of a reduced request over a canvas (GeometryOps.cpp:86-98, 399-410)
@@ -234,6 +258,26 @@ re_status finish(cudaStream_t stream, uint32_t* status_dev) {
 }  // namespace
 
 extern "C" {
+re_status re_cubic_resize_window(const float* in, size_t in_stride, re_rect window, uint32_t in_w, uint32_t in_h,
+                                 uint32_t out_w, uint32_t out_h, re_rect output, uint32_t mip, float* out,
+                                 size_t out_stride, void* stream_);
+re_status re_rotate_window(const float* in, size_t in_stride, re_rect window, uint32_t width, uint32_t height,
+                           double angle, re_rect output, uint32_t mip, float* out, size_t out_stride, void* stream_);
+
+re_status re_rotation_support(uint32_t width, uint32_t height, double angle, re_rect native_output, re_rect* support) {
+    RotateParams p{};
+    re_status s = re_rotation_coefficients(angle, &p.cosine, &p.sine);
+    if (s) return s;
+    p.cx = (double(width) - 1) / 2;
+    p.cy = (double(height) - 1) / 2;
+    p.width = (int)width;
+    p.height = (int)height;
+    if (!native_output.width || !native_output.height) {
+        *support = {0, 0, 0, 0};
+        return RE_OK;
+    }
+    return rotate_support_host(p, native_output, *support);
+}
 
 re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, uint32_t* center, uint32_t tap_index[18],
                         double tap_weight[18], uint32_t* count) {
@@ -255,7 +299,14 @@ re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, uint32_
 
 // GeometryOps.cpp:346-352 validation, 431-513 render.
 re_status re_cubic_resize(const float* in, size_t in_stride, uint32_t in_w, uint32_t in_h, uint32_t out_w,
-                          uint32_t out_h, re_rect output, uint32_t mip, float* out, size_t out_stride, void* stream_) {
+                          uint32_t out_h, re_rect output, uint32_t mip, float* out, size_t out_stride, void* stream) {
+    return re_cubic_resize_window(in, in_stride, {0, 0, in_w, in_h}, in_w, in_h, out_w, out_h, output, mip, out,
+                                  out_stride, stream);
+}
+
+re_status re_cubic_resize_window(const float* in, size_t in_stride, re_rect window, uint32_t in_w, uint32_t in_h,
+                                 uint32_t out_w, uint32_t out_h, re_rect output, uint32_t mip, float* out,
+                                 size_t out_stride, void* stream_) {
     if (!in_w || !in_h || !out_w || !out_h) {
         set_last_error("cubic resize requires positive input and canvas extents");
         return RE_INVALID_ARGUMENT;
@@ -274,7 +325,8 @@ re_status re_cubic_resize(const float* in, size_t in_stride, uint32_t in_w, uint
         return RE_OUT_OF_RANGE;
     }
     if (!output.width || !output.height) return RE_OK;
-    if (!in || !out || in_stride < (size_t)in_w * 3 || out_stride < (size_t)output.width * 3) {
+    if (!in || !out || in_stride < (size_t)window.width * 3 || out_stride < (size_t)output.width * 3 ||
+        (uint64_t)window.x + window.width > in_w || (uint64_t)window.y + window.height > in_h) {
         set_last_error("invalid cubic resize buffers");
         return RE_INVALID_ARGUMENT;
     }
@@ -295,6 +347,20 @@ re_status re_cubic_resize(const float* in, size_t in_stride, uint32_t in_w, uint
         }
     }
     const uint32_t rows = row_hi - row_lo + 1;
+    uint32_t col_lo = in_w, col_hi = 0;
+    for (const Axis& a : xs) {
+        col_lo = std::min(col_lo, a.center);
+        col_hi = std::max(col_hi, a.center);
+        for (uint32_t k = 0; k < a.count; ++k) {
+            col_lo = std::min(col_lo, a.index[k]);
+            col_hi = std::max(col_hi, a.index[k]);
+        }
+    }
+    if (col_lo < window.x || col_hi >= window.x + window.width || row_lo < window.y ||
+        row_hi >= window.y + window.height) {
+        set_last_error("cubic resize input window does not cover the taps' support");
+        return RE_INVALID_ARGUMENT;
+    }
     cudaStream_t stream = (cudaStream_t)stream_;
     const size_t axes_bytes = (xs.size() + ys.size()) * sizeof(Axis);
     const size_t h_bytes = (size_t)rows * native.width * 3 * sizeof(double);
@@ -313,7 +379,7 @@ re_status re_cubic_resize(const float* in, size_t in_stride, uint32_t in_w, uint
     GEO_CUDA(cudaMemcpyAsync(day, ys.data(), ys.size() * sizeof(Axis), cudaMemcpyHostToDevice, stream));
     dim3 b(32, 8);
     cubic_h_kernel<<<dim3((native.width + 31) / 32, (rows + 7) / 8), b, 0, stream>>>(
-        in, in_stride, dax, (int)native.width, (int)row_lo, (int)rows, H, status);
+        in, in_stride, (int)window.x, (int)window.y, dax, (int)native.width, (int)row_lo, (int)rows, H, status);
     float* target = mip ? nat : out;
     const size_t tstride = mip ? (size_t)native.width * 3 : out_stride;
     cubic_v_kernel<<<dim3((native.width + 31) / 32, (native.height + 7) / 8), b, 0, stream>>>(
@@ -350,7 +416,14 @@ re_status re_rotation_coefficients(double a, double* cosine, double* sine) {
 }
 
 re_status re_rotate(const float* in, size_t in_stride, uint32_t width, uint32_t height, double angle,
-                    re_rect output, uint32_t mip, float* out, size_t out_stride, void* stream_) {
+                    re_rect output, uint32_t mip, float* out, size_t out_stride, void* stream) {
+    return re_rotate_window(in, in_stride, {0, 0, width, height}, width, height, angle, output, mip, out, out_stride,
+                            stream);
+}
+
+re_status re_rotate_window(const float* in, size_t in_stride, re_rect window, uint32_t width, uint32_t height,
+                           double angle, re_rect output, uint32_t mip, float* out, size_t out_stride,
+                           void* stream_) {
     if (!width || !height) {
         set_last_error("rotation requires input and nonempty image bounds");
         return RE_INVALID_ARGUMENT;
@@ -372,9 +445,22 @@ re_status re_rotate(const float* in, size_t in_stride, uint32_t width, uint32_t 
         return RE_OUT_OF_RANGE;
     }
     if (!output.width || !output.height) return RE_OK;
-    if (!in || !out || in_stride < (size_t)width * 3 || out_stride < (size_t)output.width * 3) {
+    if (!in || !out || in_stride < (size_t)window.width * 3 || out_stride < (size_t)output.width * 3 ||
+        (uint64_t)window.x + window.width > width || (uint64_t)window.y + window.height > height) {
         set_last_error("invalid rotation buffers");
         return RE_INVALID_ARGUMENT;
+    }
+    if (window.x || window.y || window.width != width || window.height != height) {
+        // the taps of every native output pixel must lie inside the window (GeometryOps.cpp:99-111)
+        re_rect support;
+        re_status ss = rotate_support_host(p, native, support);
+        if (ss) return ss;
+        if (support.x < window.x || support.y < window.y ||
+            (uint64_t)support.x + support.width > (uint64_t)window.x + window.width ||
+            (uint64_t)support.y + support.height > (uint64_t)window.y + window.height) {
+            set_last_error("rotation input window does not cover the taps' support");
+            return RE_INVALID_ARGUMENT;
+        }
     }
     cudaStream_t stream = (cudaStream_t)stream_;
     const size_t nat_bytes = mip ? (size_t)native.width * native.height * 3 * sizeof(float) : 0;
@@ -388,7 +474,7 @@ re_status re_rotate(const float* in, size_t in_stride, uint32_t width, uint32_t 
     const size_t tstride = mip ? (size_t)native.width * 3 : out_stride;
     dim3 b(32, 8);
     rotate_kernel<<<dim3((native.width + 31) / 32, (native.height + 7) / 8), b, 0, stream>>>(
-        in, in_stride, p, (int)native.x, (int)native.y, (int)native.width, (int)native.height, target, tstride,
+        in, in_stride, (int)window.x, (int)window.y, p, (int)native.x, (int)native.y, (int)native.width, (int)native.height, target, tstride,
         status);
     GEO_CUDA(cudaGetLastError());
     if (mip) {

@@ -226,9 +226,12 @@ struct LsSmem {
     int n[LS_TH + 2 * LS_MAX_R][LS_TW];
 };
 
+// T = float (re_local_statistics) or double (re_local_statistics_f64, the
+// reference's LocalStatisticsTile precision).
+template <typename T>
 __global__ void __launch_bounds__(LS_THREADS)
 local_stats_kernel(const float* __restrict__ in, size_t in_stride, int width, int height, int r,
-                   float* __restrict__ mean_out, float* __restrict__ var_out, uint32_t* __restrict__ count_out) {
+                   T* __restrict__ mean_out, T* __restrict__ var_out, uint32_t* __restrict__ count_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LsSmem& S = *reinterpret_cast<LsSmem*>(smem_raw);
     const int x0 = blockIdx.x * LS_TW, y0 = blockIdx.y * LS_TH;
@@ -281,8 +284,8 @@ local_stats_kernel(const float* __restrict__ in, size_t in_stride, int width, in
             const double mean = a / n;
             double var = (b - a * mean) / n;
             if (var < 0) var = 0;
-            mean_out[o] = (float)(shift + mean);
-            var_out[o] = (float)var;
+            mean_out[o] = (T)(shift + mean);
+            var_out[o] = (T)var;
         }
         __syncthreads();
     }
@@ -304,6 +307,28 @@ struct Scratch {
             return RE_CUDA_ERROR;                                             \
         }                                                                     \
     } while (0)
+
+template <typename T>
+re_status local_statistics(const float* in, size_t in_stride, uint32_t width, uint32_t height, uint32_t radius,
+                           T* mean_out, T* var_out, uint32_t* count_out, void* stream_) {
+    if (radius > LS_MAX_R) {
+        set_last_error("local statistics radius must be in 0..32");
+        return RE_INVALID_ARGUMENT;
+    }
+    if (!width || !height || !in || !mean_out || !var_out || in_stride < (size_t)width * 3) {
+        set_last_error("spatial operation requires nonempty addressable bounds");
+        return RE_INVALID_ARGUMENT;
+    }
+    cudaStream_t stream = (cudaStream_t)stream_;
+    SP_CUDA(cudaFuncSetAttribute(local_stats_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(LsSmem)));
+    dim3 grid((width + LS_TW - 1) / LS_TW, (height + LS_TH - 1) / LS_TH);
+    local_stats_kernel<T><<<grid, LS_THREADS, sizeof(LsSmem), stream>>>(in, in_stride, (int)width, (int)height,
+                                                                         (int)radius, mean_out, var_out, count_out);
+    SP_CUDA(cudaGetLastError());
+    SP_CUDA(cudaStreamSynchronize(stream));
+    return RE_OK;
+}
 
 }  // namespace
 
@@ -362,28 +387,14 @@ re_status re_guided_filter(const float* in, size_t in_stride, float* out, size_t
 
 // SpatialOps.cpp:74-121 (radius extended to 32).
 re_status re_local_statistics(const float* in, size_t in_stride, uint32_t width, uint32_t height, uint32_t radius,
-                              float* mean_out, float* var_out, uint32_t* count_out, void* stream_) {
-    if (radius > LS_MAX_R) {
-        set_last_error("local statistics radius must be in 0..32");
-        return RE_INVALID_ARGUMENT;
-    }
-    if (!width || !height || !in || !mean_out || !var_out || in_stride < (size_t)width * 3) {
-        set_last_error("spatial operation requires nonempty addressable bounds");
-        return RE_INVALID_ARGUMENT;
-    }
-    cudaStream_t stream = (cudaStream_t)stream_;
-    static bool configured = false;
-    if (!configured) {
-        SP_CUDA(cudaFuncSetAttribute(local_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(LsSmem)));
-        configured = true;
-    }
-    dim3 grid((width + LS_TW - 1) / LS_TW, (height + LS_TH - 1) / LS_TH);
-    local_stats_kernel<<<grid, LS_THREADS, sizeof(LsSmem), stream>>>(in, in_stride, (int)width, (int)height,
-                                                                      (int)radius, mean_out, var_out, count_out);
-    SP_CUDA(cudaGetLastError());
-    SP_CUDA(cudaStreamSynchronize(stream));
-    return RE_OK;
+                              float* mean_out, float* var_out, uint32_t* count_out, void* stream) {
+    return local_statistics<float>(in, in_stride, width, height, radius, mean_out, var_out, count_out, stream);
+}
+
+re_status re_local_statistics_f64(const float* in, size_t in_stride, uint32_t width, uint32_t height,
+                                  uint32_t radius, double* mean_out, double* var_out, uint32_t* count_out,
+                                  void* stream) {
+    return local_statistics<double>(in, in_stride, width, height, radius, mean_out, var_out, count_out, stream);
 }
 
 }  // extern "C"

@@ -1,0 +1,628 @@
+// Test driver for the drop-in C++ surface (include/rawengine/*.hpp).
+//
+//   api_driver validate            host-only checks (no device work)
+//   api_driver render <dir>        renders the scenarios of <dir>/params.txt
+//
+// `render` reads the RAW and raster inputs written by the pytest side, renders
+// each scenario through the rawengine:: classes, writes <dir>/<name>.bin and
+// prints "OUT <name> <x> <y> <w> <h> <type>" lines; the pytest side compares
+// them with the oracle.  Behavioural checks (exceptions, descriptors, tile
+// assembly, scheduler order) are asserted here and reported as "CHECK <name>".
+// The checks mirror the reference's own core, spatial, geometry and scheduler
+// tests (tests/core_tests.cpp, spatial_ops_tests.cpp, rotate_tests.cpp,
+// cubic_resize_tests.cpp of tylermcm/librawops) on this path.
+#include <rawengine/GeometryOps.hpp>
+#include <rawengine/RawEngine.hpp>
+#include <rawengine/SpatialOps.hpp>
+#include <rawengine/TileScheduler.hpp>
+#include <rawengine/ToneOps.hpp>
+
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+
+using namespace rawengine;
+
+namespace {
+
+int failures = 0;
+
+void check(bool ok, const std::string& name) {
+    std::cout << (ok ? "CHECK " : "FAIL ") << name << std::endl;
+    if (!ok) ++failures;
+}
+
+template <class E, class F>
+void expect_throw(F&& f, const std::string& name) {
+    try {
+        f();
+    } catch (const E&) {
+        check(true, name);
+        return;
+    } catch (const std::exception& e) {
+        std::cout << "  (threw " << e.what() << ")" << std::endl;
+    }
+    check(false, name);
+}
+
+std::map<std::string, std::vector<double>> read_params(const std::string& path) {
+    std::map<std::string, std::vector<double>> out;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ss(line);
+        std::string key;
+        if (!(ss >> key)) continue;
+        double v;
+        while (ss >> v) out[key].push_back(v);
+    }
+    return out;
+}
+
+template <class T>
+std::vector<T> read_file(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
+    in.seekg(0, std::ios::end);
+    const size_t bytes = (size_t)in.tellg();
+    in.seekg(0);
+    std::vector<T> v(bytes / sizeof(T));
+    in.read(reinterpret_cast<char*>(v.data()), (std::streamsize)bytes);
+    return v;
+}
+
+template <class T>
+void emit(const std::string& dir, const std::string& name, Rect r, const std::vector<T>& data, const char* type) {
+    std::ofstream out(dir + "/" + name + ".bin", std::ios::binary);
+    out.write(reinterpret_cast<const char*>(data.data()), (std::streamsize)(data.size() * sizeof(T)));
+    std::cout << "OUT " << name << " " << r.x << " " << r.y << " " << r.width << " " << r.height << " " << type
+              << std::endl;
+}
+
+Rect rect_of(const std::vector<double>& v, size_t at = 0) {
+    return {(uint32_t)v[at], (uint32_t)v[at + 1], (uint32_t)v[at + 2], (uint32_t)v[at + 3]};
+}
+
+bool bit_equal(const std::vector<float>& a, const std::vector<float>& b) {
+    return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(float)) == 0;
+}
+
+// A node of another library: constant camera-linear RGB.
+class ConstantCameraNode final : public Node {
+public:
+    explicit ConstantCameraNode(std::array<float, 3> px) : px_(px) {}
+    ImageDescriptor output_descriptor() const noexcept override { return ImageDescriptor::camera_linear(); }
+    Tile render(Rect b) const override {
+        Tile t{b, std::vector<float>((size_t)b.width * b.height * 3)};
+        for (size_t i = 0; i < t.rgb.size(); i += 3) std::copy(px_.begin(), px_.end(), t.rgb.begin() + i);
+        return t;
+    }
+private:
+    std::array<float, 3> px_;
+};
+
+// A node that returns a tile with the wrong descriptor.
+class WrongDescriptorNode final : public Node {
+public:
+    ImageDescriptor output_descriptor() const noexcept override { return ImageDescriptor::camera_linear(); }
+    Tile render(Rect b) const override {
+        return {b, std::vector<float>((size_t)b.width * b.height * 3), ImageDescriptor::tone_mapped()};
+    }
+};
+
+// Scene-linear node whose render blocks until released, recording the order
+// in which requests reach it (scheduler tests).
+struct Gate {
+    std::mutex m;
+    std::condition_variable cv;
+    bool open = false;
+    int entered = 0;
+    std::vector<int> order;
+};
+class GatedNode final : public Node {
+public:
+    GatedNode(Gate* g, int id) : g_(g), id_(id) {}
+    ImageDescriptor output_descriptor() const noexcept override {
+        return ImageDescriptor::scene_linear(WorkingSpace::LinearProPhotoD50);
+    }
+    Tile render(Rect b) const override {
+        std::unique_lock<std::mutex> lock(g_->m);
+        ++g_->entered;
+        g_->order.push_back(id_);
+        g_->cv.notify_all();
+        g_->cv.wait_for(lock, std::chrono::seconds(20), [&] { return g_->open; });
+        return {b, std::vector<float>((size_t)b.width * b.height * 3, (float)id_), output_descriptor()};
+    }
+private:
+    Gate* g_;
+    int id_;
+};
+
+RawImage make_raw(const std::map<std::string, std::vector<double>>& P, const std::string& dir) {
+    const auto& m = P.at("raw_meta");
+    RawMetadata md;
+    md.width = (uint32_t)m[0];
+    md.height = (uint32_t)m[1];
+    md.row_stride_samples = (uint32_t)m[2];
+    md.pattern = (BayerPattern)(int)m[3];
+    md.cfa_phase_x = (uint8_t)m[4];
+    md.cfa_phase_y = (uint8_t)m[5];
+    md.active_area = rect_of(m, 6);
+    for (int i = 0; i < 4; ++i) {
+        md.black_levels[i] = (uint16_t)m[10 + i];
+        md.white_levels[i] = (uint16_t)m[14 + i];
+    }
+    return RawImage(md, read_file<uint16_t>(dir + "/raw.u16"));
+}
+
+CameraColorTransform camera(const std::map<std::string, std::vector<double>>& P, WorkingSpace target) {
+    CameraColorTransform t;
+    const auto& c = P.at("camera");
+    std::copy(c.begin(), c.begin() + 9, t.camera_to_xyz_d50.begin());
+    t.target = target;
+    return t;
+}
+
+// ------------------------------------------------------------------ render
+
+int run_render(const std::string& dir) {
+    const auto P = read_params(dir + "/params.txt");
+    const RawImage raw = make_raw(P, dir);
+    const Rect area = raw.metadata().active_area;
+    Renderer renderer;
+
+    // 1. ImageGraph legacy bounded output, bilinear, whole active area.
+    GraphRecipe legacy;
+    {
+        const auto& g = P.at("legacy");
+        legacy.red_gain = (float)g[0];
+        legacy.green_gain = (float)g[1];
+        legacy.blue_gain = (float)g[2];
+        legacy.exposure_stops = (float)g[3];
+        legacy.tone_shoulder = (float)g[4];
+        legacy.tone_gamma = (float)g[5];
+    }
+    ImageGraph graph(raw, legacy);
+    check(graph.output().output_descriptor() == ImageDescriptor::bounded_output(), "legacy_descriptor");
+    const Tile full = renderer.render_image(graph, area, 16);
+    check(full.descriptor == ImageDescriptor::bounded_output(), "legacy_tile_descriptor");
+    emit(dir, "legacy", full.bounds, full.rgb, "f32");
+
+    // 2. render_tiles in row-major order, tiles bit-equal to the whole render.
+    {
+        const Rect vp{area.x + 3, area.y + 2, area.width - 5, area.height - 4};
+        std::vector<Rect> order;
+        bool same = true;
+        renderer.render_tiles(graph, vp, [&](const Tile& t) {
+            order.push_back(t.bounds);
+            for (uint32_t row = 0; row < t.bounds.height; ++row)
+                same &= std::memcmp(t.rgb.data() + (size_t)row * t.bounds.width * 3,
+                                    full.rgb.data() + ((size_t)(t.bounds.y - area.y + row) * area.width +
+                                                       (t.bounds.x - area.x)) * 3,
+                                    (size_t)t.bounds.width * 3 * sizeof(float)) == 0;
+        }, 7);
+        bool row_major = !order.empty() && order.front().x == vp.x && order.front().y == vp.y;
+        for (size_t i = 1; i < order.size(); ++i)
+            row_major &= order[i].y > order[i - 1].y || (order[i].y == order[i - 1].y && order[i].x > order[i - 1].x);
+        check(same, "render_tiles_equal_whole");
+        check(row_major, "render_tiles_row_major");
+        const auto roi = renderer.render_roi(graph, vp, 5);
+        const Tile img = renderer.render_image(graph, vp, 1000);
+        check(bit_equal(roi, img.rgb), "render_roi_equal_image");
+    }
+
+    // 3/4. Menon sRGB chain at mip 1 (Preview) and native.
+    auto menon = std::make_shared<RawUnpackNode>(raw, RawDemosaicIdentity{"rawengine.menon_base", 1});
+    const auto& s = P.at("srgb");
+    auto wb = std::make_shared<WhiteBalanceNode>(menon, (float)s[0], (float)s[1], (float)s[2]);
+    auto ex = std::make_shared<ExposureNode>(wb, (float)s[3]);
+    auto ctw = std::make_shared<CameraToWorkingNode>(ex, camera(P, WorkingSpace::LinearProPhotoD50), area);
+    auto to_srgb = std::make_shared<WorkingToSrgbNode>(ctw);
+    auto tone = std::make_shared<ToneCurveNode>(to_srgb, (float)s[4], (float)s[5]);
+    auto enc = std::make_shared<SrgbEncodeNode>(tone);
+    check(enc->supports_level({1, RenderQuality::Preview}), "srgb_supports_mip1");
+    check(!enc->supports_level({1, RenderQuality::Final}), "srgb_rejects_mip1_final");
+    {
+        const Rect reduced{0, 0, (area.width + 1) / 2, (area.height + 1) / 2};
+        const Tile t = renderer.render_image(*enc, area, RenderRequest{reduced, 9, {1, RenderQuality::Preview}});
+        check(t.descriptor == ImageDescriptor::srgb_output(), "srgb_descriptor");
+        emit(dir, "srgb_mip1", t.bounds, t.rgb, "f32");
+        const Rect vp = rect_of(P.at("srgb_native_vp"));
+        const Tile n = renderer.render_image(*enc, area, vp, 64);
+        emit(dir, "srgb_native", n.bounds, n.rgb, "f32");
+        // the node's own render equals the renderer's result
+        check(bit_equal(enc->render(vp).rgb, n.rgb), "node_render_equal_renderer");
+    }
+
+    // 5. Guided filter over a working-space chain, then extended curves.
+    {
+        const auto& gp = P.at("gf");
+        auto ctw2 = std::make_shared<CameraToWorkingNode>(wb, camera(P, WorkingSpace::LinearProPhotoD50), area);
+        auto gf = std::make_shared<WorkingYGuidedFilterNode>(
+            ctw2, area, WorkingYGuidedFilterSettings{(uint32_t)gp[0], gp[1]});
+        ExtendedCurvesSettings cs;
+        cs.interpolation = CurveInterpolation::ShapePreservingCubic;
+        const auto& k = P.at("curve_master");
+        cs.master.knots.clear();
+        for (size_t i = 0; i + 1 < k.size(); i += 2) cs.master.knots.push_back({k[i], k[i + 1]});
+        auto curves = std::make_shared<ExtendedCurvesNode>(gf, cs);
+        const Rect vp = rect_of(P.at("gf_vp"));
+        const Tile t = renderer.render_image(*curves, area, vp, 32);
+        emit(dir, "gf_curves", t.bounds, t.rgb, "f32");
+        // the guided filter alone, through working_y_guided_filter_rgb on a host tile
+        const Rect needed = working_y_guided_filter_region(vp, area, (uint32_t)gp[0]);
+        const Tile in = ctw2->render(needed);
+        const Tile host = working_y_guided_filter_rgb(in, vp, area, {(uint32_t)gp[0], gp[1]});
+        const Tile node = gf->render(vp);
+        check(bit_equal(host.rgb, node.rgb), "gf_function_equal_node");
+        emit(dir, "gf_only", node.bounds, node.rgb, "f32");
+        // local statistics of the working image, tile by tile
+        const Rect lvp = rect_of(P.at("ls_vp"));
+        const uint32_t radius = (uint32_t)P.at("ls_radius")[0];
+        std::vector<double> mean((size_t)lvp.width * lvp.height * 3), var(mean.size());
+        std::vector<uint32_t> count(mean.size());
+        analyze_local_rgb(*ctw2, area, RenderRequest{lvp, 11, {}}, [&](const LocalStatisticsTile& t) {
+            for (uint32_t row = 0; row < t.bounds.height; ++row)
+                for (uint32_t col = 0; col < t.bounds.width * 3; ++col) {
+                    const size_t d = (size_t)(t.bounds.y - lvp.y + row) * lvp.width * 3 + (t.bounds.x - lvp.x) * 3 + col;
+                    const size_t s2 = (size_t)row * t.bounds.width * 3 + col;
+                    mean[d] = t.mean[s2];
+                    var[d] = t.variance[s2];
+                    count[d] = t.finite_count[s2];
+                }
+        }, radius);
+        emit(dir, "ls_mean", lvp, mean, "f64");
+        emit(dir, "ls_var", lvp, var, "f64");
+        emit(dir, "ls_count", lvp, count, "u32");
+    }
+
+    // 6/7. Cubic resize and rotation of a Rec.2020 working image.
+    {
+        auto bil_wb = std::make_shared<WhiteBalanceNode>(std::make_shared<RawUnpackNode>(raw), (float)s[0],
+                                                         (float)s[1], (float)s[2]);
+        auto rec = std::make_shared<CameraToWorkingNode>(bil_wb, camera(P, WorkingSpace::LinearRec2020D65), area);
+        const auto& cp = P.at("cubic");
+        auto cubic = std::make_shared<CubicResizeNode>(rec, area, CubicResizeSettings{(uint32_t)cp[0], (uint32_t)cp[1]});
+        const Rect cvp = rect_of(P.at("cubic_vp"));
+        const Tile c = renderer.render_image(*cubic, cubic->output_bounds(), cvp, 16);
+        emit(dir, "cubic", c.bounds, c.rgb, "f32");
+        const Rect cvp1 = rect_of(P.at("cubic_vp_mip1"));
+        const Tile c1 = renderer.render_image(*cubic, cubic->output_bounds(),
+                                              RenderRequest{cvp1, 16, {1, RenderQuality::Preview}});
+        emit(dir, "cubic_mip1", c1.bounds, c1.rgb, "f32");
+        auto rot = std::make_shared<RotateNode>(rec, area, RotateSettings{P.at("rotate_angle")[0]});
+        const Rect rvp = rect_of(P.at("rotate_vp"));
+        const Tile r = renderer.render_image(*rot, rot->output_bounds(), rvp, 16);
+        emit(dir, "rotate", r.bounds, r.rgb, "f32");
+        const Rect rvp2 = rect_of(P.at("rotate_vp_mip2"));
+        const Tile r2 = renderer.render_image(*rot, rot->output_bounds(),
+                                              RenderRequest{rvp2, 16, {2, RenderQuality::Preview}});
+        emit(dir, "rotate_mip2", r2.bounds, r2.rgb, "f32");
+        const Tile rec_full = rec->render(area);
+        emit(dir, "rec2020_native", rec_full.bounds, rec_full.rgb, "f32");
+    }
+
+    // 8. Raster graph, sRGB preview, mip 2 and native.
+    {
+        const auto& rm = P.at("raster_meta");
+        RasterMetadata md;
+        md.width = (uint32_t)rm[0];
+        md.height = (uint32_t)rm[1];
+        md.working_space = (WorkingSpace)(int)rm[2];
+        RasterImage img(md, read_file<float>(dir + "/raster.f32"));
+        GraphRecipe rr;
+        rr.exposure_stops = (float)P.at("raster_recipe")[0];
+        rr.tone_gamma = (float)P.at("raster_recipe")[1];
+        rr.output_mode = OutputMode::SrgbPreview;
+        ImageGraph rg(img, rr);
+        const Rect red{0, 0, (md.width + 3) / 4, (md.height + 3) / 4};
+        const Tile t = renderer.render_image(rg, RenderRequest{red, 8, {2, RenderQuality::Preview}});
+        emit(dir, "raster_mip2", t.bounds, t.rgb, "f32");
+        const Tile n = renderer.render_image(rg, Rect{0, 0, md.width, md.height}, 13);
+        emit(dir, "raster_native", n.bounds, n.rgb, "f32");
+        GraphRecipe bad;
+        bad.red_gain = 2.0f;
+        expect_throw<std::invalid_argument>([&] { ImageGraph x(img, bad); }, "raster_rejects_raw_controls");
+    }
+
+    // 9. Nodes of another library, uploaded into the device chain.
+    {
+        auto c = std::make_shared<ConstantCameraNode>(std::array<float, 3>{0.25f, 0.5f, 0.75f});
+        auto g = std::make_shared<WhiteBalanceNode>(c, 2.0f, 1.0f, 0.5f);
+        const Tile t = g->render({0, 0, 3, 2});
+        bool ok = t.rgb.size() == 18;
+        for (size_t i = 0; ok && i < t.rgb.size(); i += 3)
+            ok = t.rgb[i] == 0.25f * 2.0f && t.rgb[i + 1] == 0.5f && t.rgb[i + 2] == 0.75f * 0.5f;
+        check(ok, "foreign_node_uploaded");
+        auto w = std::make_shared<WhiteBalanceNode>(std::make_shared<WrongDescriptorNode>(), 1.0f, 1.0f, 1.0f);
+        expect_throw<std::domain_error>([&] { w->render({0, 0, 2, 2}); }, "foreign_wrong_descriptor_domain_error");
+    }
+
+    // 10. Errors and cancellation.
+    {
+        expect_throw<std::out_of_range>([&] { renderer.render_image(graph, Rect{0, 0, area.width + area.x + 1, 1}); },
+                                        "viewport_out_of_range");
+        expect_throw<std::invalid_argument>(
+            [&] { renderer.render_image(graph, RenderRequest{{0, 0, 2, 2}, 16, {1, RenderQuality::Preview}}); },
+            "legacy_graph_rejects_mip1");
+        expect_throw<std::out_of_range>([&] { (void)RawUnpackNode(raw).render({0, 0, 1, 1}); },
+                                        "inactive_area_out_of_range");
+        CancellationToken cancelled;
+        cancelled.cancel();
+        expect_throw<RenderCancelled>([&] { renderer.render_image(graph, area, 16, &cancelled); },
+                                      "pre_cancelled_render");
+        CancellationToken mid;
+        int tiles = 0;
+        expect_throw<RenderCancelled>([&] {
+            renderer.render_tiles(graph, area, [&](const Tile&) {
+                if (++tiles == 2) mid.cancel();
+            }, 8, &mid);
+        }, "cancel_between_tiles");
+        check(tiles == 2, "cancel_stops_after_current_tile");
+    }
+
+    // 11. TileScheduler: priority order, FIFO, pending budget, supersession,
+    // destruction.
+    {
+        const Rect b{0, 0, 4, 4};
+        auto open = [](Gate& g) {
+            {
+                std::lock_guard<std::mutex> lock(g.m);
+                g.open = true;
+            }
+            g.cv.notify_all();
+        };
+        auto wait_entered = [](Gate& g, int n) {
+            std::unique_lock<std::mutex> lock(g.m);
+            return g.cv.wait_for(lock, std::chrono::seconds(10), [&] { return g.entered >= n; });
+        };
+        auto node = [](Gate& g, int id) { return std::make_shared<GatedNode>(&g, id); };
+        {
+            Gate gate;
+            TileScheduler sched(1, 2);
+            auto busy = sched.submit(node(gate, 0), b, b, RenderPriority::Normal, 4);
+            check(wait_entered(gate, 1), "scheduler_started");
+            auto low = sched.submit(node(gate, 1), b, b, RenderPriority::Background, 4);
+            auto high = sched.submit(node(gate, 2), b, b, RenderPriority::Interactive, 4);
+            expect_throw<std::length_error>([&] { sched.submit(node(gate, 3), b, b, RenderPriority::Normal, 4); },
+                                            "scheduler_pending_budget");
+            open(gate);
+            const Tile t0 = busy.get(), t2 = high.get(), t1 = low.get();
+            check(t0.rgb[0] == 0.0f && t2.rgb[0] == 2.0f && t1.rgb[0] == 1.0f, "scheduler_results");
+            check(gate.order == std::vector<int>({0, 2, 1}), "scheduler_priority_order");
+        }
+        {
+            Gate gate;
+            TileScheduler sched(1, 3);
+            auto busy = sched.submit(node(gate, 10), b, b, RenderPriority::Interactive, 4);
+            check(wait_entered(gate, 1), "scheduler_started_2");
+            auto a = sched.submit(node(gate, 11), b, b, RenderPriority::Normal, 4);
+            auto c = sched.submit(node(gate, 12), b, b, RenderPriority::Normal, 4);
+            auto v1 = sched.submit_latest("view", node(gate, 13), b, b, RenderPriority::Normal, 4);
+            // the budget counts the queued request this one replaces
+            auto v2 = sched.submit_latest("view", node(gate, 14), b, b, RenderPriority::Normal, 4);
+            open(gate);
+            expect_throw<RenderCancelled>([&] { v1.get(); }, "superseded_queued_cancelled");
+            (void)busy.get();
+            (void)a.get();
+            (void)c.get();
+            check(v2.get().rgb[0] == 14.0f, "latest_request_renders");
+            check(gate.order == std::vector<int>({10, 11, 12, 14}), "scheduler_fifo_within_priority");
+        }
+        {
+            Gate gate;
+            TileScheduler sched(1, 2);
+            auto first = sched.submit_latest("run", node(gate, 20), b, b, RenderPriority::Interactive, 4);
+            check(wait_entered(gate, 1), "scheduler_started_3");
+            auto second = sched.submit_latest("run", node(gate, 21), b, b, RenderPriority::Interactive, 4);
+            open(gate);
+            expect_throw<RenderCancelled>([&] { first.get(); }, "superseded_running_cancelled");
+            check(second.get().rgb[0] == 21.0f, "superseding_request_renders");
+        }
+        {
+            Gate gate;
+            auto sched = std::make_unique<TileScheduler>(1, 2);
+            auto busy = sched->submit(node(gate, 30), b, b, RenderPriority::Normal, 4);
+            check(wait_entered(gate, 1), "scheduler_started_4");
+            auto queued = sched->submit(node(gate, 31), b, b, RenderPriority::Normal, 4);
+            std::thread closer([&] { sched.reset(); });
+            std::this_thread::sleep_for(std::chrono::milliseconds(300));
+            open(gate);
+            closer.join();
+            expect_throw<RenderCancelled>([&] { queued.get(); }, "destruction_cancels_pending");
+            check(busy.get().rgb[0] == 30.0f, "destruction_waits_for_running");
+        }
+        // device renders through the scheduler equal direct renders
+        {
+            TileScheduler sched(2, 8);
+            auto out = graph.output_node();
+            auto f1 = sched.submit(out, area, area, RenderPriority::Normal, 64);
+            auto f2 = sched.submit(enc, area, RenderRequest{{0, 0, 8, 6}, 4, {1, RenderQuality::Preview}});
+            check(bit_equal(f1.get().rgb, full.rgb), "scheduled_equals_direct");
+            check(bit_equal(f2.get().rgb,
+                            renderer.render_image(*enc, area, RenderRequest{{0, 0, 8, 6}, 4, {1, RenderQuality::Preview}})
+                                .rgb),
+                  "scheduled_mip1_equals_direct");
+            expect_throw<std::invalid_argument>(
+                [&] { sched.submit(out, area, Rect{0, 0, 1, 1}, RenderPriority::Normal, 0); },
+                "scheduler_rejects_zero_tile");
+        }
+    }
+    return failures ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- validate
+
+void region(const std::string& name, Rect r) {
+    std::cout << "REGION " << name << " " << r.x << " " << r.y << " " << r.width << " " << r.height << std::endl;
+}
+
+int run_validate() {
+    RawMetadata md;
+    md.width = 40;
+    md.height = 30;
+    md.active_area = {4, 2, 32, 26};
+    const RawImage raw(md, std::vector<uint16_t>(40 * 30, 1000));
+    auto bil = std::make_shared<RawUnpackNode>(raw);
+    auto menon = std::make_shared<RawUnpackNode>(raw, RawDemosaicIdentity{"rawengine.menon_base", 1});
+    const Rect area = md.active_area;
+
+    // metadata and demosaic identity
+    {
+        RawMetadata bad = md;
+        bad.row_stride_samples = 39;
+        expect_throw<std::invalid_argument>([&] { (void)RawImage(bad, std::vector<uint16_t>(39 * 30)); },
+                                            "stride_below_width");
+        expect_throw<std::invalid_argument>([&] { (void)RawImage(md, std::vector<uint16_t>(10)); }, "sample_count");
+        RawMetadata outside = md;
+        outside.active_area = {30, 0, 20, 10};
+        expect_throw<std::invalid_argument>([&] { (void)RawImage(outside, std::vector<uint16_t>(40 * 30)); },
+                                            "active_area_outside");
+        expect_throw<std::invalid_argument>(
+            [&] { (void)RawUnpackNode(raw, RawDemosaicIdentity{"rawengine.menon_base", 2}); }, "menon_version_2");
+        expect_throw<std::invalid_argument>([&] { (void)RawUnpackNode(raw, RawDemosaicIdentity{"ahd", 1}); },
+                                            "unknown_demosaic");
+        RawMetadata packed;
+        packed.width = 6;
+        packed.height = 4;
+        const RawImage p(packed, std::vector<uint16_t>(24));
+        check(p.metadata().row_stride_samples == 6 && p.metadata().active_area.width == 6 &&
+                  p.metadata().active_area.height == 4,
+              "metadata_normalized");
+    }
+    // regions (compared with the oracle on the pytest side)
+    region("bilinear_input", bil->input_region({4, 2, 5, 5}, area));
+    region("menon_input", menon->input_region({10, 9, 7, 6}, area));
+    region("menon_input_edge", menon->input_region({33, 25, 3, 3}, area));
+    expect_throw<std::invalid_argument>([&] { bil->input_region({4, 2, 5, 5}, {0, 0, 40, 30}); },
+                                        "raw_region_bounds_differ");
+    // point node validation and descriptors
+    {
+        expect_throw<std::invalid_argument>([&] { (void)WhiteBalanceNode(bil, 0.0f, 1.0f, 1.0f); }, "wb_zero_gain");
+        expect_throw<std::invalid_argument>([&] { (void)WhiteBalanceNode(bil, 1.0f, 70000.0f, 1.0f); }, "wb_large_gain");
+        expect_throw<std::invalid_argument>([&] { (void)ExposureNode(bil, 33.0f); }, "exposure_range");
+        auto tone = std::make_shared<ToneCurveNode>(bil, 0.25f, 1.0f);
+        check(tone->output_descriptor() == ImageDescriptor::tone_mapped(), "tone_on_camera_descriptor");
+        expect_throw<std::invalid_argument>([&] { (void)ExposureNode(tone, 1.0f); }, "exposure_rejects_tone_mapped");
+        expect_throw<std::invalid_argument>([&] { (void)ToneCurveNode(bil, 0.25f, 0.0f); }, "tone_zero_gamma");
+        auto clip = std::make_shared<OutputClipNode>(tone);
+        check(clip->output_descriptor() == ImageDescriptor::bounded_output(), "clip_descriptor");
+        expect_throw<std::invalid_argument>([&] { (void)OutputClipNode(bil); }, "clip_requires_tone_mapped");
+        expect_throw<std::invalid_argument>([&] { (void)SrgbEncodeNode(tone); }, "encode_requires_display_linear");
+        CameraColorTransform singular{{1, 0, 0, 1, 0, 0, 0, 0, 1}, WorkingSpace::LinearProPhotoD50};
+        expect_throw<std::invalid_argument>([&] { (void)CameraToWorkingNode(bil, singular); }, "singular_camera_matrix");
+        CameraColorTransform id{{1, 0, 0, 0, 1, 0, 0, 0, 1}, WorkingSpace::LinearRec2020D65};
+        auto ctw = std::make_shared<CameraToWorkingNode>(bil, id, area);
+        check(ctw->output_descriptor() == ImageDescriptor::scene_linear(WorkingSpace::LinearRec2020D65),
+              "ctw_descriptor");
+        expect_throw<std::invalid_argument>([&] { (void)CameraToWorkingNode(ctw, id); }, "ctw_requires_camera_linear");
+        expect_throw<std::invalid_argument>([&] { (void)CameraToWorkingNode(bil, id, Rect{1, 1, 0, 0}); },
+                                            "ctw_bad_preview_bounds");
+        region("ctw_mip1", ctw->input_region_level({3, 2, 6, 5}, area, {1, RenderQuality::Preview}));
+        region("ctw_mip2_edge", ctw->input_region_level({6, 4, 2, 3}, area, {2, RenderQuality::Preview}));
+        check(!bil->supports_level({1, RenderQuality::Preview}) && ctw->supports_level({1, RenderQuality::Preview}) &&
+                  !ctw->supports_level({3, RenderQuality::Preview}) && !ctw->supports_level({1, RenderQuality::Final}),
+              "ctw_levels");
+        auto srgb = std::make_shared<WorkingToSrgbNode>(ctw);
+        check(srgb->output_descriptor() == ImageDescriptor::linear_srgb(), "working_to_srgb_descriptor");
+        auto dl = std::make_shared<ToneCurveNode>(srgb, 0.25f, 2.2f);
+        check(dl->output_descriptor() == ImageDescriptor::display_linear_srgb(), "tone_on_srgb_descriptor");
+        check(std::make_shared<SrgbEncodeNode>(dl)->output_descriptor() == ImageDescriptor::srgb_output(),
+              "encode_descriptor");
+        auto conv = std::make_shared<WorkingSpaceConvertNode>(ctw, WorkingSpace::LinearRec2020D65);
+        check(conv->identity(), "convert_identity");
+        expect_throw<std::invalid_argument>([&] { (void)WorkingSpaceConvertNode(bil, WorkingSpace::LinearProPhotoD50); },
+                                            "convert_requires_scene_linear");
+        // spatial and geometry regions
+        region("gf_region", working_y_guided_filter_region({10, 8, 6, 5}, area, 3));
+        region("gf_region_edge", working_y_guided_filter_region({4, 2, 3, 3}, area, 2));
+        region("ls_region", local_statistics_region({10, 8, 6, 5}, area, 4));
+        expect_throw<std::invalid_argument>([&] { local_statistics_region({10, 8, 6, 5}, area, 9); }, "ls_radius_9");
+        expect_throw<std::out_of_range>([&] { local_statistics_region({0, 0, 6, 5}, area, 1); }, "ls_outside");
+        expect_throw<std::invalid_argument>(
+            [&] { (void)WorkingYGuidedFilterNode(ctw, area, WorkingYGuidedFilterSettings{9, 0.01}); }, "gf_radius_9");
+        expect_throw<std::invalid_argument>(
+            [&] { (void)WorkingYGuidedFilterNode(ctw, area, WorkingYGuidedFilterSettings{2, 0.0}); }, "gf_epsilon_0");
+        expect_throw<std::invalid_argument>([&] { (void)WorkingYGuidedFilterNode(bil, area); }, "gf_requires_scene_linear");
+        auto gf = std::make_shared<WorkingYGuidedFilterNode>(ctw, area, WorkingYGuidedFilterSettings{2, 0.01});
+        region("gf_node_mip1", gf->input_region_level({2, 3, 4, 4}, Rect{0, 0, 16, 13}, {1, RenderQuality::Preview}));
+        auto cubic = std::make_shared<CubicResizeNode>(ctw, area, CubicResizeSettings{20, 17});
+        region("cubic_support", cubic->input_region({3, 4, 6, 5}, area));
+        region("cubic_support_mip1", cubic->input_region_level({1, 2, 4, 3}, area, {1, RenderQuality::Preview}));
+        expect_throw<std::invalid_argument>([&] { (void)CubicResizeNode(ctw, area, CubicResizeSettings{7, 17}); },
+                                            "cubic_shrink_over_4");
+        auto rot = std::make_shared<RotateNode>(ctw, area, RotateSettings{23.5});
+        region("rotate_support", rot->input_region({5, 6, 7, 4}, area));
+        region("rotate_support_mip2", rot->input_region_level({1, 1, 3, 2}, area, {2, RenderQuality::Preview}));
+        expect_throw<std::invalid_argument>([&] { (void)RotateNode(ctw, area, RotateSettings{190}); }, "rotate_angle");
+        expect_throw<std::out_of_range>([&] { rot->input_region({30, 0, 5, 5}, area); }, "rotate_outside");
+    }
+    // graphs
+    {
+        GraphRecipe icc;
+        icc.output_mode = OutputMode::IccDisplay;
+        expect_throw<std::invalid_argument>([&] { (void)ImageGraph(raw, icc); }, "icc_output_unavailable");
+        GraphRecipe preview;
+        preview.output_mode = OutputMode::SrgbPreview;
+        preview.camera_color = CameraColorTransform{{0.6, 0.3, 0.1, 0.25, 0.7, 0.05, 0.02, 0.1, 0.8},
+                                                    WorkingSpace::LinearProPhotoD50};
+        ImageGraph g(raw, preview);
+        check(g.output().output_descriptor() == ImageDescriptor::srgb_output() &&
+                  g.output().supports_level({1, RenderQuality::Preview}) &&
+                  g.output().supports_level({2, RenderQuality::Preview}),
+              "preview_graph_levels");
+        ImageGraph legacy(raw);
+        check(!legacy.output().supports_level({1, RenderQuality::Preview}), "legacy_graph_native_only");
+        expect_throw<std::logic_error>(
+            [&] {
+                ImageGraph r(std::make_shared<CameraToWorkingNode>(
+                                 bil, CameraColorTransform{{1, 0, 0, 0, 1, 0, 0, 0, 1}, WorkingSpace::LinearProPhotoD50}),
+                             area);
+                (void)r.image();
+            },
+            "node_graph_has_no_raw_image");
+    }
+    // scheduler argument checks (no work is queued)
+    {
+        expect_throw<std::invalid_argument>([&] { (void)TileScheduler(0, 4); }, "scheduler_zero_workers");
+        expect_throw<std::invalid_argument>([&] { (void)TileScheduler(65, 4); }, "scheduler_65_workers");
+        expect_throw<std::invalid_argument>([&] { (void)TileScheduler(1, 0); }, "scheduler_zero_budget");
+        TileScheduler sched(1, 1);
+        expect_throw<std::invalid_argument>([&] { sched.submit(bil, area, Rect{0, 0, 2, 2}); },
+                                            "scheduler_viewport_outside");
+        expect_throw<std::invalid_argument>([&] { sched.submit(nullptr, area, area); }, "scheduler_null_node");
+        expect_throw<std::invalid_argument>([&] { sched.submit_latest("", bil, area, area); },
+                                            "scheduler_empty_group");
+        expect_throw<std::invalid_argument>(
+            [&] { sched.submit(bil, area, RenderRequest{{0, 0, 2, 2}, 16, {1, RenderQuality::Preview}}); },
+            "scheduler_unsupported_level");
+    }
+    return failures ? 1 : 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::cerr << "usage: api_driver validate | render <dir>\n";
+        return 2;
+    }
+    const std::string mode = argv[1];
+    try {
+        if (mode == "render" && argc == 3) return run_render(argv[2]);
+        if (mode == "validate") return run_validate();
+    } catch (const std::exception& e) {
+        std::cout << "FAIL uncaught " << e.what() << std::endl;
+        return 1;
+    }
+    std::cerr << "unknown mode\n";
+    return 2;
+}
