@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -47,11 +48,12 @@ def _peaks():
 
 def _traffic_from_profile():
     """DRAM bytes per launch of the render kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "menon_srgb_24mp.json")
+    path = os.path.join(ROOT, "profiles", "menon_kernel_24mp_srgb.md")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    except Exception:
+            m = re.search(r"DRAM traffic of one launch \(read \+ write\): (\d+) bytes", f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
         return None
 
 
