@@ -4,8 +4,12 @@ Workload: the 24 MP Menon -> sRGB render (6016x4016 BGGR sensor, stride 6080,
 active 6000x4000 at (16,8), per-site black (510,512,511,513), white 15800;
 Menon demosaic, WB (1.9,1.0,1.5), 3x3 calibration, 16-knot monotone tone
 curve, working->sRGB, clip + sRGB encode; float32 RGB out).  One step renders
-the whole active area in one fused launch.  Inputs (48.8 MB) and outputs
-(288 MB) exceed the 126 MB L2, so no explicit flush is needed between steps.
+the frame as the reference's renderer cuts it -- 96 tile requests of 512 with
+edge remainders -- drained by one persistent batched launch.  The same
+requests launched one by one (per tile), the whole frame as one launch, and the
+mixed batch (16 RAWs, ~3,000 tiles at mip 0/1/2, batched vs per request) are
+reported beside it.  Inputs (48.8 MB) and outputs (288 MB) exceed the 126 MB
+L2, so no explicit flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -216,17 +220,23 @@ def run_ours(args, rank, world, local_rank):
     img = render.Image(meta, samples_dev)
     pipe = workloads.pipeline_for(w)
     out = torch.empty((ah, aw, 3), dtype=torch.float32, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(device=dev)
+    # the frame as the reference renders it: tile-size requests in row-major
+    # order (RawEngine.cpp:1390-1412), each writing its part of the frame
+    tiles = render.plan_tiles(w.active, w.tile)
+    requests = [(img, pipe, t, 0, render.FINAL, out[t[1] - ay:t[1] - ay + t[3], t[0] - ax:t[0] - ax + t[2]])
+                for t in tiles]
+    batch = render.Batch().plan(requests)
+    with torch.cuda.stream(stream):
+        tuned = batch.autotune(reps=3, stream=stream)
 
     def step():
-        render.render_async(img, pipe, w.active, out, status, stream=stream)
+        batch.launch(stream=stream)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
-    torch.cuda.synchronize()
-    render.status_from_device(int(status.item()))
+    batch.status(stream=stream)
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -249,7 +259,27 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     total_ms = t_begin.elapsed_time(t_end)
     launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    batch.status(stream=stream)
+
+    # the same tile requests launched one by one, and the whole frame as one launch
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = max(3, min(args.steps, 50))
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    per_tile_ms = timed(lambda: batch.launch_per_request(stream=stream), reps)
+    batch.status(stream=stream)
+    whole_ms = timed(lambda: render.render_async(img, pipe, w.active, out, status, stream=stream), reps)
     render.status_from_device(int(status.item()))
+    mixed = _mixed_batch(render, workloads, torch, dev, stream, reps=max(3, min(args.steps, 20)))
 
     # end-to-end through the public API: pinned host Bayer in, host RGB out
     pinned_in = torch.from_numpy(samples_host.reshape(-1).view(np.int16)).pin_memory()
@@ -274,6 +304,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    batch.status(stream=stream)
 
     stats = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -298,14 +329,23 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "frame": f"{aw}x{ah} active of {w.width}x{w.height} BGGR stride {w.stride}",
-                   "tile": w.tile, "per_launch": "whole active area (CTA grid = tile grid)",
+                   "tile": w.tile,
+                   "per_launch": f"{len(tiles)} tile requests of {w.tile} (edge remainders) drained by one "
+                                 "persistent batched launch (CUDA graph)",
+                   "batch_options": tuned,
                    "l2": "inputs+outputs 337 MB > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{world}"},
+        "batched_vs_per_tile": {
+            "batched_mpix_s": round(pixels / (ms_per_step * 1e-3) / 1e6, 2),
+            "per_tile_mpix_s": round(pixels / (per_tile_ms * 1e-3) / 1e6, 2),
+            "speedup": round(per_tile_ms / ms_per_step, 3),
+            "single_launch_whole_frame_mpix_s": round(pixels / (whole_ms * 1e-3) / 1e6, 2),
+            "mixed_batch": mixed},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s", "algorithmic_bytes_per_px": ALGO_BYTES_PER_PX,
-                     "kernel_ms": round(kernel_ms, 5)},
+                     "kernel": "batch_render_kernel", "kernel_ms": round(kernel_ms, 5)},
         "cpu_baseline": cpu,
         "e2e": {"value": round(world * pixels / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s",
                 "h2d_bytes_per_step": int(samples_host.nbytes), "d2h_bytes_per_step": int(pixels * 12)},
@@ -313,6 +353,57 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def _mixed_batch(render, workloads, torch, dev, stream, reps):
+    """The mixed batch (16 RAWs, ~3,000 tiles, mip 0/1/2): batched persistent
+    launch vs the same requests launched one by one, device time per pass."""
+    images, recipes, tiles = workloads.mixed_batch()
+    imgs = []
+    for im in images:
+        meta = render.Metadata(im.width, im.height, im.stride, im.pattern, im.phase[0], im.phase[1], im.active,
+                               im.black, (im.white,) * 4)
+        imgs.append(render.Image(meta, render.synthetic_samples(im, device=dev)))
+    pipes = [workloads.mixed_pipeline(im, r) for im, r in zip(images, recipes)]
+    sizes = [t.viewport[2] * t.viewport[3] * 3 for t in tiles]
+    arena = torch.empty(sum(sizes), dtype=torch.float32, device=dev)
+    outs, off = [], 0
+    for t, n in zip(tiles, sizes):
+        outs.append(arena[off:off + n].view(t.viewport[3], t.viewport[2], 3))
+        off += n
+    reqs = [(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality, o) for t, o in zip(tiles, outs)]
+    batch = render.Batch().plan(reqs)
+    with torch.cuda.stream(stream):
+        tuned = batch.autotune(reps=3, stream=stream)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    batched_ms = timed(lambda: batch.launch(stream=stream))
+    batch.status(stream=stream)
+    per_ms = timed(lambda: batch.launch_per_request(stream=stream))
+    batch.status(stream=stream)
+    info = batch.info()
+    algo = info["raw_bytes"] + info["output_bytes"]
+    out_px = info["output_pixels"]
+    result = {"requests": info["requests"], "reduced_requests": info["reduced_requests"],
+              "tiles_queued": info["tiles"], "output_mpix": round(out_px / 1e6, 2),
+              "native_mpix": round(info["native_pixels"] / 1e6, 2),
+              "batched_ms": round(batched_ms, 4), "per_request_ms": round(per_ms, 4),
+              "speedup": round(per_ms / batched_ms, 3),
+              "batched_mpix_s": round(out_px / (batched_ms * 1e-3) / 1e6, 1),
+              "batched_gb_s": round(algo / (batched_ms * 1e-3) / 1e9, 1), "options": tuned}
+    batch.close()
+    del arena
+    return result
 
 
 def main():

@@ -234,6 +234,69 @@ RE_API re_status re_render_tiles(const re_image* image, const re_render_desc* de
                                  uint32_t quality, re_tile_callback callback, void* user,
                                  void* stream);
 
+/* ------------------------------------------------------------ batched render */
+
+/* Many render requests -- tiles of several images, recipes, viewports and mip
+ * levels, as TileScheduler and Renderer::render_tiles issue them
+ * (TileScheduler.cpp:19-304, RawEngine.cpp:1390-1412) -- rendered by one
+ * persistent kernel that drains a device queue of CTA tiles, plus one launch
+ * that reduces the mip 1/2 footprints.  Every request's pixels equal
+ * re_render_raw's for the same request bit for bit.  Outputs are DEVICE
+ * memory.  No counterpart in the reference: its scheduler renders request by
+ * request. */
+typedef struct re_batch_item {
+    const re_image* image;
+    const re_render_desc* desc;
+    re_rect viewport;           /* level coordinates, as re_render_raw */
+    uint32_t mip, quality;
+    float* out;                 /* device memory */
+    size_t out_row_stride;      /* floats, >= 3 * viewport.width */
+} re_batch_item;
+
+typedef struct re_batch_options {
+    uint32_t dispatch;          /* 0: persistent grid draining an atomic tile queue; 1: one CTA per
+                                   tile; 2: persistent grid taking every grid-th tile, prefetching
+                                   the next tile's record while the current one renders */
+    uint32_t ctas_per_sm;       /* persistent grid = SMs x this (1..4); 0 = 4 */
+    uint32_t order;             /* 0: requests in submission order; 1: Menon requests first */
+    uint32_t use_graph;         /* nonzero: launches replayed from a CUDA graph */
+} re_batch_options;
+
+typedef struct re_batch_info {
+    uint32_t requests, reduced_requests;
+    uint32_t tiles;             /* phase-1 CTA tiles (queue length) */
+    uint32_t reduce_blocks;     /* phase-2 blocks */
+    uint32_t grid;              /* phase-1 CTAs launched */
+    uint64_t native_pixels, output_pixels;
+    uint64_t raw_bytes, output_bytes;    /* algorithmic: 2 B per native pixel, 12 B per output pixel */
+    re_batch_options options;
+} re_batch_info;
+
+typedef struct re_batch re_batch;
+
+RE_API re_status re_batch_create(re_batch** out);
+RE_API re_status re_batch_destroy(re_batch* batch);
+/* Validates every item like re_render_raw_async, lays out the tile queue and
+ * the reduction blocks, uploads them and sizes the mip scratch (held by the
+ * batch).  options may be NULL (defaults, or the autotuned choice cached for
+ * a batch of the same shape). */
+RE_API re_status re_batch_plan(re_batch* batch, const re_batch_item* items, size_t count,
+                               const re_batch_options* options);
+/* Enqueues the planned batch on `stream` (no host synchronization). */
+RE_API re_status re_batch_launch(re_batch* batch, void* stream);
+/* The same planned requests launched one by one with the single-request
+ * kernels (demosaic, then the mip reduction for reduced requests): the
+ * per-tile form the batch replaces, for comparison.  Same outputs. */
+RE_API re_status re_batch_launch_per_request(re_batch* batch, void* stream);
+/* Waits for `stream` and maps the batch's device status word (non-finite or
+ * out-of-range values at the output boundary, as re_render_raw). */
+RE_API re_status re_batch_status(re_batch* batch, void* stream);
+RE_API re_status re_batch_info_get(const re_batch* batch, re_batch_info* info);
+/* Times the dispatch choices (queue or strided persistent grids of 2..4
+ * CTAs/SM, one CTA per tile; either request order) over `reps` launches of the planned batch and re-plans
+ * with the fastest; the choice is cached for batches of the same shape. */
+RE_API re_status re_batch_autotune(re_batch* batch, uint32_t reps, void* stream, re_batch_options* best);
+
 /* ------------------------------------------------------------- raster I/O */
 
 /* RasterSourceNode::render_level (RawEngine.cpp:346-406) followed by the

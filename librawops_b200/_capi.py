@@ -31,6 +31,9 @@ EXPORTS = [
     "re_cubic_axis", "re_rotation_coefficients", "re_cubic_resize_window", "re_rotate_window",
     "re_rotation_support",
     "re_render_raw_reduced_noalloc", "re_render_raw_reduced_noalloc_max_native_pixels",
+    "re_batch_create", "re_batch_destroy", "re_batch_plan", "re_batch_launch", "re_batch_launch_per_request",
+    "re_batch_status",
+    "re_batch_info_get", "re_batch_autotune",
 ]
 
 
@@ -71,6 +74,23 @@ class RenderDesc(C.Structure):
 class RenderStats(C.Structure):
     _fields_ = [("pixels", C.c_uint64), ("native_pixels", C.c_uint64), ("menon_decisions", C.c_uint64),
                 ("menon_near_ties", C.c_uint64), ("launches", C.c_uint32), ("device_ms", C.c_float)]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("image", C.c_void_p), ("desc", C.POINTER(RenderDesc)), ("viewport", Rect), ("mip", C.c_uint32),
+                ("quality", C.c_uint32), ("out", C.c_void_p), ("out_row_stride", C.c_size_t)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("dispatch", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("order", C.c_uint32),
+                ("use_graph", C.c_uint32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("requests", C.c_uint32), ("reduced_requests", C.c_uint32), ("tiles", C.c_uint32),
+                ("reduce_blocks", C.c_uint32), ("grid", C.c_uint32), ("native_pixels", C.c_uint64),
+                ("output_pixels", C.c_uint64), ("raw_bytes", C.c_uint64), ("output_bytes", C.c_uint64),
+                ("options", BatchOptions)]
 
 
 TILE_CALLBACK = C.CFUNCTYPE(C.c_int, C.POINTER(Rect), C.POINTER(C.c_float), C.c_void_p)
@@ -125,6 +145,14 @@ def lib() -> C.CDLL:
         L.re_rotation_support.argtypes = [u32, u32, C.c_double, Rect, C.POINTER(Rect)]
         L.re_render_raw_reduced_noalloc.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, vp, sz, vp]
         L.re_render_raw_reduced_noalloc_max_native_pixels.restype = sz
+        L.re_batch_create.argtypes = [C.POINTER(vp)]
+        L.re_batch_destroy.argtypes = [vp]
+        L.re_batch_plan.argtypes = [vp, C.POINTER(BatchItem), sz, C.POINTER(BatchOptions)]
+        L.re_batch_launch.argtypes = [vp, vp]
+        L.re_batch_launch_per_request.argtypes = [vp, vp]
+        L.re_batch_status.argtypes = [vp, vp]
+        L.re_batch_info_get.argtypes = [vp, C.POINTER(BatchInfo)]
+        L.re_batch_autotune.argtypes = [vp, u32, vp, C.POINTER(BatchOptions)]
         _lib = L
     return _lib
 

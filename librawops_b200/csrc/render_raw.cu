@@ -11,6 +11,7 @@
 // tiling/blocking never changes a value), so one launch over the viewport with
 // the CTA grid as the tile grid gives the reference's result for any tile size.
 #include "re_program.cuh"
+#include "re_batch.cuh"
 
 namespace re {
 
@@ -86,12 +87,9 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
 // are never read: the reference skips them and counts only present neighbours).
 // Tiles are anchored at even sensor coordinates; interior tiles take the quad
 // path, tiles meeting the active-area edge the general neighbour scan.
-__global__ void __launch_bounds__(BL_THREADS, 4)
-bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
-                const __grid_constant__ DevProgram P, float* __restrict__ out,
-                size_t out_stride, uint32_t* status) {
-    __shared__ float tile[BL_SH][BL_SW];
-    const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
+__device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw& raw, int x0, int y0, int ox,
+                                             int oy, int ow, int oh, int layout, int stage_end, const DevProgram& P,
+                                             float* __restrict__ out, size_t out_stride, uint32_t& err) {
     for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
         const int sx = i % BL_SW, sy = i / BL_SW;
         const int x = x0 - 1 + sx, y = y0 - 1 + sy;
@@ -101,7 +99,6 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
         tile[sy][sx] = v;
     }
     __syncthreads();
-    uint32_t err = 0;
     const bool interior = x0 - 1 >= raw.ax && y0 - 1 >= raw.ay && x0 + BL_TW + 1 <= raw.ax + raw.aw &&
                           y0 + BL_TH + 1 <= raw.ay + raw.ah;
     if (interior) {
@@ -111,7 +108,6 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
         case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
-        report(status, err);
         return;
     }
     for (int i = threadIdx.x; i < BL_TW * BL_TH; i += BL_THREADS) {
@@ -149,6 +145,16 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
         o[1] = rgb[1];
         o[2] = rgb[2];
     }
+}
+
+__global__ void __launch_bounds__(BL_THREADS, 4)
+bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
+                const __grid_constant__ DevProgram P, float* __restrict__ out,
+                size_t out_stride, uint32_t* status) {
+    __shared__ float tile[BL_SH][BL_SW];
+    const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
+    uint32_t err = 0;
+    bilinear_cta(tile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
     report(status, err);
 }
 
@@ -545,14 +551,10 @@ union MenonShared {
 // sensor coordinate.  Interior tiles take the fast quad path; tiles whose
 // footprint meets the active-area edge take the general mirrored path.
 // Writes float32 RGB after stages [0, stage_end) (row stride in floats).
-__global__ void __launch_bounds__(MN_THREADS, 4)
-menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
-             const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
-             uint32_t* status, unsigned long long* ties) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
-    const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
-    uint32_t err = 0;
+__device__ __forceinline__ void menon_cta(unsigned char* smem_raw, const DevRaw& raw, int x0, int y0, int ox,
+                                          int oy, int ow, int oh, int layout, int stage_end, const DevProgram& P,
+                                          float* __restrict__ out, size_t out_stride, unsigned long long* ties,
+                                          uint32_t& err) {
     const bool interior = !ties && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay && x0 + MN_TW + 6 <= raw.ax + raw.aw &&
                           y0 + MN_TH + 6 <= raw.ay + raw.ah;
     if (interior) {
@@ -563,7 +565,6 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
         case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
-        report(status, err);
         return;
     }
     MenonSmem& S = reinterpret_cast<MenonShared*>(smem_raw)->generic;
@@ -597,6 +598,17 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
         o[1] = g;
         o[2] = b;
     }
+}
+
+__global__ void __launch_bounds__(MN_THREADS, 4)
+menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
+             const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
+             uint32_t* status, unsigned long long* ties) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
+    const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
+    uint32_t err = 0;
+    menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, ties, err);
     report(status, err);
 }
 
@@ -605,13 +617,10 @@ menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh,
 // RawEngine.cpp:585-600: each reduced pixel averages its native footprint
 // (clipped at the native region's edge, actual count) in double, row-major
 // footprint order; then the stages after the anchor run on the reduced pixel.
-__global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int nh,
-                                  size_t native_stride, int scale, int ow, int oh, int stage_begin,
-                                  int stage_end, const __grid_constant__ DevProgram P,
-                                  float* __restrict__ out, size_t out_stride, uint32_t* status) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= ow || y >= oh) return;
+__device__ __forceinline__ void reduce_pixel(const float* __restrict__ native, int nw, int nh, size_t native_stride,
+                                             int scale, int x, int y, int stage_begin, int stage_end,
+                                             const DevProgram& P, float* __restrict__ out, size_t out_stride,
+                                             uint32_t& err) {
     double s0 = 0, s1 = 0, s2 = 0;
     int count = 0;
     const int y1 = min((y + 1) * scale, nh), x1 = min((x + 1) * scale, nw);
@@ -625,13 +634,126 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
         }
     const double n = (double)count;
     float r = (float)__ddiv_rn(s0, n), g = (float)__ddiv_rn(s1, n), b = (float)__ddiv_rn(s2, n);
-    uint32_t err = 0;
     apply_stages(P, stage_begin, stage_end, r, g, b, err);
     float* o = out + (size_t)y * out_stride + (size_t)x * 3;
     o[0] = r;
     o[1] = g;
     o[2] = b;
+}
+
+__global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int nh,
+                                  size_t native_stride, int scale, int ow, int oh, int stage_begin,
+                                  int stage_end, const __grid_constant__ DevProgram P,
+                                  float* __restrict__ out, size_t out_stride, uint32_t* status) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= ow || y >= oh) return;
+    uint32_t err = 0;
+    reduce_pixel(native, nw, nh, native_stride, scale, x, y, stage_begin, stage_end, P, out, out_stride, err);
     report(status, err);
+}
+
+// ----------------------------------------------------------- batched render
+
+// Phase 1 of a batched render.  Dispatch 0: a grid sized to the SMs takes
+// tiles from an atomic queue until it is empty; 1: one CTA per tile; 2: a grid
+// sized to the SMs takes tiles blockIdx.x, +gridDim.x, ..., prefetching the
+// next tile's record into shared memory (cp.async) while the current tile
+// renders.  Each tile runs exactly the per-tile code of the single-request
+// kernels, so a batched request's pixels equal its single render bit for bit.
+__device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchParams& A, const BatchUnit& T,
+                                           uint32_t& err) {
+    const int image = T.image, program = T.program, x0 = T.x0, y0 = T.y0, ox = T.ox, oy = T.oy, ow = T.ow,
+              oh = T.oh, layout = T.layout, stage_end = T.stage_end, menon = T.menon;
+    float* out = T.out;
+    const size_t out_stride = (size_t)T.out_stride;
+    const DevRaw& raw = A.images[image];
+    const DevProgram& P = A.programs[program];
+    if (menon)
+        menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, nullptr, err);
+    else
+        bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw), raw, x0, y0, ox, oy, ow, oh, layout, stage_end,
+                     P, out, out_stride, err);
+}
+
+__device__ __forceinline__ void prefetch_unit(BatchUnit* dst, const BatchUnit* src) {
+    if (threadIdx.x < 4) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst) + 16 * threadIdx.x);
+        const char* g = reinterpret_cast<const char*>(src) + 16 * threadIdx.x;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(g) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(MN_THREADS, 4) batch_render_kernel(const __grid_constant__ BatchParams A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) BatchUnit s_rec[2];
+    __shared__ uint32_t s_unit;
+    uint32_t err = 0;
+    if (A.dispatch == 1) {
+        if (blockIdx.x < A.units) batch_tile(smem_raw, A, A.units_rec[blockIdx.x], err);
+    } else if (A.dispatch == 0) {
+        for (;;) {
+            if (threadIdx.x == 0) s_unit = atomicAdd(A.queue, 1u);
+            __syncthreads();
+            const uint32_t u = s_unit;
+            __syncthreads();
+            if (u >= A.units) break;
+            batch_tile(smem_raw, A, A.units_rec[u], err);
+            __syncthreads();
+        }
+    } else {
+        uint32_t u = blockIdx.x;
+        if (u < A.units) prefetch_unit(&s_rec[0], &A.units_rec[u]);
+        for (uint32_t i = 0; u < A.units; ++i) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            __syncthreads();
+            const uint32_t next = u + gridDim.x;
+            if (next < A.units) prefetch_unit(&s_rec[(i + 1) & 1], &A.units_rec[next]);
+            batch_tile(smem_raw, A, s_rec[i & 1], err);
+            __syncthreads();
+            u = next;
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
+    report(A.status, err);
+}
+
+// Phase 2: one CTA of RD_TW x RD_TH threads per block of reduced pixels.
+__global__ void __launch_bounds__(RD_TW * RD_TH) batch_reduce_kernel(const __grid_constant__ BatchParams A) {
+    const uint32_t u = blockIdx.x;
+    if (u >= A.runits) return;
+    const ReduceTask& T = A.rtasks[A.runit_task[u]];
+    const int local = (int)(u - T.unit_begin);
+    const int x = (local % T.tiles_x) * RD_TW + (int)threadIdx.x % RD_TW;
+    const int y = (local / T.tiles_x) * RD_TH + (int)threadIdx.x / RD_TW;
+    if (x >= T.ow || y >= T.oh) return;
+    uint32_t err = 0;
+    reduce_pixel(T.native, T.nw, T.nh, T.native_stride, T.scale, x, y, T.stage_begin, T.stage_end,
+                 A.programs[T.program], T.out, T.out_stride, err);
+    report(A.status, err);
+}
+
+static_assert(BL_THREADS == MN_THREADS, "batched tiles share one block size");
+static_assert(BATCH_MENON_TW == MN_TW && BATCH_MENON_TH == MN_TH && BATCH_BILINEAR_TW == BL_TW &&
+                  BATCH_BILINEAR_TH == BL_TH,
+              "batch planner tile sizes");
+static_assert(sizeof(MenonShared) >= sizeof(float) * BL_SH * BL_SW, "bilinear tile fits the batch's shared memory");
+
+static_assert(sizeof(BatchParams) <= 32000, "batch launch parameters exceed the 32 KB kernel parameter limit");
+
+// Phase 1 of one launch group (grid CTAs), or phase 2 when reduce is set.
+cudaError_t launch_batch_group(const BatchParams& A, uint32_t grid, bool reduce, cudaStream_t stream) {
+    if (!reduce) {
+        const size_t smem = sizeof(MenonShared);
+        cudaError_t e =
+            cudaFuncSetAttribute(batch_render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (A.units && grid) batch_render_kernel<<<grid, MN_THREADS, smem, stream>>>(A);
+    } else if (A.runits) {
+        batch_reduce_kernel<<<A.runits, RD_TW * RD_TH, 0, stream>>>(A);
+    }
+    return cudaGetLastError();
 }
 
 // ----------------------------------------------------------- raster sources
@@ -691,7 +813,7 @@ cudaError_t launch_raster(const float* in, size_t in_stride, int width, int heig
 size_t menon_smem_bytes() { return sizeof(MenonShared); }
 
 // Bayer layout seen from an even sensor coordinate (the fast path's template).
-static int quad_layout(const DevRaw& raw) {
+int quad_layout(const DevRaw& raw) {
     int e[4];
     for (int k = 0; k < 4; ++k) {
         const int i = k & 1, j = k >> 1;

@@ -333,6 +333,89 @@ def render_tiles(image: Image, pipe: Pipeline, viewport, tile_size: int, callbac
     check(status)
 
 
+# ------------------------------------------------------------------ batches
+
+def synthetic_samples(img, device="cuda"):
+    """Device-synthesized sensor codes for a workloads.MixedImage."""
+    from . import synthetic
+    return synthetic.bayer_device(img.width, img.height, seed=img.seed, pattern=img.pattern, phase=img.phase,
+                                  stride=img.stride, black=img.black, white=img.white, device=device)
+
+
+class Batch:
+    """Many render requests drained by one persistent kernel (re_batch_*).
+
+    requests: (image, pipeline, viewport, mip, quality, out) with `out` a CUDA
+    float32 tensor of shape (h, w, 3) (row stride from the tensor).  The batch
+    keeps references to the images, pipelines' descriptions and outputs it was
+    planned with."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib().re_batch_create(C.byref(h)))
+        self.handle = h.value
+        self._keep = []
+
+    def plan(self, requests, dispatch=None, ctas_per_sm=4, order=1, use_graph=True):
+        items = (_capi.BatchItem * max(len(requests), 1))()
+        descs = []
+        cache = {}
+        for i, (image, pipe, viewport, mip, quality, out) in enumerate(requests):
+            if id(pipe) not in cache:
+                cache[id(pipe)] = pipe.desc()
+                descs.append(cache[id(pipe)])
+            items[i].image = image.handle
+            items[i].desc = C.pointer(cache[id(pipe)])
+            items[i].viewport = _rect(viewport)
+            items[i].mip = mip
+            items[i].quality = quality
+            items[i].out = out.data_ptr()
+            items[i].out_row_stride = out.stride(0)
+        opt = None
+        if dispatch is not None:
+            opt = _capi.BatchOptions(dispatch, ctas_per_sm, order, int(use_graph))
+        check(lib().re_batch_plan(self.handle, items, len(requests), C.byref(opt) if opt is not None else None))
+        self._keep = [requests, descs, items]
+        return self
+
+    def launch(self, stream=None):
+        check(lib().re_batch_launch(self.handle, C.c_void_p(_stream_ptr(stream))))
+
+    def launch_per_request(self, stream=None):
+        """The planned requests as one single-request launch sequence each."""
+        check(lib().re_batch_launch_per_request(self.handle, C.c_void_p(_stream_ptr(stream))))
+
+    def status(self, stream=None):
+        check(lib().re_batch_status(self.handle, C.c_void_p(_stream_ptr(stream))))
+
+    def info(self) -> dict:
+        i = _capi.BatchInfo()
+        check(lib().re_batch_info_get(self.handle, C.byref(i)))
+        o = i.options
+        return {"requests": i.requests, "reduced_requests": i.reduced_requests, "tiles": i.tiles,
+                "reduce_blocks": i.reduce_blocks, "grid": i.grid, "native_pixels": i.native_pixels,
+                "output_pixels": i.output_pixels, "raw_bytes": i.raw_bytes, "output_bytes": i.output_bytes,
+                "options": {"dispatch": o.dispatch, "ctas_per_sm": o.ctas_per_sm, "order": o.order,
+                            "use_graph": o.use_graph}}
+
+    def autotune(self, reps: int = 5, stream=None) -> dict:
+        best = _capi.BatchOptions()
+        check(lib().re_batch_autotune(self.handle, reps, C.c_void_p(_stream_ptr(stream)), C.byref(best)))
+        return {"dispatch": best.dispatch, "ctas_per_sm": best.ctas_per_sm, "order": best.order,
+                "use_graph": best.use_graph}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().re_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------ spatial / geometry
 
 def _dev(t):

@@ -117,3 +117,26 @@ def raster(width: int, height: int, seed: int) -> np.ndarray:
     hi = rng.choice(n, n // 200, replace=False)
     flat[hi] = rng.uniform(1.0, 4.0, hi.size).astype(np.float32)
     return rgb
+
+
+def bayer_device(width: int, height: int, *, seed: int, pattern: int = 0, phase=(0, 0), stride: int = 0,
+                 black=(512, 512, 512, 512), white=16383, device="cuda"):
+    """A CUDA int16 tensor (height, stride) of 14-bit sensor codes (all below
+    2^15, so the int16 bits are the uint16 codes), synthesized on the device for
+    large batches: a smooth colour field with edges plus Gaussian read noise.
+    Content is seeded and deterministic on one device."""
+    import torch
+    stride = stride or width
+    g = torch.Generator(device=device).manual_seed(seed)
+    y = torch.arange(height, device=device, dtype=torch.float32)[:, None]
+    x = torch.arange(stride, device=device, dtype=torch.float32)[None, :]
+    f1, f2, f3 = 17.0 + seed % 11, 29.0 + seed % 7, 211.0 + seed % 97
+    base = 0.30 + 0.22 * torch.sin(x / f1 + seed) * torch.cos(y / f2) + 0.18 * (x / stride) + \
+        0.15 * torch.sign(torch.sin((x + 0.6 * y) / f3))
+    site = ((((y.long() & 1) + phase[1]) & 1) * 2 + (((x.long() & 1) + phase[0]) & 1))
+    colours = torch.tensor(PATTERN_COLORS[pattern], device=device)[site]
+    gain = torch.tensor([0.85, 1.0, 0.7], device=device)[colours]
+    lv = torch.tensor(black, device=device, dtype=torch.float32)[site]
+    signal = base.clamp(0.0, 1.3) * gain * (float(white) - lv) + lv
+    noise = torch.randn(signal.shape, generator=g, device=device) * 6.0
+    return (signal + noise).round().clamp(0, 16383 + 900).to(torch.int16)

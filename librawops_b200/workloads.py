@@ -9,6 +9,13 @@
   sRGB encode; tiles 512.
 * ``raster_24mp``   -- 6000x4000 float32 ProPhoto raster for the guided filter
   (r 8/32, eps 1e-3/1e-2) and box local statistics (r 16).
+* ``mixed_batch``   -- 16 RAWs (4x 1920x1080, 6x 4000x3000, 4x 6000x4000,
+  2x 8256x5504; all patterns, both phases, padded strides, inset active areas),
+  half Menon and half bilinear, each with its own recipe (WB, exposure in
+  [-1, 1] EV, a perturbed calibration matrix, a tone curve or a random monotone
+  extended curve, sRGB output); render requests over random viewports at mip 0
+  Final and mip 1/2 Preview, split into the reference renderer's tiles of 128,
+  256, 512 or 1024 with edge remainders -- about 3,000 tiles.
 """
 from __future__ import annotations
 
@@ -93,6 +100,108 @@ def pipeline_for(w: RawWorkload):
     if w.curve is not None:
         p.extended_curves(CurveSet(w.curve, cubic=True))
     if w.srgb:
+        p.working_to_srgb()
+        p.srgb_encode()
+    return p
+
+
+# ------------------------------------------------------------------ mixed batch
+
+@dataclass
+class MixedImage:
+    width: int
+    height: int
+    stride: int
+    pattern: int
+    phase: tuple
+    active: tuple
+    black: tuple
+    white: int
+    demosaic: int
+    seed: int
+
+
+@dataclass
+class MixedRecipe:
+    wb: tuple
+    stops: float
+    camera_to_xyz: np.ndarray
+    tone: tuple | None          # (shoulder, gamma) of the ToneCurve chain
+    curve: list | None          # extended-curve knots of the curves chain
+
+
+@dataclass
+class MixedTile:
+    image: int
+    recipe: int
+    viewport: tuple
+    mip: int
+    quality: int
+
+
+MIXED_SIZES = [(1920, 1080)] * 4 + [(4000, 3000)] * 6 + [(6000, 4000)] * 4 + [(8256, 5504)] * 2
+
+
+def mixed_batch(seed: int = 4, target_tiles: int = 3000):
+    """Images, recipes (one per image) and the tile list of the mixed batch."""
+    rng = np.random.default_rng(seed)
+    images, recipes = [], []
+    for i, (w, h) in enumerate(MIXED_SIZES):
+        stride = w + 64 * (i % 3)
+        inset = (i % 2) * 8
+        active = (inset, inset // 2, w - 2 * inset, h - inset)
+        black = tuple(int(v) for v in rng.integers(500, 530, 4))
+        images.append(MixedImage(w, h, stride, i % 4, ((i // 4) % 2, (i // 2) % 2), active, black,
+                                 int(rng.integers(15800, 16384)), i % 2, seed * 100 + i))
+        cam = CALIBRATION_24MP * (1.0 + rng.uniform(-0.05, 0.05, (3, 3)))
+        wb = (float(rng.uniform(1.5, 2.2)), 1.0, float(rng.uniform(1.2, 1.8)))
+        if i % 3 == 0:
+            n = int(rng.integers(4, 17))
+            xs = np.concatenate([[0.0], np.sort(rng.uniform(0.01, 1.4, n - 2)), [1.5]])
+            xs = np.maximum.accumulate(xs + np.arange(n) * 1e-3)
+            ys = np.maximum.accumulate(np.sort(rng.uniform(0, 1.2, n)))
+            ys = ys + np.arange(n) * 1e-3
+            recipes.append(MixedRecipe(wb, float(rng.uniform(-1, 1)), cam, None,
+                                       [(float(a), float(b)) for a, b in zip(xs, ys)]))
+        else:
+            recipes.append(MixedRecipe(wb, float(rng.uniform(-1, 1)), cam,
+                                       (float(rng.uniform(0.15, 0.4)), float(rng.uniform(1.0, 2.4))), None))
+    tiles = []
+    while len(tiles) < target_tiles:
+        i = int(rng.integers(0, len(images)))
+        img = images[i]
+        level = rng.choice(3, p=[0.5, 0.3, 0.2])
+        mip, quality = (0, 1) if level == 0 else (int(level), 0)
+        ax, ay, aw, ah = img.active
+        s = 1 << mip
+        lw, lh = (aw, ah) if mip == 0 else (-(-aw // s), -(-ah // s))
+        ox0, oy0 = (ax, ay) if mip == 0 else (0, 0)
+        vw = max(1, int(lw * rng.uniform(0.05, 0.35)))
+        vh = max(1, int(lh * rng.uniform(0.05, 0.35)))
+        vx = ox0 + int(rng.integers(0, lw - vw + 1))
+        vy = oy0 + int(rng.integers(0, lh - vh + 1))
+        t = int(rng.choice([128, 256, 512, 1024]))
+        for y in range(vy, vy + vh, t):
+            for x in range(vx, vx + vw, t):
+                tiles.append(MixedTile(i, i, (x, y, min(t, vx + vw - x), min(t, vy + vh - y)), mip, quality))
+    return images, recipes, tiles
+
+
+def mixed_pipeline(image: MixedImage, recipe: MixedRecipe):
+    """The render chain of one mixed-batch recipe (CameraToWorking is the mip anchor)."""
+    from .render import CurveSet, Pipeline
+    p = Pipeline(demosaic=image.demosaic)
+    p.white_balance(*recipe.wb)
+    if recipe.curve is None:
+        p.exposure(recipe.stops)
+        p.camera_to_working(recipe.camera_to_xyz, 0)
+        p.working_to_srgb()
+        p.tone_curve(*recipe.tone)
+        p.srgb_encode()
+    else:
+        p.camera_to_working(recipe.camera_to_xyz, 0)
+        p.exposure(recipe.stops)
+        p.extended_curves(CurveSet(recipe.curve, cubic=True))
         p.working_to_srgb()
         p.srgb_encode()
     return p

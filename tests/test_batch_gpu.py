@@ -1,0 +1,178 @@
+"""The batched render (re_batch_*): many requests, one persistent kernel.
+
+A batch mixes images (all Bayer patterns, both CFA phases, padded strides,
+inset active areas), demosaic policies, recipes (with and without extended
+curves), mip 0 Final and mip 1/2 Preview, and tiles with edge remainders, as
+TileScheduler and Renderer::render_tiles issue them (TileScheduler.cpp:19-304,
+RawEngine.cpp:1390-1412).  Every request's pixels must equal the single-request
+render (re_render_raw, itself pinned to the oracle) bit for bit, under every
+dispatch choice the autotuner can make and in the per-request launch form.
+"""
+import numpy as np
+import pytest
+
+from conftest import bits_equal
+from librawops_b200 import render, workloads
+from librawops_b200._capi import ReError
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _small_batch(seed=11):
+    rng = np.random.default_rng(seed)
+    sizes = [(300, 200), (257, 181), (160, 96), (411, 233), (96, 64), (333, 250)]
+    images, recipes = [], []
+    for i, (w, h) in enumerate(sizes):
+        stride = w + 16 * (i % 3)
+        inset = (i % 2) * 5
+        images.append(workloads.MixedImage(w, h, stride, i % 4, (i % 2, (i // 2) % 2),
+                                           (inset, inset // 2 + 1, w - 2 * inset, h - inset - 1),
+                                           tuple(int(v) for v in rng.integers(500, 530, 4)),
+                                           int(rng.integers(15800, 16384)), (i // 2) % 2, 70 + i))
+        cam = workloads.CALIBRATION_24MP * (1.0 + rng.uniform(-0.05, 0.05, (3, 3)))
+        wb = (float(rng.uniform(1.5, 2.2)), 1.0, float(rng.uniform(1.2, 1.8)))
+        if i % 3 == 0:
+            knots = [(0.0, 0.0), (0.2, 0.3), (0.5, 0.62), (0.9, 0.95), (1.5, 1.2)]
+            recipes.append(workloads.MixedRecipe(wb, float(rng.uniform(-1, 1)), cam, None, knots))
+        else:
+            recipes.append(workloads.MixedRecipe(wb, float(rng.uniform(-1, 1)), cam,
+                                                 (float(rng.uniform(0.15, 0.4)), float(rng.uniform(1.0, 2.4))),
+                                                 None))
+    tiles = []
+    for i, img in enumerate(images):
+        ax, ay, aw, ah = img.active
+        for mip, quality in ((0, 1), (1, 0), (2, 0)):
+            s = 1 << mip
+            lw, lh = (aw, ah) if mip == 0 else (-(-aw // s), -(-ah // s))
+            ox0, oy0 = (ax, ay) if mip == 0 else (0, 0)
+            vw, vh = max(1, int(lw * 0.7)), max(1, int(lh * 0.6))
+            vx, vy = ox0 + (lw - vw) // 3, oy0 + (lh - vh) // 2
+            t = [37, 64, 100][(i + mip) % 3]
+            for y in range(vy, vy + vh, t):
+                for x in range(vx, vx + vw, t):
+                    tiles.append(workloads.MixedTile(i, i, (x, y, min(t, vx + vw - x), min(t, vy + vh - y)),
+                                                     mip, quality))
+    return images, recipes, tiles
+
+
+def _device_images(images):
+    out = []
+    for img in images:
+        samples = render.synthetic_samples(img)
+        meta = render.Metadata(img.width, img.height, img.stride, img.pattern, img.phase[0], img.phase[1],
+                               img.active, img.black, (img.white,) * 4)
+        out.append(render.Image(meta, samples))
+    return out
+
+
+def _requests(imgs, pipes, tiles):
+    outs = [torch.full((t.viewport[3], t.viewport[2], 3), float("nan"), device="cuda") for t in tiles]
+    reqs = [(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality, o) for t, o in zip(tiles, outs)]
+    return reqs, outs
+
+
+def test_batch_equals_single_requests():
+    images, recipes, tiles = _small_batch()
+    imgs = _device_images(images)
+    pipes = [workloads.mixed_pipeline(im, r) for im, r in zip(images, recipes)]
+    want = [render.render(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality) for t in tiles]
+    reqs, outs = _requests(imgs, pipes, tiles)
+    batch = render.Batch()
+    combos = [(d, c, o, g) for d in (0, 1, 2) for c in ((1, 4) if d != 1 else (4,)) for o in (0, 1) for g in (0, 1)]
+    for d, c, o, g in combos:
+        for out in outs:
+            out.fill_(float("nan"))
+        batch.plan(reqs, dispatch=d, ctas_per_sm=c, order=o, use_graph=bool(g))
+        batch.launch()
+        batch.status()
+        for k, (out, w) in enumerate(zip(outs, want)):
+            assert bits_equal(out.cpu().numpy(), w), (d, c, o, g, k, tiles[k])
+    info = batch.info()
+    assert info["requests"] == len(tiles)
+    assert info["reduced_requests"] == sum(1 for t in tiles if t.mip)
+    assert info["output_pixels"] == sum(t.viewport[2] * t.viewport[3] for t in tiles)
+    for out in outs:
+        out.fill_(float("nan"))
+    batch.launch_per_request()
+    batch.status()
+    for out, w in zip(outs, want):
+        assert bits_equal(out.cpu().numpy(), w)
+    best = batch.autotune(reps=2)
+    assert best["dispatch"] in (0, 1, 2) and 1 <= best["ctas_per_sm"] <= 4
+    for out in outs:
+        out.fill_(float("nan"))
+    batch.launch()
+    batch.status()
+    for out, w in zip(outs, want):
+        assert bits_equal(out.cpu().numpy(), w)
+    # a plan without options takes the tuned choice for this shape
+    batch.plan(reqs)
+    assert batch.info()["options"] == best
+    batch.close()
+
+
+def test_batch_validates_like_single_requests():
+    images, recipes, tiles = _small_batch()
+    imgs = _device_images(images[:1])
+    pipes = [workloads.mixed_pipeline(images[0], recipes[0])]
+    out = torch.zeros((8, 8, 3), device="cuda")
+    batch = render.Batch()
+    ax, ay, aw, ah = images[0].active
+    with pytest.raises(ReError) as e:
+        batch.plan([(imgs[0], pipes[0], (ax + aw - 4, ay, 8, 8), 0, 1, out)])
+    assert e.value.kind == "out_of_range"
+    with pytest.raises(ReError) as e:
+        batch.plan([(imgs[0], pipes[0], (0, 0, 8, 8), 1, 1, out)])   # mip 1 Final
+    assert e.value.kind == "invalid_argument"
+    legacy = render.Pipeline(demosaic=0)
+    legacy.white_balance(2.0, 1.0, 1.5)
+    with pytest.raises(ReError) as e:
+        batch.plan([(imgs[0], legacy, (0, 0, 8, 8), 1, 0, out)])      # no mip anchor
+    assert e.value.kind == "invalid_argument"
+    batch.plan([])
+    batch.launch()
+    batch.status()
+    batch.close()
+
+
+def test_mixed_batch_shape():
+    images, recipes, tiles = workloads.mixed_batch()
+    assert len(images) == 16 and 2900 <= len(tiles) <= 3300
+    assert {t.mip for t in tiles} == {0, 1, 2}
+    assert {im.pattern for im in images} == {0, 1, 2, 3}
+
+
+def test_batch_splits_into_launch_groups():
+    """More distinct programs than one launch group holds (24): the batch is
+    split into groups launched back to back, with identical results."""
+    images, recipes, _ = _small_batch(seed=5)
+    imgs = _device_images(images)
+    rng = np.random.default_rng(3)
+    pipes, tiles = [], []
+    for k in range(30):
+        i = k % len(images)
+        r = recipes[i]
+        wb = (r.wb[0] * float(rng.uniform(0.9, 1.1)), 1.0, r.wb[2])
+        pipes.append(workloads.mixed_pipeline(images[i], workloads.MixedRecipe(wb, r.stops, r.camera_to_xyz,
+                                                                                r.tone, r.curve)))
+        ax, ay, aw, ah = images[i].active
+        mip = k % 3
+        if mip == 0:
+            vp = (ax + k % 7, ay + k % 5, min(40, aw - k % 7), min(30, ah - k % 5))
+        else:
+            vp = (k % 4, k % 3, 20, 12)
+        tiles.append(workloads.MixedTile(i, k, vp, mip, 1 if mip == 0 else 0))
+    want = [render.render(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality) for t in tiles]
+    reqs, outs = _requests(imgs, pipes, tiles)
+    batch = render.Batch()
+    for d in (0, 1, 2):
+        for out in outs:
+            out.fill_(float("nan"))
+        batch.plan(reqs, dispatch=d, ctas_per_sm=2, order=0, use_graph=True)
+        batch.launch()
+        batch.status()
+        for k, (out, w) in enumerate(zip(outs, want)):
+            assert bits_equal(out.cpu().numpy(), w), (d, k)
+    batch.close()
