@@ -297,6 +297,59 @@ RE_API re_status re_batch_info_get(const re_batch* batch, re_batch_info* info);
  * with the fastest; the choice is cached for batches of the same shape. */
 RE_API re_status re_batch_autotune(re_batch* batch, uint32_t reps, void* stream, re_batch_options* best);
 
+/* ------------------------------------------------------- differentiable render */
+
+/* Forward kernels of the render path with the recipe as parameters, and their
+ * hand-written adjoints (vector-Jacobian products), for fitting recipes by
+ * gradient descent.  No counterpart in the reference, which has no gradients;
+ * the forward arithmetic restates RawEngine.cpp:299-344 (bilinear),
+ * :417-431/488-500/539-545 (WB, exposure, 3x3), ToneOps.cpp:795-844 (the
+ * master curve, shape-preserving cubic) and SpatialOps.cpp:168-287 (the
+ * working-Y guided filter, used as a detail boost v + k (v - GF(v))).  All
+ * buffers are DEVICE memory; images are contiguous float32 (h, w, 3); the
+ * sensor plane is (h, w) over the active area; `quad` packs the colours of the
+ * 2x2 CFA cell at the plane's origin, 2 bits each, index (y&1)*2+(x&1).
+ * Calls enqueue on `stream` and return. */
+RE_API re_status re_diff_bilinear_forward(const float* plane, size_t plane_row_stride, uint32_t width,
+                                          uint32_t height, uint32_t quad, float* rgb, void* stream);
+RE_API re_status re_diff_bilinear_backward(const float* drgb, uint32_t width, uint32_t height, uint32_t quad,
+                                           float* dplane, size_t dplane_row_stride, void* stream);
+
+/* WB gains, exposure multiplier, row-major 3x3, then the master curve: knots
+ * kx/ky (n of each), Bezier controls c0/c1 (n-1 of each) and the end slopes
+ * used for linear extrapolation (device arrays; knots = 0: no curve). */
+typedef struct re_diff_point_params {
+    float wb[3];
+    float exposure;
+    float matrix[9];
+    uint32_t knots;
+    const float* kx;
+    const float* ky;
+    const float* c0;
+    const float* c1;
+    float slope_first, slope_last;
+} re_diff_point_params;
+RE_API re_status re_diff_point_forward(const float* x, size_t pixels, const re_diff_point_params* params,
+                                       float* y, void* stream);
+/* Adds the parameter gradients to `grads` (double, caller-zeroed, length
+ * re_diff_point_grad_count(knots)): wb[3], exposure, matrix[9], ky[n],
+ * c0[n-1], c1[n-1], slope_first, slope_last. */
+RE_API re_status re_diff_point_backward(const float* x, const float* dy, size_t pixels,
+                                        const re_diff_point_params* params, float* dx, double* grads,
+                                        void* stream);
+RE_API size_t re_diff_point_grad_count(uint32_t knots);
+
+/* Detail boost out = p + strength (p - GF(p)), GF the self-guided working-Y
+ * guided filter (radius 0..64, epsilon [2^-24, 65536], clipped windows with
+ * actual counts).  The backward recomputes every box mean from p and adds
+ * d loss / d strength to *dstrength (double, device). */
+RE_API re_status re_diff_detail_forward(const float* p, uint32_t width, uint32_t height, uint32_t radius,
+                                        double epsilon, float strength, uint32_t working_space, float* out,
+                                        void* stream);
+RE_API re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t width, uint32_t height,
+                                         uint32_t radius, double epsilon, float strength, uint32_t working_space,
+                                         float* dp, double* dstrength, void* stream);
+
 /* ------------------------------------------------------------- raster I/O */
 
 /* RasterSourceNode::render_level (RawEngine.cpp:346-406) followed by the

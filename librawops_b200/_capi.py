@@ -34,6 +34,8 @@ EXPORTS = [
     "re_batch_create", "re_batch_destroy", "re_batch_plan", "re_batch_launch", "re_batch_launch_per_request",
     "re_batch_status",
     "re_batch_info_get", "re_batch_autotune",
+    "re_diff_bilinear_forward", "re_diff_bilinear_backward", "re_diff_point_forward", "re_diff_point_backward",
+    "re_diff_point_grad_count", "re_diff_detail_forward", "re_diff_detail_backward",
 ]
 
 
@@ -91,6 +93,12 @@ class BatchInfo(C.Structure):
                 ("reduce_blocks", C.c_uint32), ("grid", C.c_uint32), ("native_pixels", C.c_uint64),
                 ("output_pixels", C.c_uint64), ("raw_bytes", C.c_uint64), ("output_bytes", C.c_uint64),
                 ("options", BatchOptions)]
+
+
+class DiffPointParams(C.Structure):
+    _fields_ = [("wb", C.c_float * 3), ("exposure", C.c_float), ("matrix", C.c_float * 9), ("knots", C.c_uint32),
+                ("kx", C.c_void_p), ("ky", C.c_void_p), ("c0", C.c_void_p), ("c1", C.c_void_p),
+                ("slope_first", C.c_float), ("slope_last", C.c_float)]
 
 
 TILE_CALLBACK = C.CFUNCTYPE(C.c_int, C.POINTER(Rect), C.POINTER(C.c_float), C.c_void_p)
@@ -153,6 +161,14 @@ def lib() -> C.CDLL:
         L.re_batch_status.argtypes = [vp, vp]
         L.re_batch_info_get.argtypes = [vp, C.POINTER(BatchInfo)]
         L.re_batch_autotune.argtypes = [vp, u32, vp, C.POINTER(BatchOptions)]
+        L.re_diff_bilinear_forward.argtypes = [vp, sz, u32, u32, u32, vp, vp]
+        L.re_diff_bilinear_backward.argtypes = [vp, u32, u32, u32, vp, sz, vp]
+        L.re_diff_point_forward.argtypes = [vp, sz, C.POINTER(DiffPointParams), vp, vp]
+        L.re_diff_point_backward.argtypes = [vp, vp, sz, C.POINTER(DiffPointParams), vp, vp, vp]
+        L.re_diff_point_grad_count.argtypes = [u32]
+        L.re_diff_point_grad_count.restype = sz
+        L.re_diff_detail_forward.argtypes = [vp, u32, u32, u32, C.c_double, C.c_float, u32, vp, vp]
+        L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, C.c_float, u32, vp, vp, vp]
         _lib = L
     return _lib
 

@@ -1,0 +1,195 @@
+"""Differentiable render: torch.autograd Functions over the CUDA adjoints.
+
+    plane (h, w)  --BilinearDemosaic-->  camera RGB  --PointStages(wb, stops,
+    matrix, curve knots)-->  working RGB  --DetailBoost(strength)-->  out
+
+Each Function's forward and backward are the hand-written kernels of
+csrc/diff.cu (include/rawengine_b200.h, re_diff_*), launched on torch's current
+stream; there is no autograd-traced fallback.  The curve's Bezier controls and
+end slopes are derived from the knot values with torch operations
+(`curve_controls`, the tangent rule of ToneOps.cpp:795-816), so gradients with
+respect to the knots flow through them by autograd.  `RecipeModel` bundles the
+parameters; `fit_recipe` fits them to a target render with Adam.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from ._capi import DiffPointParams, check, lib
+
+PROPHOTO, REC2020 = 0, 1
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def quad_code(colours) -> int:
+    """Packs the colours (0 R, 1 G, 2 B) of the 2x2 CFA cell at the plane origin."""
+    return sum(int(c) << (2 * i) for i, c in enumerate(colours))
+
+
+# ------------------------------------------------------------------ demosaic
+
+class BilinearDemosaic(torch.autograd.Function):
+    """Bilinear demosaic of a normalized sensor plane (RawEngine.cpp:299-344)."""
+
+    @staticmethod
+    def forward(ctx, plane, quad: int):
+        plane = plane.contiguous()
+        h, w = plane.shape
+        out = torch.empty((h, w, 3), dtype=torch.float32, device=plane.device)
+        check(lib().re_diff_bilinear_forward(_ptr(plane), w, w, h, quad, _ptr(out), _stream()))
+        ctx.quad = quad
+        ctx.shape = (h, w)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        grad = grad.contiguous()
+        h, w = ctx.shape
+        dplane = torch.empty((h, w), dtype=torch.float32, device=grad.device)
+        check(lib().re_diff_bilinear_backward(_ptr(grad), w, h, ctx.quad, _ptr(dplane), w, _stream()))
+        return dplane, None
+
+
+# --------------------------------------------------------------------- curve
+
+def curve_controls(kx: torch.Tensor, ky: torch.Tensor):
+    """Bezier controls c0, c1 and end slopes of the shape-preserving cubic
+    (ToneOps.cpp:795-816), differentiable in ky: tangent = the smaller-magnitude
+    neighbouring slope, zero on a sign change or a flat neighbour."""
+    h = kx[1:] - kx[:-1]
+    s = (ky[1:] - ky[:-1]) / h
+    a, b = s[:-1], s[1:]
+    flat = (a == 0) | (b == 0) | (torch.signbit(a) != torch.signbit(b))
+    inner = torch.where(flat, torch.zeros_like(a), torch.where(a.abs() <= b.abs(), a, b))
+    m = torch.cat([s[:1], inner, s[-1:]])
+    c0 = ky[:-1] + h * m[:-1] / 3
+    c1 = ky[1:] - h * m[1:] / 3
+    return c0, c1, s[0], s[-1]
+
+
+class PointStages(torch.autograd.Function):
+    """WB -> exposure multiplier -> 3x3 -> master curve, per pixel."""
+
+    @staticmethod
+    def forward(ctx, x, wb, exposure, matrix, kx, ky, c0, c1, s_first, s_last):
+        x = x.contiguous()
+        p = DiffPointParams()
+        wbl, ml = wb.detach().double().tolist(), matrix.detach().reshape(-1).double().tolist()
+        for i in range(3):
+            p.wb[i] = wbl[i]
+        p.exposure = float(exposure)
+        for i in range(9):
+            p.matrix[i] = ml[i]
+        knots = [t.detach().float().contiguous() for t in (kx, ky, c0, c1)]
+        p.knots = kx.numel()
+        p.kx, p.ky, p.c0, p.c1 = (t.data_ptr() for t in knots)
+        p.slope_first, p.slope_last = float(s_first), float(s_last)
+        y = torch.empty_like(x)
+        check(lib().re_diff_point_forward(_ptr(x), x.numel() // 3, C.byref(p), _ptr(y), _stream()))
+        ctx.save_for_backward(x, *knots)
+        ctx.p = p
+        ctx.n = kx.numel()
+        return y
+
+    @staticmethod
+    def backward(ctx, grad):
+        x, kx, ky, c0, c1 = ctx.saved_tensors
+        p = ctx.p
+        p.kx, p.ky, p.c0, p.c1 = kx.data_ptr(), ky.data_ptr(), c0.data_ptr(), c1.data_ptr()
+        n = ctx.n
+        grad = grad.contiguous()
+        g = torch.zeros(int(lib().re_diff_point_grad_count(n)), dtype=torch.float64, device=x.device)
+        dx = torch.empty_like(x)
+        check(lib().re_diff_point_backward(_ptr(x), _ptr(grad), x.numel() // 3, C.byref(p), _ptr(dx), _ptr(g),
+                                           _stream()))
+        gf = g.float()
+        gk = gf[13:]
+        return (dx, gf[0:3], gf[3], gf[4:13].reshape(3, 3), None, gk[:n], gk[n:2 * n - 1],
+                gk[2 * n - 1:3 * n - 2], gk[3 * n - 2], gk[3 * n - 1])
+
+
+def point_stages(x, wb, stops, matrix, kx, ky):
+    """Point stages with the exposure in stops and the curve given by its knots."""
+    c0, c1, sf, sl = curve_controls(kx, ky)
+    exposure = torch.exp2(stops)
+    return PointStages.apply(x, wb, exposure, matrix, kx, ky, c0, c1, sf, sl)
+
+
+# -------------------------------------------------------------- detail boost
+
+class DetailBoost(torch.autograd.Function):
+    """out = v + strength (v - GF(v)), GF the self-guided working-Y guided filter."""
+
+    @staticmethod
+    def forward(ctx, v, strength, radius: int, eps: float, space: int):
+        v = v.contiguous()
+        h, w = v.shape[:2]
+        out = torch.empty_like(v)
+        check(lib().re_diff_detail_forward(_ptr(v), w, h, radius, eps, float(strength), space, _ptr(out),
+                                           _stream()))
+        ctx.save_for_backward(v)
+        ctx.args = (radius, eps, float(strength), space)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        (v,) = ctx.saved_tensors
+        radius, eps, k, space = ctx.args
+        h, w = v.shape[:2]
+        grad = grad.contiguous()
+        dv = torch.empty_like(v)
+        dk = torch.zeros(1, dtype=torch.float64, device=v.device)
+        check(lib().re_diff_detail_backward(_ptr(v), _ptr(grad), w, h, radius, eps, k, space, _ptr(dv), _ptr(dk),
+                                            _stream()))
+        return dv, dk.float()[0], None, None, None
+
+
+# --------------------------------------------------------------------- model
+
+class RecipeModel(torch.nn.Module):
+    """The differentiable render with learnable recipe parameters: WB gains,
+    exposure stops, the 3x3 camera->working matrix, the master-curve knot values
+    (knot positions fixed) and the detail-boost strength."""
+
+    def __init__(self, quad, kx, ky, wb=(1.0, 1.0, 1.0), stops=0.0, matrix=None, strength=0.0, radius=16,
+                 eps=1e-3, space=PROPHOTO, device="cuda"):
+        super().__init__()
+        f = dict(dtype=torch.float32, device=device)
+        self.quad = quad_code(quad)
+        self.radius, self.eps, self.space = radius, eps, space
+        self.register_buffer("kx", torch.tensor(kx, **f))
+        self.wb = torch.nn.Parameter(torch.tensor(wb, **f))
+        self.stops = torch.nn.Parameter(torch.tensor(float(stops), **f))
+        m = torch.eye(3) if matrix is None else torch.as_tensor(matrix, dtype=torch.float32)
+        self.matrix = torch.nn.Parameter(m.to(**f).clone())
+        self.ky = torch.nn.Parameter(torch.tensor(ky, **f))
+        self.strength = torch.nn.Parameter(torch.tensor(float(strength), **f))
+
+    def forward(self, plane):
+        x = BilinearDemosaic.apply(plane, self.quad)
+        v = point_stages(x, self.wb, self.stops, self.matrix, self.kx, self.ky)
+        return DetailBoost.apply(v, self.strength, self.radius, self.eps, self.space)
+
+
+def fit_recipe(model: RecipeModel, planes, targets, steps: int = 200, lr: float = 0.01, params=None):
+    """Adam on the mean squared error between model(plane) and target over a
+    list of frames; returns the loss history."""
+    opt = torch.optim.Adam(params if params is not None else model.parameters(), lr=lr)
+    history = []
+    for _ in range(steps):
+        opt.zero_grad(set_to_none=True)
+        loss = sum(torch.mean((model(p) - t) ** 2) for p, t in zip(planes, targets)) / len(planes)
+        loss.backward()
+        opt.step()
+        history.append(float(loss.detach()))
+    return history
+

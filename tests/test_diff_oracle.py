@@ -1,0 +1,53 @@
+"""The float64 adjoint restatement (oracle/diff_oracle.py) against central
+finite differences of its own forward model (CPU)."""
+import numpy as np
+
+from oracle import diff_oracle as D
+
+
+def _case(seed=0, h=14, w=17):
+    rng = np.random.default_rng(seed)
+    return dict(s=rng.uniform(0.05, 0.9, (h, w)), quad=(2, 1, 1, 0), wb=np.array([1.8, 1.0, 1.4]), stops=0.3,
+                M=np.array([[1.5, -0.3, -0.2], [-0.2, 1.4, -0.2], [0.05, -0.4, 1.35]]),
+                kx=np.array([0, 0.1, 0.3, 0.6, 1.0, 1.6]), ky=np.array([0, 0.18, 0.4, 0.62, 0.85, 1.05]),
+                r=2, eps=1e-3, k=0.5, dout=rng.normal(size=(h, w, 3)))
+
+
+def _fd(fun, x, step):
+    x = np.array(x, dtype=float)
+    out = np.zeros_like(x)
+    for i in np.ndindex(x.shape):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += step
+        xm[i] -= step
+        out[i] = (fun(xp) - fun(xm)) / (2 * step)
+    return out
+
+
+def test_adjoint_matches_central_differences():
+    c = _case()
+    quad, kx, r, eps, dout = c["quad"], c["kx"], c["r"], c["eps"], c["dout"]
+
+    def f(s, wb, stops, M, ky, k):
+        return float((D.render_forward(s, quad, wb, stops, M, kx, ky, r, eps, k) * dout).sum())
+
+    g = D.render_backward(c["s"], dout, quad, c["wb"], c["stops"], c["M"], kx, c["ky"], r, eps, c["k"])
+    args = [c["s"], c["wb"], c["stops"], c["M"], c["ky"], c["k"]]
+    for j, name in enumerate(["s", "wb", "stops", "M", "ky", "k"]):
+        def fj(z, j=j):
+            a = list(args)
+            a[j] = z if np.ndim(args[j]) else float(z)
+            return f(*a)
+        fd = _fd(fj, args[j], 1e-6)
+        err = np.max(np.abs(fd - g[j])) / max(1e-12, np.max(np.abs(fd)))
+        assert err < 1e-6, (name, err)
+
+
+def test_bilinear_adjoint_is_transpose():
+    rng = np.random.default_rng(4)
+    for quad in [(0, 1, 1, 2), (1, 0, 2, 1), (1, 2, 0, 1), (2, 1, 1, 0)]:
+        s = rng.normal(size=(9, 11))
+        d = rng.normal(size=(9, 11, 3))
+        lhs = float((D.bilinear_forward(s, quad) * d).sum())
+        rhs = float((s * D.bilinear_backward(d, quad)).sum())
+        assert abs(lhs - rhs) < 1e-10 * max(1.0, abs(lhs))
