@@ -280,6 +280,7 @@ def run_ours(args, rank, world, local_rank):
     whole_ms = timed(lambda: render.render_async(img, pipe, w.active, out, status, stream=stream), reps)
     render.status_from_device(int(status.item()))
     mixed = _mixed_batch(render, workloads, torch, dev, stream, reps=max(3, min(args.steps, 20)))
+    differentiable = _differentiable(torch, dev, reps=3)
 
     # end-to-end through the public API: pinned host Bayer in, host RGB out
     pinned_in = torch.from_numpy(samples_host.reshape(-1).view(np.int16)).pin_memory()
@@ -346,6 +347,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s", "algorithmic_bytes_per_px": ALGO_BYTES_PER_PX,
                      "kernel": "batch_render_kernel", "kernel_ms": round(kernel_ms, 5)},
+        "differentiable": differentiable,
         "cpu_baseline": cpu,
         "e2e": {"value": round(world * pixels / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s",
                 "h2d_bytes_per_step": int(samples_host.nbytes), "d2h_bytes_per_step": int(pixels * 12)},
@@ -404,6 +406,44 @@ def _mixed_batch(render, workloads, torch, dev, stream, reps):
     batch.close()
     del arena
     return result
+
+
+def _differentiable(torch, dev, reps):
+    """The differentiable render on 8 frames of 4000x3000 RGGB (bilinear, WB,
+    exposure, 3x3, 16-knot curve, detail boost r 16 / eps 1e-3 / strength 0.5),
+    MSE loss: device time of the forward and of the backward (all adjoints)."""
+    from librawops_b200 import diff, synthetic, workloads
+    knots = workloads.tone_knots_16()
+    model = diff.RecipeModel((0, 1, 1, 2), [k[0] for k in knots], [k[1] for k in knots], wb=(2.0, 1.0, 1.6),
+                             stops=0.2, matrix=workloads.CAMERA_TO_PROPHOTO, strength=0.5, radius=16, eps=1e-3,
+                             device=dev)
+    planes, targets = [], []
+    for i in range(8):
+        codes = synthetic.bayer_device(4000, 3000, seed=40 + i, pattern=0, black=(512,) * 4, white=16383,
+                                       device=dev)
+        planes.append(((codes.float() - 512.0) / (16383.0 - 512.0)).contiguous())
+    with torch.no_grad():
+        for pl in planes:
+            targets.append(model(pl) * 1.01)
+    fwd, bwd = [], []
+    for it in range(reps + 1):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        model.zero_grad(set_to_none=True)
+        e0.record()
+        loss = sum(torch.mean((model(pl) - t) ** 2) for pl, t in zip(planes, targets)) / len(planes)
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        if it:
+            fwd.append(e0.elapsed_time(e1))
+            bwd.append(e1.elapsed_time(e2))
+    f, b = statistics.median(fwd), statistics.median(bwd)
+    px = 8 * 4000 * 3000
+    return {"frames": 8, "frame": "4000x3000 RGGB", "chain": "bilinear, WB, exposure, 3x3, 16-knot curve, "
+            "detail boost r16 eps1e-3", "forward_ms": round(f, 3), "backward_ms": round(b, 3),
+            "backward_over_forward": round(b / f, 3), "forward_mpix_s": round(px / (f * 1e-3) / 1e6, 1),
+            "forward_backward_mpix_s": round(px / ((f + b) * 1e-3) / 1e6, 1)}
 
 
 def main():
