@@ -157,8 +157,13 @@ RE_API re_status re_curve_set_create(uint32_t interpolation, const uint32_t coun
                                      const double* knots, re_curve_set** out);
 RE_API re_status re_curve_set_destroy(re_curve_set* curves);
 
-/* A render description: demosaic policy (0 rawengine.bilinear v1, 1
- * rawengine.menon_base v1; RawEngine.cpp:276-280), then `count` stages.  Stages
+/* A render description: demosaic policy (RawEngine.cpp:276-280) -- 0
+ * rawengine.bilinear v1; 1 rawengine.menon_base v1 in binary64, bit-exact; 2
+ * rawengine.menon_base v1 computed in binary32 with every direction decision
+ * equal to the reference's (decisions inside the binary32 error band are
+ * recomputed in binary64) and demosaic outputs within a few ulp of the
+ * reference's (steep curves after it can magnify that past 1e-5) -- then
+ * `count` stages.  Stages
  * [0, anchor] run at native resolution; when a reduced level is requested the
  * result is averaged over each output pixel's native footprint after stage
  * `anchor` (the CameraToWorking mip anchor, RawEngine.cpp:580-601), and stages
@@ -193,6 +198,15 @@ RE_API re_status re_render_raw(const re_image* image, const re_render_desc* desc
                                re_rect viewport, uint32_t mip, uint32_t quality, float* out,
                                size_t out_row_stride, int out_on_device, void* stream,
                                re_render_stats* stats);
+
+/* The Menon direction of every pixel of a viewport (1 horizontal, 0
+ * vertical; green sites 1), as demosaic policy `demosaic` (1 or 2) decides
+ * it, into DEVICE memory `out` (viewport.width x viewport.height bytes).
+ * *near_ties (host, may be NULL) receives the number of exact ties v == h
+ * (policy 1) or of decisions taken by the binary64 recheck (policy 2).
+ * Returns after completion on `stream`. */
+RE_API re_status re_menon_directions(const re_image* image, uint32_t demosaic, re_rect viewport, uint8_t* out,
+                                     uint64_t* near_ties, void* stream);
 
 /* Asynchronous device-only form: enqueues the render on `stream` and returns.
  * Non-finite/overflow guards are OR-ed into *device_status (a device word the
@@ -317,17 +331,17 @@ RE_API re_status re_diff_bilinear_backward(const float* drgb, uint32_t width, ui
 
 /* WB gains, exposure multiplier, row-major 3x3, then the master curve: knots
  * kx/ky (n of each), Bezier controls c0/c1 (n-1 of each) and the end slopes
- * used for linear extrapolation (device arrays; knots = 0: no curve). */
+ * used for linear extrapolation.  All device memory, so that parameters that
+ * live on the device (an optimizer's) need no host round trip: `scalars` holds
+ * wb[3], exposure, matrix[9], slope_first, slope_last (15 floats); knots = 0:
+ * no curve. */
 typedef struct re_diff_point_params {
-    float wb[3];
-    float exposure;
-    float matrix[9];
+    const float* scalars;
     uint32_t knots;
     const float* kx;
     const float* ky;
     const float* c0;
     const float* c1;
-    float slope_first, slope_last;
 } re_diff_point_params;
 RE_API re_status re_diff_point_forward(const float* x, size_t pixels, const re_diff_point_params* params,
                                        float* y, void* stream);
@@ -341,14 +355,15 @@ RE_API size_t re_diff_point_grad_count(uint32_t knots);
 
 /* Detail boost out = p + strength (p - GF(p)), GF the self-guided working-Y
  * guided filter (radius 0..64, epsilon [2^-24, 65536], clipped windows with
- * actual counts).  The backward recomputes every box mean from p and adds
- * d loss / d strength to *dstrength (double, device). */
+ * actual counts; at most 65535 rows).  `strength` is one device float.  The
+ * backward recomputes every box mean from p and adds d loss / d strength to
+ * *dstrength (double, device). */
 RE_API re_status re_diff_detail_forward(const float* p, uint32_t width, uint32_t height, uint32_t radius,
-                                        double epsilon, float strength, uint32_t working_space, float* out,
+                                        double epsilon, const float* strength, uint32_t working_space, float* out,
                                         void* stream);
 RE_API re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t width, uint32_t height,
-                                         uint32_t radius, double epsilon, float strength, uint32_t working_space,
-                                         float* dp, double* dstrength, void* stream);
+                                         uint32_t radius, double epsilon, const float* strength,
+                                         uint32_t working_space, float* dp, double* dstrength, void* stream);
 
 /* ------------------------------------------------------------- raster I/O */
 

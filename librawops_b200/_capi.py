@@ -26,7 +26,7 @@ EXPORTS = [
     "re_request_bounds", "re_raw_input_region", "re_mip_native_region", "re_plan_tiles",
     "re_camera_to_working_matrix", "re_working_to_srgb_matrix", "re_working_to_working_matrix",
     "re_exposure_multiplier", "re_curve_set_create", "re_curve_set_destroy",
-    "re_render_raw", "re_render_raw_async", "re_render_scratch_bytes", "re_status_from_device",
+    "re_render_raw", "re_render_raw_async", "re_menon_directions", "re_render_scratch_bytes", "re_status_from_device",
     "re_render_tiles", "re_render_raster", "re_guided_filter", "re_local_statistics", "re_local_statistics_f64", "re_cubic_resize", "re_rotate",
     "re_cubic_axis", "re_rotation_coefficients", "re_cubic_resize_window", "re_rotate_window",
     "re_rotation_support",
@@ -96,9 +96,8 @@ class BatchInfo(C.Structure):
 
 
 class DiffPointParams(C.Structure):
-    _fields_ = [("wb", C.c_float * 3), ("exposure", C.c_float), ("matrix", C.c_float * 9), ("knots", C.c_uint32),
-                ("kx", C.c_void_p), ("ky", C.c_void_p), ("c0", C.c_void_p), ("c1", C.c_void_p),
-                ("slope_first", C.c_float), ("slope_last", C.c_float)]
+    _fields_ = [("scalars", C.c_void_p), ("knots", C.c_uint32), ("kx", C.c_void_p), ("ky", C.c_void_p),
+                ("c0", C.c_void_p), ("c1", C.c_void_p)]
 
 
 TILE_CALLBACK = C.CFUNCTYPE(C.c_int, C.POINTER(Rect), C.POINTER(C.c_float), C.c_void_p)
@@ -135,6 +134,7 @@ def lib() -> C.CDLL:
         L.re_render_raw.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, C.c_int, vp,
                                     C.POINTER(RenderStats)]
         L.re_render_raw_async.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, vp, vp, vp]
+        L.re_menon_directions.argtypes = [vp, u32, Rect, vp, C.POINTER(C.c_uint64), vp]
         L.re_render_scratch_bytes.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32]
         L.re_render_scratch_bytes.restype = sz
         L.re_status_from_device.argtypes = [u32]
@@ -167,8 +167,8 @@ def lib() -> C.CDLL:
         L.re_diff_point_backward.argtypes = [vp, vp, sz, C.POINTER(DiffPointParams), vp, vp, vp]
         L.re_diff_point_grad_count.argtypes = [u32]
         L.re_diff_point_grad_count.restype = sz
-        L.re_diff_detail_forward.argtypes = [vp, u32, u32, u32, C.c_double, C.c_float, u32, vp, vp]
-        L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, C.c_float, u32, vp, vp, vp]
+        L.re_diff_detail_forward.argtypes = [vp, u32, u32, u32, C.c_double, vp, u32, vp, vp]
+        L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, vp, u32, vp, vp, vp]
         _lib = L
     return _lib
 

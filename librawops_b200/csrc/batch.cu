@@ -28,7 +28,7 @@ namespace re {
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
                             int stage_end, const DevProgram& P, float* out, size_t out_stride,
                             uint32_t* status, unsigned long long* ties, cudaStream_t stream,
-                            uint32_t* launches);
+                            uint32_t* launches, uint8_t* dirs = nullptr);
 cudaError_t launch_mip_reduce(const float* native, int nw, int nh, size_t native_stride, int mip,
                               int ow, int oh, int stage_begin, int stage_end, const DevProgram& P,
                               float* out, size_t out_stride, uint32_t* status, cudaStream_t stream,
@@ -180,7 +180,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         r.item = i;
         r.desc = it.desc;
         r.mip = (int)it.mip;
-        r.menon = it.desc->demosaic == 1 && r.raw->aw > 1 && r.raw->ah > 1;
+        r.menon = it.desc->demosaic >= 1 && r.raw->aw > 1 && r.raw->ah > 1 ? (int)it.desc->demosaic : 0;
         r.layout = quad_layout(*r.raw);
         r.stage_end = it.mip ? r.program.anchor + 1 : (int)r.program.count;
         const int tw = r.menon ? BATCH_MENON_TW : BATCH_BILINEAR_TW;

@@ -23,7 +23,7 @@ size_t menon_smem_bytes();
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
                             int stage_end, const DevProgram& P, float* out, size_t out_stride,
                             uint32_t* status, unsigned long long* ties, cudaStream_t stream,
-                            uint32_t* launches);
+                            uint32_t* launches, uint8_t* dirs = nullptr);
 cudaError_t launch_mip_reduce(const float* native, int nw, int nh, size_t native_stride, int mip,
                               int ow, int oh, int stage_begin, int stage_end, const DevProgram& P,
                               float* out, size_t out_stride, uint32_t* status, cudaStream_t stream,
@@ -201,7 +201,7 @@ re_status status_from_key(uint32_t key) {
 
 re_status build_program(const re_render_desc* d, DevProgram& P) {
     if (!d) return fail(RE_INVALID_ARGUMENT, "render description is null");
-    if (d->demosaic > 1) return fail(RE_INVALID_ARGUMENT, "unsupported RAW demosaic algorithm or processing version");
+    if (d->demosaic > 2) return fail(RE_INVALID_ARGUMENT, "unsupported RAW demosaic algorithm or processing version");
     if (d->count > RE_MAX_STAGES) return fail(RE_LENGTH_ERROR, "too many fused stages");
     if (d->anchor < -1 || d->anchor >= (int32_t)d->count)
         return fail(RE_INVALID_ARGUMENT, "mip anchor is not a stage of this chain");
@@ -341,7 +341,7 @@ re_status re_request_bounds(re_rect s, uint32_t mip, uint32_t quality, re_rect* 
 re_status re_raw_input_region(const re_raw_metadata* m, uint32_t demosaic, re_rect output, re_rect* region) {
     const re_rect a = m->active_area;
     if (!inside(a, output)) return fail(RE_OUT_OF_RANGE, "viewport is outside the active RAW area");
-    const uint32_t radius = demosaic == 1 && a.width > 1 && a.height > 1 ? 6u : 1u;
+    const uint32_t radius = demosaic >= 1 && a.width > 1 && a.height > 1 ? 6u : 1u;
     const int64_t left = std::max<int64_t>(a.x, (int64_t)output.x - radius);
     const int64_t top = std::max<int64_t>(a.y, (int64_t)output.y - radius);
     const uint64_t right = std::min<uint64_t>((uint64_t)a.x + a.width, (uint64_t)output.x + output.width + radius);
@@ -686,11 +686,41 @@ re_status re_render_raw(const re_image* img, const re_render_desc* desc, re_rect
         cudaEventDestroy(e1);
         stats->pixels = (uint64_t)viewport.width * viewport.height;
         stats->native_pixels = (uint64_t)native.width * native.height;
-        stats->menon_decisions = desc->demosaic == 1 ? stats->native_pixels / 2 : 0;
+        stats->menon_decisions = desc->demosaic >= 1 ? stats->native_pixels / 2 : 0;
         stats->menon_near_ties = head_host[1];
         stats->launches = launches;
     }
     return status_from_key((uint32_t)head_host[0]);
+}
+
+// The direction map of a Menon render (viewport pixels, 1 = horizontal).
+re_status re_menon_directions(const re_image* img, uint32_t demosaic, re_rect viewport, uint8_t* out,
+                              uint64_t* near_ties, void* stream_) {
+    if (!img || (!out && viewport.width && viewport.height)) return fail(RE_INVALID_ARGUMENT, "null arguments");
+    if (demosaic < 1 || demosaic > 2) return fail(RE_INVALID_ARGUMENT, "directions exist for the Menon policies only");
+    if (!inside(img->meta.active_area, viewport)) return fail(RE_OUT_OF_RANGE, "viewport is outside the active RAW area");
+    if (near_ties) *near_ties = 0;
+    if (!viewport.width || !viewport.height) return RE_OK;
+    if (img->raw.aw <= 1 || img->raw.ah <= 1) return fail(RE_INVALID_ARGUMENT, "a singleton active axis is bilinear");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    DevProgram P;
+    std::memset(&P, 0, sizeof(P));
+    P.anchor = -1;
+    const size_t rgb = (size_t)viewport.width * viewport.height * 3 * sizeof(float);
+    DeviceScratch scratch;
+    scratch.s = stream;
+    RE_CUDA(cudaMallocAsync(&scratch.p, 256 + rgb, stream));
+    char* base = static_cast<char*>(scratch.p);
+    RE_CUDA(cudaMemsetAsync(base, 0, 256, stream));
+    RE_CUDA(launch_demosaic(demosaic, img->raw, (int)viewport.x, (int)viewport.y, (int)viewport.width,
+                            (int)viewport.height, 0, P, reinterpret_cast<float*>(base + 256), (size_t)viewport.width * 3,
+                            reinterpret_cast<uint32_t*>(base), reinterpret_cast<unsigned long long*>(base + 8), stream,
+                            nullptr, out));
+    uint64_t ties = 0;
+    RE_CUDA(cudaMemcpyAsync(&ties, base + 8, 8, cudaMemcpyDeviceToHost, stream));
+    RE_CUDA(cudaStreamSynchronize(stream));
+    if (near_ties) *near_ties = ties;
+    return RE_OK;
 }
 
 // RasterSourceNode::render_level (RawEngine.cpp:346-406) + fused stages.

@@ -114,15 +114,24 @@ __global__ void bilinear_bwd_kernel(const float* __restrict__ dout, int w, int h
 constexpr int PT_THREADS = 256, MAX_KNOTS = 256;
 
 struct PointParams {
-    float wb[3], e, m[9];
+    const float* scalars;          // device: wb[3], e, m[9], s_first, s_last
     int n;                         // knots (0: no curve)
     const float *kx, *ky, *c0, *c1;
-    float s_first, s_last;
 };
+
+// The point-stage constants, read once per block from device memory.
+struct PointScalars {
+    float wb[3], e, m[9], s_first, s_last;
+};
+static_assert(sizeof(PointScalars) == 15 * sizeof(float), "scalar block layout");
 
 struct CurveSmem {
     float kx[MAX_KNOTS], ky[MAX_KNOTS], c0[MAX_KNOTS], c1[MAX_KNOTS];
 };
+
+__device__ __forceinline__ void load_scalars(PointScalars& K, const PointParams& P) {
+    if (threadIdx.x < 15) reinterpret_cast<float*>(&K)[threadIdx.x] = P.scalars[threadIdx.x];
+}
 
 __device__ __forceinline__ void load_curve(CurveSmem& C, const PointParams& P) {
     for (int i = threadIdx.x; i < P.n; i += blockDim.x) {
@@ -146,15 +155,15 @@ __device__ __forceinline__ int segment(const CurveSmem& C, int n, float v) {
     return lo;
 }
 
-__device__ __forceinline__ float curve_eval(const CurveSmem& C, const PointParams& P, float v, float* dvdx) {
-    const int n = P.n;
+__device__ __forceinline__ float curve_eval(const CurveSmem& C, const PointScalars& K, int n, float v,
+                                            float* dvdx) {
     if (v < C.kx[0]) {
-        *dvdx = P.s_first;
-        return C.ky[0] + (v - C.kx[0]) * P.s_first;
+        *dvdx = K.s_first;
+        return C.ky[0] + (v - C.kx[0]) * K.s_first;
     }
     if (v > C.kx[n - 1]) {
-        *dvdx = P.s_last;
-        return C.ky[n - 1] + (v - C.kx[n - 1]) * P.s_last;
+        *dvdx = K.s_last;
+        return C.ky[n - 1] + (v - C.kx[n - 1]) * K.s_last;
     }
     const int i = segment(C, n, v);
     const float h = C.kx[i + 1] - C.kx[i];
@@ -167,16 +176,18 @@ __device__ __forceinline__ float curve_eval(const CurveSmem& C, const PointParam
 __global__ void __launch_bounds__(PT_THREADS) point_fwd_kernel(const float* __restrict__ x, size_t count,
                                                                const PointParams P, float* __restrict__ y) {
     __shared__ CurveSmem C;
+    __shared__ PointScalars K;
     load_curve(C, P);
+    load_scalars(K, P);
     __syncthreads();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
         float z[3];
-        for (int c = 0; c < 3; ++c) z[c] = x[i * 3 + c] * P.wb[c] * P.e;
+        for (int c = 0; c < 3; ++c) z[c] = x[i * 3 + c] * K.wb[c] * K.e;
         for (int r = 0; r < 3; ++r) {
-            float v = P.m[3 * r] * z[0] + P.m[3 * r + 1] * z[1] + P.m[3 * r + 2] * z[2];
+            float v = K.m[3 * r] * z[0] + K.m[3 * r + 1] * z[1] + K.m[3 * r + 2] * z[2];
             if (P.n) {
                 float d;
-                v = curve_eval(C, P, v, &d);
+                v = curve_eval(C, K, P.n, v, &d);
             }
             y[i * 3 + r] = v;
         }
@@ -200,7 +211,9 @@ __global__ void __launch_bounds__(PT_THREADS) point_bwd_kernel(const float* __re
     __shared__ CurveSmem C;
     __shared__ CurveGradSmem G;
     __shared__ double red[PT_THREADS / 32][13];
+    __shared__ PointScalars K;
     load_curve(C, P);
+    load_scalars(K, P);
     for (int i = threadIdx.x; i < MAX_KNOTS; i += blockDim.x) G.ky[i] = G.c0[i] = G.c1[i] = 0.0;
     if (threadIdx.x < 2) G.s[threadIdx.x] = 0.0;
     __syncthreads();
@@ -210,20 +223,20 @@ __global__ void __launch_bounds__(PT_THREADS) point_bwd_kernel(const float* __re
         float xs[3], t1[3], z[3], g[3];
         for (int c = 0; c < 3; ++c) {
             xs[c] = x[i * 3 + c];
-            t1[c] = xs[c] * P.wb[c];
-            z[c] = t1[c] * P.e;
+            t1[c] = xs[c] * K.wb[c];
+            z[c] = t1[c] * K.e;
         }
         for (int r = 0; r < 3; ++r) {
-            const float v = P.m[3 * r] * z[0] + P.m[3 * r + 1] * z[1] + P.m[3 * r + 2] * z[2];
+            const float v = K.m[3 * r] * z[0] + K.m[3 * r + 1] * z[1] + K.m[3 * r + 2] * z[2];
             const float go = dy[i * 3 + r];
             float d = 1.0f;
             if (n) {
                 if (v < C.kx[0]) {
-                    d = P.s_first;
+                    d = K.s_first;
                     atomicAdd(&G.ky[0], (double)go);
                     atomicAdd(&G.s[0], (double)go * (double)(v - C.kx[0]));
                 } else if (v > C.kx[n - 1]) {
-                    d = P.s_last;
+                    d = K.s_last;
                     atomicAdd(&G.ky[n - 1], (double)go);
                     atomicAdd(&G.s[1], (double)go * (double)(v - C.kx[n - 1]));
                 } else {
@@ -242,12 +255,12 @@ __global__ void __launch_bounds__(PT_THREADS) point_bwd_kernel(const float* __re
             for (int c = 0; c < 3; ++c) acc[4 + 3 * r + c] += (double)g[r] * (double)z[c];
         }
         float dz[3];
-        for (int c = 0; c < 3; ++c) dz[c] = P.m[c] * g[0] + P.m[3 + c] * g[1] + P.m[6 + c] * g[2];
+        for (int c = 0; c < 3; ++c) dz[c] = K.m[c] * g[0] + K.m[3 + c] * g[1] + K.m[6 + c] * g[2];
         for (int c = 0; c < 3; ++c) {
             acc[3] += (double)dz[c] * (double)t1[c];
-            const float dt1 = dz[c] * P.e;
+            const float dt1 = dz[c] * K.e;
             acc[c] += (double)dt1 * (double)xs[c];
-            dx[i * 3 + c] = dt1 * P.wb[c];
+            dx[i * 3 + c] = dt1 * K.wb[c];
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -289,25 +302,26 @@ __device__ __forceinline__ double count_at(const GfGeom& g, int x, int y) {
 
 constexpr int BOX_CHUNK = 64;
 
-// out[p][y][x] = sum of in[p][y][x-r..x+r] clipped; one thread per (plane, row, chunk)
-__global__ void box_rows_kernel(const double* __restrict__ in, double* __restrict__ out, GfGeom g, int planes) {
-    const int chunks = (g.w + BOX_CHUNK - 1) / BOX_CHUNK;
-    const size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (id >= (size_t)planes * g.h * chunks) return;
-    const int chunk = (int)(id % chunks);
-    const int y = (int)((id / chunks) % g.h);
-    const int p = (int)(id / ((size_t)chunks * g.h));
+// out[p][y][x] = sum of in[p][y][x-r..x+r] clipped.  One CTA per (plane, row,
+// segment of BOX_SEG columns): the segment and its halo are staged in shared
+// memory with coalesced loads, then each thread sums its window from there.
+constexpr int BOX_SEG = 256, BOX_MAX_R = 64;
+__global__ void __launch_bounds__(BOX_SEG) box_rows_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                           GfGeom g, int planes) {
+    __shared__ double seg[BOX_SEG + 2 * BOX_MAX_R];
+    const int x0 = blockIdx.x * BOX_SEG, y = blockIdx.y, p = blockIdx.z;
     const double* row = in + p * g.plane + (size_t)y * g.w;
-    double* orow = out + p * g.plane + (size_t)y * g.w;
-    const int x0 = chunk * BOX_CHUNK, x1 = min(x0 + BOX_CHUNK, g.w);
-    double s = 0;
-    for (int j = max(0, x0 - g.r); j <= min(g.w - 1, x0 + g.r); ++j) s += row[j];
-    for (int x = x0; x < x1; ++x) {
-        orow[x] = s;
-        const int add = x + 1 + g.r, sub = x - g.r;
-        if (add < g.w) s += row[add];
-        if (sub >= 0) s -= row[sub];
+    const int n = BOX_SEG + 2 * g.r;
+    for (int i = threadIdx.x; i < n; i += BOX_SEG) {
+        const int x = x0 - g.r + i;
+        seg[i] = (x >= 0 && x < g.w) ? row[x] : 0.0;
     }
+    __syncthreads();
+    const int x = x0 + (int)threadIdx.x;
+    if (x >= g.w) return;
+    double s = 0;
+    for (int j = 0; j <= 2 * g.r; ++j) s += seg[threadIdx.x + j];
+    out[p * g.plane + (size_t)y * g.w + x] = s;
 }
 
 // out[p][y][x] = sum of in[p][y-r..y+r][x] clipped; one thread per (plane, column, chunk of rows)
@@ -385,8 +399,9 @@ __global__ void gf_coef_kernel(const double* __restrict__ S8, GfGeom g, double e
     }
 }
 
-__global__ void gf_out_kernel(const float* __restrict__ p, const double* __restrict__ SAB, GfGeom g, YW w, float k,
-                              float* __restrict__ out) {
+__global__ void gf_out_kernel(const float* __restrict__ p, const double* __restrict__ SAB, GfGeom g, YW w,
+                              const float* __restrict__ kp, float* __restrict__ out) {
+    const float k = *kp;
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= g.plane) return;
     const int x = (int)(i % g.w), y = (int)(i / g.w);
@@ -401,9 +416,10 @@ __global__ void gf_out_kernel(const float* __restrict__ p, const double* __restr
 
 // Backward step 1: planes dq I / N and dq / N; dk partial sums.
 __global__ void gf_bwd1_kernel(const float* __restrict__ p, const float* __restrict__ dout,
-                               const double* __restrict__ SAB, GfGeom g, YW w, float k, double* __restrict__ G6,
-                               double* __restrict__ dk) {
+                               const double* __restrict__ SAB, GfGeom g, YW w, const float* __restrict__ kp,
+                               double* __restrict__ G6, double* __restrict__ dk) {
     __shared__ double red[8];
+    const float k = *kp;
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     double part = 0;
     if (i < g.plane) {
@@ -459,8 +475,9 @@ __global__ void gf_bwd2_kernel(const double* __restrict__ S8, const double* __re
 }
 
 __global__ void gf_bwd3_kernel(const float* __restrict__ p, const float* __restrict__ dout,
-                               const double* __restrict__ SAB, const double* __restrict__ B8, GfGeom g, YW w, float k,
-                               float* __restrict__ dp) {
+                               const double* __restrict__ SAB, const double* __restrict__ B8, GfGeom g, YW w,
+                               const float* __restrict__ kp, float* __restrict__ dp) {
+    const float k = *kp;
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= g.plane) return;
     const int x = (int)(i % g.w), y = (int)(i / g.w);
@@ -489,9 +506,7 @@ YW weights(uint32_t space) {
 }
 
 void box(const double* in, double* tmp, double* out, const GfGeom& g, int planes, cudaStream_t s) {
-    const int chunks_x = (g.w + BOX_CHUNK - 1) / BOX_CHUNK;
-    const size_t rows = (size_t)planes * g.h * chunks_x;
-    box_rows_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(in, tmp, g, planes);
+    box_rows_kernel<<<dim3((g.w + BOX_SEG - 1) / BOX_SEG, g.h, planes), BOX_SEG, 0, s>>>(in, tmp, g, planes);
     dim3 grid((g.w + 127) / 128, (g.h + BOX_CHUNK - 1) / BOX_CHUNK, planes);
     box_cols_kernel<<<grid, 128, 0, s>>>(tmp, out, g, planes);
 }
@@ -506,6 +521,7 @@ struct DScratch {
 
 re_status gf_check(uint32_t w, uint32_t h, uint32_t radius, double eps, uint32_t space) {
     if (!w || !h) return df_fail(RE_INVALID_ARGUMENT, "detail boost needs a nonempty image");
+    if (h > 65535) return df_fail(RE_LENGTH_ERROR, "detail boost supports at most 65535 rows");
     if (radius > 64 || !(eps >= 0x1p-24) || !(eps <= 65536.0))
         return df_fail(RE_INVALID_ARGUMENT, "detail boost needs radius 0..64 and finite epsilon [2^-24,65536]");
     if (space > 1) return df_fail(RE_INVALID_ARGUMENT, "detail boost needs a scene-linear working space");
@@ -545,20 +561,16 @@ re_status re_diff_bilinear_backward(const float* drgb, uint32_t w, uint32_t h, u
 }
 
 static re_status point_params(const re_diff_point_params* in, PointParams& P) {
-    if (!in) return df_fail(RE_INVALID_ARGUMENT, "null point parameters");
+    if (!in || !in->scalars) return df_fail(RE_INVALID_ARGUMENT, "null point parameters");
     if (in->knots == 1 || in->knots > MAX_KNOTS) return df_fail(RE_INVALID_ARGUMENT, "curve needs 2..256 knots");
     if (in->knots && (!in->kx || !in->ky || !in->c0 || !in->c1))
         return df_fail(RE_INVALID_ARGUMENT, "curve arrays are null");
-    std::memcpy(P.wb, in->wb, sizeof(P.wb));
-    P.e = in->exposure;
-    std::memcpy(P.m, in->matrix, sizeof(P.m));
+    P.scalars = in->scalars;
     P.n = (int)in->knots;
     P.kx = in->kx;
     P.ky = in->ky;
     P.c0 = in->c0;
     P.c1 = in->c1;
-    P.s_first = in->slope_first;
-    P.s_last = in->slope_last;
     return RE_OK;
 }
 
@@ -595,11 +607,11 @@ re_status re_diff_point_backward(const float* x, const float* dy, size_t count, 
 
 size_t re_diff_point_grad_count(uint32_t knots) { return 13 + (knots ? 3 * (size_t)knots : 0); }
 
-re_status re_diff_detail_forward(const float* p, uint32_t w, uint32_t h, uint32_t radius, double eps, float strength,
-                                 uint32_t space, float* out, void* stream_) {
+re_status re_diff_detail_forward(const float* p, uint32_t w, uint32_t h, uint32_t radius, double eps,
+                                 const float* strength, uint32_t space, float* out, void* stream_) {
     re_status st = gf_check(w, h, radius, eps, space);
     if (st) return st;
-    if (!p || !out) return df_fail(RE_INVALID_ARGUMENT, "null image");
+    if (!p || !out || !strength) return df_fail(RE_INVALID_ARGUMENT, "null image or strength");
     cudaStream_t s = (cudaStream_t)stream_;
     const GfGeom g{(int)w, (int)h, (int)radius, (size_t)w * h};
     DScratch sc;
@@ -617,11 +629,12 @@ re_status re_diff_detail_forward(const float* p, uint32_t w, uint32_t h, uint32_
 }
 
 re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t w, uint32_t h, uint32_t radius,
-                                  double eps, float strength, uint32_t space, float* dp, double* dstrength,
+                                  double eps, const float* strength, uint32_t space, float* dp, double* dstrength,
                                   void* stream_) {
     re_status st = gf_check(w, h, radius, eps, space);
     if (st) return st;
-    if (!p || !dout || !dp || !dstrength) return df_fail(RE_INVALID_ARGUMENT, "null image or gradient");
+    if (!p || !dout || !dp || !dstrength || !strength)
+        return df_fail(RE_INVALID_ARGUMENT, "null image, strength or gradient");
     cudaStream_t s = (cudaStream_t)stream_;
     const GfGeom g{(int)w, (int)h, (int)radius, (size_t)w * h};
     DScratch sc;

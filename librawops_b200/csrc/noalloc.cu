@@ -27,7 +27,7 @@ namespace re {
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
                             int stage_end, const DevProgram& P, float* out, size_t out_stride,
                             uint32_t* status, unsigned long long* ties, cudaStream_t stream,
-                            uint32_t* launches);
+                            uint32_t* launches, uint8_t* dirs = nullptr);
 cudaError_t launch_mip_reduce(const float* native, int nw, int nh, size_t native_stride, int mip,
                               int ow, int oh, int stage_begin, int stage_end, const DevProgram& P,
                               float* out, size_t out_stride, uint32_t* status, cudaStream_t stream,

@@ -19,6 +19,7 @@ namespace re {
 
 constexpr int BL_TW = 64, BL_TH = 16, BL_THREADS = 256;
 constexpr int BL_SW = BL_TW + 2, BL_SH = BL_TH + 2;
+constexpr int BL_OTILE_OFFSET = (BL_SW * BL_SH * 4 + 15) / 16 * 16;   // staged output in the batch's smem
 
 // Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
 __host__ __device__ constexpr int pat(int l, int k) {
@@ -28,14 +29,42 @@ __host__ __device__ constexpr int pat(int l, int k) {
                     : (k == 1 ? 2 : k == 2 ? 0 : 1);
 }
 
+// Writes a tile's float RGB, staged in shared memory (rows of TW pixels, 3
+// floats each), to the output rows it covers: one warp per row, aligned 16-byte
+// stores in the row's middle and single floats at its two ends, so the 12-byte
+// pixels of a row leave as full, contiguous lines instead of strided scalars.
+template <int TW, int TH, int THREADS>
+__device__ __forceinline__ void store_tile(const float* __restrict__ otile, int x0, int y0, int ox, int oy, int ow,
+                                           int oh, float* __restrict__ out, size_t out_stride) {
+    const int xa = max(x0, ox), xb = min(x0 + TW, ox + ow);
+    if (xa >= xb) return;
+    const int n = 3 * (xb - xa);
+    const int lane = threadIdx.x & 31;
+    for (int row = threadIdx.x >> 5; row < TH; row += THREADS / 32) {
+        const int y = y0 + row;
+        if (y < oy || y >= oy + oh) continue;
+        const float* src = otile + row * (TW * 3) + (xa - x0) * 3;
+        float* dst = out + (size_t)(y - oy) * out_stride + (size_t)(xa - ox) * 3;
+        const int lead = min(n, (int)(((16u - ((unsigned)(uintptr_t)dst & 15u)) & 15u) >> 2));
+        if (lane < lead) dst[lane] = src[lane];
+        const int nv = (n - lead) >> 2;
+        float4* d4 = reinterpret_cast<float4*>(dst + lead);
+        for (int v = lane; v < nv; v += 32) {
+            const float* s4 = src + lead + 4 * v;
+            d4[v] = make_float4(s4[0], s4[1], s4[2], s4[3]);
+        }
+        for (int i = lead + 4 * nv + lane; i < n; i += 32) dst[i] = src[i];
+    }
+}
+
 // Interior tiles of RawEngine.cpp:299-344: every 3x3 neighbourhood is present,
 // so each colour's neighbours and their row-major order are fixed by the
 // quad position -- four edge neighbours (N, W, E, S) or four diagonals at R/B
 // sites, a horizontal or vertical pair at G sites -- and the division by the
 // count (4 or 2, a power of two) is an exact multiply.
 template <int L>
-__device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0, int y0, int ox, int oy,
-                                              int ow, int oh, int stage_end, const DevProgram& P,
+__device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], float* otile, int x0, int y0, int ox,
+                                              int oy, int ow, int oh, int stage_end, const DevProgram& P,
                                               float* __restrict__ out, size_t out_stride, uint32_t& err) {
     for (int q = threadIdx.x; q < (BL_TW / 2) * (BL_TH / 2); q += BL_THREADS) {
         const int qx = q % (BL_TW / 2), qy = q / (BL_TW / 2);
@@ -72,14 +101,14 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
         apply_stages_n<4>(P, 0, stage_end, R, G, B, err);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (!keep[k]) continue;
-            const int x = x0 + 2 * qx + (k & 1), y = y0 + 2 * qy + (k >> 1);
-            float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+            float* o = otile + (2 * qy + (k >> 1)) * (BL_TW * 3) + (2 * qx + (k & 1)) * 3;
             o[0] = R[k];
             o[1] = G[k];
             o[2] = B[k];
         }
     }
+    __syncthreads();
+    store_tile<BL_TW, BL_TH, BL_THREADS>(otile, x0, y0, ox, oy, ow, oh, out, out_stride);
 }
 
 // RawEngine.cpp:299-344.  The normalized samples of the tile and its one-pixel
@@ -87,9 +116,10 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
 // are never read: the reference skips them and counts only present neighbours).
 // Tiles are anchored at even sensor coordinates; interior tiles take the quad
 // path, tiles meeting the active-area edge the general neighbour scan.
-__device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw& raw, int x0, int y0, int ox,
-                                             int oy, int ow, int oh, int layout, int stage_end, const DevProgram& P,
-                                             float* __restrict__ out, size_t out_stride, uint32_t& err) {
+__device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], float* otile, const DevRaw& raw, int x0, int y0,
+                                             int ox, int oy, int ow, int oh, int layout, int stage_end,
+                                             const DevProgram& P, float* __restrict__ out, size_t out_stride,
+                                             uint32_t& err) {
     for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
         const int sx = i % BL_SW, sy = i / BL_SW;
         const int x = x0 - 1 + sx, y = y0 - 1 + sy;
@@ -103,10 +133,10 @@ __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw&
                           y0 + BL_TH + 1 <= raw.ay + raw.ah;
     if (interior) {
         switch (layout) {
-        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 0: bilinear_fast<0>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 1: bilinear_fast<1>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 2: bilinear_fast<2>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        default: bilinear_fast<3>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
         return;
     }
@@ -152,9 +182,10 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
     __shared__ float tile[BL_SH][BL_SW];
+    __shared__ __align__(16) float otile[BL_TH * BL_TW * 3];
     const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
     uint32_t err = 0;
-    bilinear_cta(tile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
+    bilinear_cta(tile, otile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
     report(status, err);
 }
 
@@ -174,17 +205,20 @@ constexpr int DV_W = MN_TW + 8, DV_H = MN_TH + 6;       // origin (-4,-4), y to 
 constexpr int GR_W = MN_TW + 4, GR_H = MN_TH + 4;       // origin (-2,-2)
 constexpr int CO_W = MN_TW + 2, CO_H = MN_TH + 2;       // origin (-1,-1)
 
-struct MenonSmem {
-    double ch[CH_H][CH_W];
-    double cv[CH_H][CH_W];
-    double dh[DH_H][DH_W];
-    double dv[DV_H][DV_W];
-    double green[GR_H][GR_W];
-    double red[CO_H][CO_W];
-    double blue[CO_H][CO_W];
+template <typename T>
+struct MenonSmemT {
+    T ch[CH_H][CH_W];
+    T cv[CH_H][CH_W];
+    T dh[DH_H][DH_W];
+    T dv[DV_H][DV_W];
+    T green[GR_H][GR_W];
+    T red[CO_H][CO_W];
+    T blue[CO_H][CO_W];
     float raw[RAW_H][RAW_W];
     uint8_t horiz[GR_H][GR_W];
+    unsigned smax_bits;          // max |sample| of the loaded footprint (float bits)
 };
+using MenonSmem = MenonSmemT<double>;
 
 struct MenonCtx {
     int x0, y0;                  // tile origin (sensor coordinates)
@@ -203,41 +237,108 @@ struct MenonCtx {
     }
 };
 
+// Correctly rounded binary64 / binary32 operations (no contraction).
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T half_sum(T a, T b) { return r_mul(T(0.5), r_add(a, b)); }
+
+// Whether a binary32 decision lies inside the error band.
+__device__ __forceinline__ bool near_tie(float h, float v, float band_abs) {
+    const float band = __fmaf_rn(9.0f * 5.9604644775390625e-8f, __fadd_rn(h, v), band_abs);
+    return fabsf(__fsub_rn(v, h)) <= band;
+}
+__device__ __forceinline__ bool near_tie(double, double, float) { return false; }
+
 // MenonDemosaic.cpp:112-115 directional five-tap green estimate along one axis.
-__device__ __forceinline__ double five_tap(double m2, double m1, double own, double p1, double p2) {
-    return __dadd_rn(__dadd_rn(__dmul_rn(0.5, __dadd_rn(m1, p1)), __dmul_rn(0.5, own)),
-                     -__dmul_rn(0.25, __dadd_rn(m2, p2)));
+template <typename T>
+__device__ __forceinline__ T five_tap(T m2, T m1, T own, T p1, T p2) {
+    return r_sub(r_add(r_mul(T(0.5), r_add(m1, p1)), r_mul(T(0.5), own)), r_mul(T(0.25), r_add(m2, p2)));
 }
 
-__device__ __forceinline__ double raw_at(const MenonSmem& S, const MenonCtx& c, int x, int y) {
-    return (double)S.raw[y - (c.y0 - 6)][x - (c.x0 - 6)];
+template <typename R, typename Sm>
+__device__ __forceinline__ R raw_at(const Sm& S, const MenonCtx& c, int x, int y) {
+    return (R)S.raw[y - (c.y0 - 6)][x - (c.x0 - 6)];
 }
 
-__device__ __forceinline__ double green_h(const MenonSmem& S, const MenonCtx& c, int x, int y) {
-    return five_tap(raw_at(S, c, x - 2, y), raw_at(S, c, x - 1, y), raw_at(S, c, x, y),
-                    raw_at(S, c, x + 1, y), raw_at(S, c, x + 2, y));
+template <typename R, typename Sm>
+__device__ __forceinline__ R green_h(const Sm& S, const MenonCtx& c, int x, int y) {
+    return five_tap(raw_at<R>(S, c, x - 2, y), raw_at<R>(S, c, x - 1, y), raw_at<R>(S, c, x, y),
+                    raw_at<R>(S, c, x + 1, y), raw_at<R>(S, c, x + 2, y));
 }
-__device__ __forceinline__ double green_v(const MenonSmem& S, const MenonCtx& c, int x, int y) {
-    return five_tap(raw_at(S, c, x, y - 2), raw_at(S, c, x, y - 1), raw_at(S, c, x, y),
-                    raw_at(S, c, x, y + 1), raw_at(S, c, x, y + 2));
+template <typename R, typename Sm>
+__device__ __forceinline__ R green_v(const Sm& S, const MenonCtx& c, int x, int y) {
+    return five_tap(raw_at<R>(S, c, x, y - 2), raw_at<R>(S, c, x, y - 1), raw_at<R>(S, c, x, y),
+                    raw_at<R>(S, c, x, y + 1), raw_at<R>(S, c, x, y + 2));
 }
 
 // MenonDemosaic.cpp:148-150 pair mean of a mirrored plane.
-template <int W, int OX, int OY>
-__device__ __forceinline__ double pair_mean(const double (*p)[W], const MenonCtx& c, int x, int y,
-                                            int dx, int dy) {
-    return __dmul_rn(0.5, __dadd_rn(p[y - dy - (c.y0 + OY)][x - dx - (c.x0 + OX)],
-                                    p[y + dy - (c.y0 + OY)][x + dx - (c.x0 + OX)]));
+template <int W, int OX, int OY, typename T>
+__device__ __forceinline__ T pair_mean(const T (*p)[W], const MenonCtx& c, int x, int y, int dx, int dy) {
+    return r_mul(T(0.5), r_add(p[y - dy - (c.y0 + OY)][x - dx - (c.x0 + OX)],
+                               p[y + dy - (c.y0 + OY)][x + dx - (c.x0 + OX)]));
 }
 
-__device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, const MenonCtx& c,
+// The reference's classifier in binary64 at the site (x, y) of the general
+// path: chroma at virtual positions is the chroma of the mirrored position
+// (zero at green sites), gradients are zero at virtual positions outside the
+// active area (MenonDemosaic.cpp:107-147).
+__device__ __forceinline__ bool generic_exact_horizontal(const MenonSmemT<float>& S, const DevRaw& raw,
+                                                         const MenonCtx& c, int x, int y) {
+    auto chroma = [&](int xv, int yv, bool horizontal_axis) {
+        const int mxp = c.mx(xv), myp = c.my(yv);
+        if (color_of(raw, mxp, myp) == 1) return 0.0;
+        const double g = horizontal_axis ? green_h<double>(S, c, mxp, myp) : green_v<double>(S, c, mxp, myp);
+        return dsub(raw_at<double>(S, c, mxp, myp), g);
+    };
+    auto dh = [&](int xv, int yv) {
+        return c.inside(xv, yv) ? fabs(dsub(chroma(xv, yv, true), chroma(xv + 2, yv, true))) : 0.0;
+    };
+    auto dv = [&](int xv, int yv) {
+        return c.inside(xv, yv) ? fabs(dsub(chroma(xv, yv, false), chroma(xv, yv + 2, false))) : 0.0;
+    };
+    double h = 0.0, v = 0.0;
+    h = dadd(h, dh(x, y + 2));                     v = dadd(v, dv(x + 2, y));
+    h = dadd(h, dh(x - 2, y + 2));                 v = dadd(v, dv(x + 2, y - 2));
+    h = dadd(h, dh(x - 1, y + 1));                 v = dadd(v, dv(x + 1, y - 1));
+    h = dadd(h, __dmul_rn(3.0, dh(x, y)));         v = dadd(v, __dmul_rn(3.0, dv(x, y)));
+    h = dadd(h, __dmul_rn(3.0, dh(x - 2, y)));     v = dadd(v, __dmul_rn(3.0, dv(x, y - 2)));
+    h = dadd(h, dh(x - 1, y - 1));                 v = dadd(v, dv(x - 1, y - 1));
+    h = dadd(h, dh(x, y - 2));                     v = dadd(v, dv(x - 2, y));
+    h = dadd(h, dh(x - 2, y - 2));                 v = dadd(v, dv(x - 2, y - 2));
+    return v >= h;
+}
+
+// The general (mirrored) path.  T = double: the reference's binary64
+// arithmetic; T = float: the same operations in binary32 with exact decisions
+// (the band test and binary64 recheck of the fast path), so that an interior
+// pixel gets the same float whichever path its tile takes.
+template <typename T>
+__device__ __forceinline__ void menon_tile(MenonSmemT<T>& S, const DevRaw& raw, const MenonCtx& c,
                                            unsigned long long* ties) {
+    constexpr bool F32 = sizeof(T) == 4;
     const int t = threadIdx.x;
+    if (t == 0) S.smax_bits = 0;
     // 1. normalized raw over r=6 at mirrored positions (MenonDemosaic.cpp:106).
+    float local_max = 0.0f;
     for (int i = t; i < RAW_W * RAW_H; i += MN_THREADS) {
         const int sx = i % RAW_W, sy = i / RAW_W;
         if (!c.needed(c.x0 - 6 + sx, c.y0 - 6 + sy, 6, 6)) continue;
-        S.raw[sy][sx] = normalize_sample(raw, c.mx(c.x0 - 6 + sx), c.my(c.y0 - 6 + sy));
+        const float v = normalize_sample(raw, c.mx(c.x0 - 6 + sx), c.my(c.y0 - 6 + sy));
+        local_max = fmaxf(local_max, fabsf(v));
+        S.raw[sy][sx] = v;
+    }
+    if constexpr (F32) {
+        for (int o = 16; o; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+        __syncthreads();
+        if ((t & 31) == 0) atomicMax(&S.smax_bits, __float_as_uint(local_max));
     }
     __syncthreads();
     // 2. directional chroma (MenonDemosaic.cpp:107-119), evaluated at the
@@ -246,11 +347,11 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
         const int sx = i % CH_W, sy = i / CH_W;
         if (!c.needed(c.x0 - 4 + sx, c.y0 - 4 + sy, 4, 4)) continue;
         const int x = c.mx(c.x0 - 4 + sx), y = c.my(c.y0 - 4 + sy);
-        double h = 0.0, v = 0.0;
+        T h = 0, v = 0;
         if (color_of(raw, x, y) != 1) {
-            const double own = raw_at(S, c, x, y);
-            h = __dadd_rn(own, -green_h(S, c, x, y));
-            v = __dadd_rn(own, -green_v(S, c, x, y));
+            const T own = raw_at<T>(S, c, x, y);
+            h = r_sub(own, green_h<T>(S, c, x, y));
+            v = r_sub(own, green_v<T>(S, c, x, y));
         }
         S.ch[sy][sx] = h;
         S.cv[sy][sx] = v;
@@ -261,21 +362,22 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
         const int sx = i % DH_W, sy = i / DH_W;
         const int x = c.x0 - 4 + sx, y = c.y0 - 4 + sy;
         if (!c.needed(x, y, 2, 4)) continue;
-        double d = 0.0;
-        if (c.inside(x, y)) d = fabs(__dadd_rn(S.ch[sy][sx], -S.ch[sy][sx + 2]));
+        T d = 0;
+        if (c.inside(x, y)) d = fabs(r_sub(S.ch[sy][sx], S.ch[sy][sx + 2]));
         S.dh[sy][sx] = d;
     }
     for (int i = t; i < DV_W * DV_H; i += MN_THREADS) {
         const int sx = i % DV_W, sy = i / DV_W;
         const int x = c.x0 - 4 + sx, y = c.y0 - 4 + sy;
         if (!c.needed(x, y, 4, 2)) continue;
-        double d = 0.0;
-        if (c.inside(x, y)) d = fabs(__dadd_rn(S.cv[sy][sx], -S.cv[sy + 2][sx]));
+        T d = 0;
+        if (c.inside(x, y)) d = fabs(r_sub(S.cv[sy][sx], S.cv[sy + 2][sx]));
         S.dv[sy][sx] = d;
     }
     __syncthreads();
     // 4. classifier and green (MenonDemosaic.cpp:130-147): terms in the
     //    reference's order, horizontal wins ties (v >= h).
+    const float band_abs = F32 ? 640.0f * 5.9604644775390625e-8f * __uint_as_float(S.smax_bits) : 0.0f;
     unsigned long long local_ties = 0;
     for (int i = t; i < GR_W * GR_H; i += MN_THREADS) {
         const int sx = i % GR_W, sy = i / GR_W;
@@ -283,34 +385,42 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
         const int x = c.mx(c.x0 - 2 + sx), y = c.my(c.y0 - 2 + sy);
         if (color_of(raw, x, y) == 1) {
             S.horiz[sy][sx] = 1;
-            S.green[sy][sx] = raw_at(S, c, x, y);
+            S.green[sy][sx] = raw_at<T>(S, c, x, y);
             continue;
         }
         // dh index of (x+a, y+b): [y+b-(y0-4)][x+a-(x0-4)]
         const int hx = x - (c.x0 - 4), hy = y - (c.y0 - 4);
-        const double (*dh)[DH_W] = S.dh;
-        const double (*dv)[DV_W] = S.dv;
-        double h = 0.0, v = 0.0;
-        h = __dadd_rn(h, dh[hy + 2][hx + 0]);
-        v = __dadd_rn(v, dv[hy + 0][hx + 2]);
-        h = __dadd_rn(h, dh[hy + 2][hx - 2]);
-        v = __dadd_rn(v, dv[hy - 2][hx + 2]);
-        h = __dadd_rn(h, dh[hy + 1][hx - 1]);
-        v = __dadd_rn(v, dv[hy - 1][hx + 1]);
-        h = __dadd_rn(h, __dmul_rn(3.0, dh[hy + 0][hx + 0]));
-        v = __dadd_rn(v, __dmul_rn(3.0, dv[hy + 0][hx + 0]));
-        h = __dadd_rn(h, __dmul_rn(3.0, dh[hy + 0][hx - 2]));
-        v = __dadd_rn(v, __dmul_rn(3.0, dv[hy - 2][hx + 0]));
-        h = __dadd_rn(h, dh[hy - 1][hx - 1]);
-        v = __dadd_rn(v, dv[hy - 1][hx - 1]);
-        h = __dadd_rn(h, dh[hy - 2][hx + 0]);
-        v = __dadd_rn(v, dv[hy + 0][hx - 2]);
-        h = __dadd_rn(h, dh[hy - 2][hx - 2]);
-        v = __dadd_rn(v, dv[hy - 2][hx - 2]);
-        const bool horizontal = v >= h;
-        if (ties && v == h && sx >= 2 && sx < GR_W - 2 && sy >= 2 && sy < GR_H - 2) ++local_ties;
+        const T (*dh)[DH_W] = S.dh;
+        const T (*dv)[DV_W] = S.dv;
+        const T three = T(3);
+        T h = 0, v = 0;
+        h = r_add(h, dh[hy + 2][hx + 0]);
+        v = r_add(v, dv[hy + 0][hx + 2]);
+        h = r_add(h, dh[hy + 2][hx - 2]);
+        v = r_add(v, dv[hy - 2][hx + 2]);
+        h = r_add(h, dh[hy + 1][hx - 1]);
+        v = r_add(v, dv[hy - 1][hx + 1]);
+        h = r_add(h, r_mul(three, dh[hy + 0][hx + 0]));
+        v = r_add(v, r_mul(three, dv[hy + 0][hx + 0]));
+        h = r_add(h, r_mul(three, dh[hy + 0][hx - 2]));
+        v = r_add(v, r_mul(three, dv[hy - 2][hx + 0]));
+        h = r_add(h, dh[hy - 1][hx - 1]);
+        v = r_add(v, dv[hy - 1][hx - 1]);
+        h = r_add(h, dh[hy - 2][hx + 0]);
+        v = r_add(v, dv[hy + 0][hx - 2]);
+        h = r_add(h, dh[hy - 2][hx - 2]);
+        v = r_add(v, dv[hy - 2][hx - 2]);
+        bool horizontal = v >= h;
+        if constexpr (F32) {
+            if (near_tie(h, v, band_abs)) {
+                horizontal = generic_exact_horizontal(S, raw, c, x, y);
+                if (ties && sx >= 2 && sx < GR_W - 2 && sy >= 2 && sy < GR_H - 2) ++local_ties;
+            }
+        } else {
+            if (ties && v == h && sx >= 2 && sx < GR_W - 2 && sy >= 2 && sy < GR_H - 2) ++local_ties;
+        }
         S.horiz[sy][sx] = horizontal;
-        S.green[sy][sx] = horizontal ? green_h(S, c, x, y) : green_v(S, c, x, y);
+        S.green[sy][sx] = horizontal ? green_h<T>(S, c, x, y) : green_v<T>(S, c, x, y);
     }
     if (ties && local_ties) atomicAdd(ties, local_ties);
     __syncthreads();
@@ -320,24 +430,55 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
         if (!c.needed(c.x0 - 1 + sx, c.y0 - 1 + sy, 1, 1)) continue;
         const int x = c.mx(c.x0 - 1 + sx), y = c.my(c.y0 - 1 + sy);
         const int own = color_of(raw, x, y);
-        double rr = 0.0, bb = 0.0;
-        if (own == 0) rr = raw_at(S, c, x, y);
-        if (own == 2) bb = raw_at(S, c, x, y);
+        T rr = 0, bb = 0;
+        if (own == 0) rr = raw_at<T>(S, c, x, y);
+        if (own == 2) bb = raw_at<T>(S, c, x, y);
         if (own == 1) {
             const bool red_h = color_of(raw, x + 1, y) == 0;
             const int dx = red_h ? 1 : 0, dy = red_h ? 0 : 1;
-            const double g = S.green[y - (c.y0 - 2)][x - (c.x0 - 2)];
-            const double rm = __dmul_rn(0.5, __dadd_rn(raw_at(S, c, x - dx, y - dy), raw_at(S, c, x + dx, y + dy)));
-            const double bm = __dmul_rn(0.5, __dadd_rn(raw_at(S, c, x - dy, y - dx), raw_at(S, c, x + dy, y + dx)));
-            const double gr = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dx, dy);
-            const double gb = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dy, dx);
-            rr = __dadd_rn(__dadd_rn(g, rm), -gr);
-            bb = __dadd_rn(__dadd_rn(g, bm), -gb);
+            const T g = S.green[y - (c.y0 - 2)][x - (c.x0 - 2)];
+            const T rm = r_mul(T(0.5), r_add(raw_at<T>(S, c, x - dx, y - dy), raw_at<T>(S, c, x + dx, y + dy)));
+            const T bm = r_mul(T(0.5), r_add(raw_at<T>(S, c, x - dy, y - dx), raw_at<T>(S, c, x + dy, y + dx)));
+            const T gr = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dx, dy);
+            const T gb = pair_mean<GR_W, -2, -2>(S.green, c, x, y, dy, dx);
+            rr = r_sub(r_add(g, rm), gr);
+            bb = r_sub(r_add(g, bm), gb);
         }
         S.red[sy][sx] = rr;
         S.blue[sy][sx] = bb;
     }
     __syncthreads();
+}
+
+// Final opposite colour at R/B sites, float cast, stage program
+// (MenonDemosaic.cpp:162-173) for the general path.
+template <typename T>
+__device__ __forceinline__ void menon_tile_out(MenonSmemT<T>& S, const DevRaw& raw, const MenonCtx& c, int ox, int oy,
+                                               int ow, int oh, int stage_end, const DevProgram& P,
+                                               float* __restrict__ out, size_t out_stride, uint32_t& err,
+                                               uint8_t* dirs) {
+    for (int i = threadIdx.x; i < MN_TW * MN_TH; i += MN_THREADS) {
+        const int tx = i % MN_TW, ty = i / MN_TW;
+        const int x = c.x0 + tx, y = c.y0 + ty;
+        if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
+        const int own = color_of(raw, x, y);
+        const bool horizontal = S.horiz[ty + 2][tx + 2];
+        const int dx = horizontal ? 1 : 0, dy = horizontal ? 0 : 1;
+        T rr = S.red[ty + 1][tx + 1], bb = S.blue[ty + 1][tx + 1];
+        if (own == 2)
+            rr = r_sub(r_add(bb, pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy)),
+                       pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy));
+        if (own == 0)
+            bb = r_sub(r_add(rr, pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy)),
+                       pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy));
+        float r = (float)rr, g = (float)S.green[ty + 2][tx + 2], b = (float)bb;
+        apply_stages(P, 0, stage_end, r, g, b, err);
+        float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+        o[0] = r;
+        o[1] = g;
+        o[2] = b;
+        if (dirs) dirs[(size_t)(y - oy) * ow + (x - ox)] = horizontal;
+    }
 }
 
 // ------------------------------------------------- menon fast interior path
@@ -347,51 +488,108 @@ __device__ __forceinline__ void menon_tile(MenonSmem& S, const DevRaw& raw, cons
 // position of a 2x2 quad is a compile-time constant (template L = the Bayer
 // layout seen from the quad's top-left).  Each thread then works on whole
 // quads with constant shared-memory offsets: chroma/gradients only at the two
-// non-green sites, greens copied, every neighbour a single shared load.  The
-// arithmetic is the reference's, in binary64, in the reference's order.
+// non-green sites, greens copied, every neighbour a single shared load.
+//
+// T = double: the reference's arithmetic, in binary64, in the reference's
+// order (bit-exact outputs).  T = float: the same steps in binary32 (outputs
+// within a few ulp of the reference's float cast) with the direction decision
+// made exactly.  The binary32 classifier sums h and v are within
+//   300 u smax + 8 u h      (u = 2^-24, smax = max |sample| of the tile's
+// footprint: every five-tap green, chroma, gradient and weighted sum rounds at
+// most once per operation on values bounded by small multiples of smax), so a
+// site with |v - h| <= 640 u smax + 9 u (h + v) is re-decided by the
+// reference's classifier in binary64 (a second pass over a list of such
+// sites); every other site's binary32 decision equals the reference's.
 
 constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, full resolution, origin (-6,-6)
 constexpr int QW = (MN_TW + 8) / 2, QH = (MN_TH + 8) / 2;  // quad grid of the r=4 planes, origin (-4,-4)
 constexpr int QN = QW * QH;
 constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, full resolution, origin (-2,-2)
+constexpr int CLS_N = (QW - 2) * (QH - 2);             // quads of the r=2 region
 
 // The two non-green sites of a quad: A in the quad's first row at column
 // ax(L), B in its second row at column 1 - ax(L).  Chroma-stage planes keep
-// one value per quad and class (consecutive quads are consecutive doubles, so
+// one value per quad and class (consecutive quads are consecutive elements, so
 // a warp's accesses are bank-conflict free), halving their footprint.
 __host__ __device__ constexpr int ng_col(int l) { return l < 2 ? 0 : 1; }
 
 enum { GH_A, GH_B, GV_A, GV_B, CH_A, CH_B, CV_A, CV_B, DH_A, DH_B, DV_A, DV_B, NG_PLANES };
 
-struct FastSmem {
-    double raw[FR_H * FR_W];
-    double ng[NG_PLANES][QN];        // red and blue reuse planes 0..5 in the last stages
-    double green[FG_H * FG_W];
+template <typename T>
+struct FastSmemT {
+    T raw[FR_H * FR_W];
+    T ng[NG_PLANES][QN];        // red and blue reuse planes 0..5 in the last stages
+    T green[FG_H * FG_W];
     uint8_t horiz[FG_H * FG_W];
+    unsigned smax_bits;          // max |sample| of the footprint (float bits)
+    unsigned rechecks;           // entries of `recheck`
+    uint16_t recheck[2 * CLS_N]; // near-tie sites: quad of the r=2 region * 2 + (class B)
 };
+using FastSmem = FastSmemT<double>;
 static_assert(2 * FG_W * FG_H <= 6 * QN, "red/blue must fit in the dead chroma planes");
 
-__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double half_sum(double a, double b) { return __dmul_rn(0.5, __dadd_rn(a, b)); }
 
 // MenonDemosaic.cpp:112-115 five-tap directional green at raw index r (stride d).
-__device__ __forceinline__ double five(const double* r, int d) {
-    return dsub(dadd(half_sum(r[-d], r[d]), __dmul_rn(0.5, r[0])), __dmul_rn(0.25, dadd(r[-2 * d], r[2 * d])));
+template <typename T>
+__device__ __forceinline__ T five(const T* r, int d) {
+    return r_sub(r_add(half_sum(r[-d], r[d]), r_mul(T(0.5), r[0])), r_mul(T(0.25), r_add(r[-2 * d], r[2 * d])));
 }
 
-template <int L>
-__device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
+// The reference's classifier at one non-green site, in binary64 from the
+// binary32 samples, terms in its order (MenonDemosaic.cpp:120-147): chroma
+// C = s - five-tap green, gradients |C(p) - C(p + 2 along the axis)|,
+// horizontal iff v >= h.  raw points at the site (row stride FR_W).
+__device__ __forceinline__ bool exact_horizontal(const float* raw) {
+    auto five_d = [](const float* r, int d) {
+        return dsub(dadd(__dmul_rn(0.5, dadd((double)r[-d], (double)r[d])), __dmul_rn(0.5, (double)r[0])),
+                    __dmul_rn(0.25, dadd((double)r[-2 * d], (double)r[2 * d])));
+    };
+    auto dh = [&](int x, int y) {
+        const float* a = raw + y * FR_W + x;
+        return fabs(dsub(dsub((double)a[0], five_d(a, 1)), dsub((double)a[2], five_d(a + 2, 1))));
+    };
+    auto dv = [&](int x, int y) {
+        const float* a = raw + y * FR_W + x;
+        return fabs(dsub(dsub((double)a[0], five_d(a, FR_W)),
+                         dsub((double)a[2 * FR_W], five_d(a + 2 * FR_W, FR_W))));
+    };
+    double h = 0.0, v = 0.0;
+    h = dadd(h, dh(0, 2));                    v = dadd(v, dv(2, 0));
+    h = dadd(h, dh(-2, 2));                   v = dadd(v, dv(2, -2));
+    h = dadd(h, dh(-1, 1));                   v = dadd(v, dv(1, -1));
+    h = dadd(h, __dmul_rn(3.0, dh(0, 0)));    v = dadd(v, __dmul_rn(3.0, dv(0, 0)));
+    h = dadd(h, __dmul_rn(3.0, dh(-2, 0)));   v = dadd(v, __dmul_rn(3.0, dv(0, -2)));
+    h = dadd(h, dh(-1, -1));                  v = dadd(v, dv(-1, -1));
+    h = dadd(h, dh(0, -2));                   v = dadd(v, dv(-2, 0));
+    h = dadd(h, dh(-2, -2));                  v = dadd(v, dv(-2, -2));
+    return v >= h;
+}
+
+template <int L, typename T>
+__device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, int x0, int y0, int ox, int oy,
                                            int ow, int oh, int stage_end, const DevProgram& P,
-                                           float* __restrict__ out, size_t out_stride,
-                                           uint32_t& err) {
+                                           float* __restrict__ out, size_t out_stride, uint32_t& err,
+                                           unsigned long long* ties, uint8_t* dirs) {
+    constexpr bool F32 = sizeof(T) == 4;
     constexpr int AX = ng_col(L), BX = 1 - AX;
     const int t = threadIdx.x;
-    // 1. normalized raw (RawEngine.cpp:89-97) as binary64, r = 6 around the tile
+    if (t == 0) {
+        S.smax_bits = 0;
+        S.rechecks = 0;
+    }
+    // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile
+    float local_max = 0.0f;
 #pragma unroll 4
     for (int i = t; i < FR_W * FR_H; i += MN_THREADS) {
         const int sx = i % FR_W, sy = i / FR_W;
-        S.raw[i] = (double)normalize_sample(raw, x0 - 6 + sx, y0 - 6 + sy);
+        const float v = normalize_sample(raw, x0 - 6 + sx, y0 - 6 + sy);
+        local_max = fmaxf(local_max, fabsf(v));
+        S.raw[i] = (T)v;
+    }
+    if constexpr (F32) {
+        for (int o = 16; o; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+        __syncthreads();   // smax_bits and rechecks are zeroed
+        if ((t & 31) == 0) atomicMax(&S.smax_bits, __float_as_uint(local_max));
     }
     __syncthreads();
     // 2. directional green and chroma at the two non-green sites of every quad
@@ -399,18 +597,18 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
 #pragma unroll 2
     for (int q = t; q < QN; q += MN_THREADS) {
         const int qx = q % QW, qy = q / QW;
-        const double* ra = S.raw + (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
-        const double* rb = S.raw + (2 * qy + 3) * FR_W + 2 * qx + BX + 2;
-        const double ha = five(ra, 1), va = five(ra, FR_W);
-        const double hb = five(rb, 1), vb = five(rb, FR_W);
+        const T* ra = S.raw + (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
+        const T* rb = S.raw + (2 * qy + 3) * FR_W + 2 * qx + BX + 2;
+        const T ha = five(ra, 1), va = five(ra, FR_W);
+        const T hb = five(rb, 1), vb = five(rb, FR_W);
         S.ng[GH_A][q] = ha;
         S.ng[GV_A][q] = va;
-        S.ng[CH_A][q] = dsub(ra[0], ha);
-        S.ng[CV_A][q] = dsub(ra[0], va);
+        S.ng[CH_A][q] = r_sub(ra[0], ha);
+        S.ng[CV_A][q] = r_sub(ra[0], va);
         S.ng[GH_B][q] = hb;
         S.ng[GV_B][q] = vb;
-        S.ng[CH_B][q] = dsub(rb[0], hb);
-        S.ng[CV_B][q] = dsub(rb[0], vb);
+        S.ng[CH_B][q] = r_sub(rb[0], hb);
+        S.ng[CV_B][q] = r_sub(rb[0], vb);
     }
     __syncthreads();
     // 3. forward chroma gradients (MenonDemosaic.cpp:120-125): the same-class
@@ -419,47 +617,52 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
     for (int q = t; q < QN; q += MN_THREADS) {
         const int qx = q % QW, qy = q / QW;
         if (qx < QW - 1) {
-            S.ng[DH_A][q] = fabs(dsub(S.ng[CH_A][q], S.ng[CH_A][q + 1]));
-            S.ng[DH_B][q] = fabs(dsub(S.ng[CH_B][q], S.ng[CH_B][q + 1]));
+            S.ng[DH_A][q] = fabs(r_sub(S.ng[CH_A][q], S.ng[CH_A][q + 1]));
+            S.ng[DH_B][q] = fabs(r_sub(S.ng[CH_B][q], S.ng[CH_B][q + 1]));
         }
         if (qy < QH - 1) {
-            S.ng[DV_A][q] = fabs(dsub(S.ng[CV_A][q], S.ng[CV_A][q + QW]));
-            S.ng[DV_B][q] = fabs(dsub(S.ng[CV_B][q], S.ng[CV_B][q + QW]));
+            S.ng[DV_A][q] = fabs(r_sub(S.ng[CV_A][q], S.ng[CV_A][q + QW]));
+            S.ng[DV_B][q] = fabs(r_sub(S.ng[CV_B][q], S.ng[CV_B][q + QW]));
         }
     }
     __syncthreads();
     // 4. classifier and green (MenonDemosaic.cpp:130-147) for the quads of the r=2
     //    region, terms in the reference's order; (-1,+-1) offsets land on the other class
+    const float band_abs = F32 ? 640.0f * 5.9604644775390625e-8f * __uint_as_float(S.smax_bits) : 0.0f;
 #pragma unroll 2
-    for (int k = t; k < (QW - 2) * (QH - 2); k += MN_THREADS) {
+    for (int k = t; k < CLS_N; k += MN_THREADS) {
         const int qx = k % (QW - 2) + 1, qy = k / (QW - 2) + 1;
         const int q = qy * QW + qx;
-        const double* dhA = S.ng[DH_A];
-        const double* dhB = S.ng[DH_B];
-        const double* dvA = S.ng[DV_A];
-        const double* dvB = S.ng[DV_B];
+        const T* dhA = S.ng[DH_A];
+        const T* dhB = S.ng[DH_B];
+        const T* dvA = S.ng[DV_A];
+        const T* dvB = S.ng[DV_B];
+        const T three = T(3);
         // A site: other-class (B) quads at column offsets -(1-AX) / +AX
-        double h = 0.0, v = 0.0;
-        h = dadd(h, dhA[q + QW]);                 v = dadd(v, dvA[q + 1]);
-        h = dadd(h, dhA[q + QW - 1]);             v = dadd(v, dvA[q - QW + 1]);
-        h = dadd(h, dhB[q - BX]);                 v = dadd(v, dvB[q - QW + AX]);
-        h = dadd(h, __dmul_rn(3.0, dhA[q]));      v = dadd(v, __dmul_rn(3.0, dvA[q]));
-        h = dadd(h, __dmul_rn(3.0, dhA[q - 1]));  v = dadd(v, __dmul_rn(3.0, dvA[q - QW]));
-        h = dadd(h, dhB[q - QW - BX]);            v = dadd(v, dvB[q - QW - BX]);
-        h = dadd(h, dhA[q - QW]);                 v = dadd(v, dvA[q - 1]);
-        h = dadd(h, dhA[q - QW - 1]);             v = dadd(v, dvA[q - QW - 1]);
+        T h = 0, v = 0;
+        h = r_add(h, dhA[q + QW]);               v = r_add(v, dvA[q + 1]);
+        h = r_add(h, dhA[q + QW - 1]);           v = r_add(v, dvA[q - QW + 1]);
+        h = r_add(h, dhB[q - BX]);               v = r_add(v, dvB[q - QW + AX]);
+        h = r_add(h, r_mul(three, dhA[q]));      v = r_add(v, r_mul(three, dvA[q]));
+        h = r_add(h, r_mul(three, dhA[q - 1]));  v = r_add(v, r_mul(three, dvA[q - QW]));
+        h = r_add(h, dhB[q - QW - BX]);          v = r_add(v, dvB[q - QW - BX]);
+        h = r_add(h, dhA[q - QW]);               v = r_add(v, dvA[q - 1]);
+        h = r_add(h, dhA[q - QW - 1]);           v = r_add(v, dvA[q - QW - 1]);
         const bool hzA = v >= h;
+        if (F32 && near_tie(h, v, band_abs)) S.recheck[atomicAdd(&S.rechecks, 1u)] = (uint16_t)(2 * k);
         // B site: other-class (A) quads at column offsets -AX / +(1-AX)
-        h = 0.0; v = 0.0;
-        h = dadd(h, dhB[q + QW]);                 v = dadd(v, dvB[q + 1]);
-        h = dadd(h, dhB[q + QW - 1]);             v = dadd(v, dvB[q - QW + 1]);
-        h = dadd(h, dhA[q + QW - AX]);            v = dadd(v, dvA[q + BX]);
-        h = dadd(h, __dmul_rn(3.0, dhB[q]));      v = dadd(v, __dmul_rn(3.0, dvB[q]));
-        h = dadd(h, __dmul_rn(3.0, dhB[q - 1]));  v = dadd(v, __dmul_rn(3.0, dvB[q - QW]));
-        h = dadd(h, dhA[q - AX]);                 v = dadd(v, dvA[q - AX]);
-        h = dadd(h, dhB[q - QW]);                 v = dadd(v, dvB[q - 1]);
-        h = dadd(h, dhB[q - QW - 1]);             v = dadd(v, dvB[q - QW - 1]);
+        h = 0;
+        v = 0;
+        h = r_add(h, dhB[q + QW]);               v = r_add(v, dvB[q + 1]);
+        h = r_add(h, dhB[q + QW - 1]);           v = r_add(v, dvB[q - QW + 1]);
+        h = r_add(h, dhA[q + QW - AX]);          v = r_add(v, dvA[q + BX]);
+        h = r_add(h, r_mul(three, dhB[q]));      v = r_add(v, r_mul(three, dvB[q]));
+        h = r_add(h, r_mul(three, dhB[q - 1]));  v = r_add(v, r_mul(three, dvB[q - QW]));
+        h = r_add(h, dhA[q - AX]);               v = r_add(v, dvA[q - AX]);
+        h = r_add(h, dhB[q - QW]);               v = r_add(v, dvB[q - 1]);
+        h = r_add(h, dhB[q - QW - 1]);           v = r_add(v, dvB[q - QW - 1]);
         const bool hzB = v >= h;
+        if (F32 && near_tie(h, v, band_abs)) S.recheck[atomicAdd(&S.rechecks, 1u)] = (uint16_t)(2 * k + 1);
         // full-resolution green/direction on the r=2 grid (origin -2)
         const int ga = (2 * qy - 2) * FG_W + 2 * qx - 2 + AX;          // A site
         const int gb = (2 * qy - 1) * FG_W + 2 * qx - 2 + BX;          // B site
@@ -475,9 +678,28 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
         S.green[g1] = S.raw[(2 * qy + 3) * FR_W + 2 * qx + 2 + AX];
     }
     __syncthreads();
+    if constexpr (F32) {
+        // the near-tie sites, re-decided by the reference's binary64 classifier
+        const unsigned n = S.rechecks;
+        if (n) {
+            for (unsigned e = t; e < n; e += MN_THREADS) {
+                const int code = S.recheck[e];
+                const int k = code >> 1, cls = code & 1;
+                const int qx = k % (QW - 2) + 1, qy = k / (QW - 2) + 1;
+                const int q = qy * QW + qx;
+                const int site = cls ? (2 * qy + 3) * FR_W + 2 * qx + BX + 2 : (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
+                const bool hz = exact_horizontal(S.raw + site);
+                const int g = cls ? (2 * qy - 1) * FG_W + 2 * qx - 2 + BX : (2 * qy - 2) * FG_W + 2 * qx - 2 + AX;
+                S.horiz[g] = hz;
+                S.green[g] = hz ? S.ng[cls ? GH_B : GH_A][q] : S.ng[cls ? GV_B : GV_A][q];
+            }
+            if (ties && t == 0) atomicAdd(ties, (unsigned long long)n);
+            __syncthreads();
+        }
+    }
     // 5. red and blue on the r=1 ring (MenonDemosaic.cpp:151-161); chroma planes are dead
-    double* red = S.ng[0];
-    double* blue = S.ng[0] + FG_W * FG_H;
+    T* red = S.ng[0];
+    T* blue = S.ng[0] + FG_W * FG_H;
 #pragma unroll 2
     for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
         const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
@@ -489,18 +711,18 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
             const int pg = gy * FG_W + gx;
             const int pr = (gy + 4) * FR_W + gx + 4;
             const int own = pat(L, k);
-            double rr = 0.0, bb = 0.0;
+            T rr = 0, bb = 0;
             if (own == 0) rr = S.raw[pr];
             if (own == 2) bb = S.raw[pr];
             if (own == 1) {
                 const bool red_h = pat(L, (j << 1) | (i ^ 1)) == 0;   // colour of the row's non-green
                 const int dr = red_h ? 1 : FR_W, dg = red_h ? 1 : FG_W;
                 const int br = red_h ? FR_W : 1, bg = red_h ? FG_W : 1;
-                const double g = S.green[pg];
-                rr = dsub(dadd(g, half_sum(S.raw[pr - dr], S.raw[pr + dr])),
-                          half_sum(S.green[pg - dg], S.green[pg + dg]));
-                bb = dsub(dadd(g, half_sum(S.raw[pr - br], S.raw[pr + br])),
-                          half_sum(S.green[pg - bg], S.green[pg + bg]));
+                const T g = S.green[pg];
+                rr = r_sub(r_add(g, half_sum(S.raw[pr - dr], S.raw[pr + dr])),
+                           half_sum(S.green[pg - dg], S.green[pg + dg]));
+                bb = r_sub(r_add(g, half_sum(S.raw[pr - br], S.raw[pr + br])),
+                           half_sum(S.green[pg - bg], S.green[pg + bg]));
             }
             red[pg] = rr;
             blue[pg] = bb;
@@ -508,44 +730,49 @@ __device__ __forceinline__ void menon_fast(FastSmem& S, const DevRaw& raw, int x
     }
     __syncthreads();
     // 6. opposite colour at R/B sites, float cast (MenonDemosaic.cpp:162-173), then the
-    //    fused stages over the quad's four pixels at once
-    for (int q = t; q < (MN_TW / 2) * (MN_TH / 2); q += MN_THREADS) {
+    //    fused stages over one row pair of a quad per thread (every thread busy)
+    for (int u = t; u < (MN_TW / 2) * MN_TH; u += MN_THREADS) {
+        const int q = u >> 1, j = u & 1;
         const int qx = q % (MN_TW / 2), qy = q / (MN_TW / 2);
-        float R[4], G[4], B[4];
-        bool keep[4];
+        float R[2], G[2], B[2];
+        bool keep[2];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = k & 1, j = k >> 1;
+        for (int i = 0; i < 2; ++i) {
+            const int k = 2 * j + i;
             const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
             const int pg = (2 * qy + j + 2) * FG_W + 2 * qx + i + 2;
             const int own = pat(L, k);
             const int d = S.horiz[pg] ? 1 : FG_W;
-            double rr = red[pg], bb = blue[pg];
-            if (own == 2) rr = dsub(dadd(bb, half_sum(red[pg - d], red[pg + d])), half_sum(blue[pg - d], blue[pg + d]));
-            if (own == 0) bb = dsub(dadd(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
-            keep[k] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
+            T rr = red[pg], bb = blue[pg];
+            if (own == 2) rr = r_sub(r_add(bb, half_sum(red[pg - d], red[pg + d])), half_sum(blue[pg - d], blue[pg + d]));
+            if (own == 0) bb = r_sub(r_add(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
+            keep[i] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
             // pixels outside the viewport enter the stages as zeros (never written)
-            R[k] = keep[k] ? (float)rr : 0.0f;
-            G[k] = keep[k] ? (float)S.green[pg] : 0.0f;
-            B[k] = keep[k] ? (float)bb : 0.0f;
+            R[i] = keep[i] ? (float)rr : 0.0f;
+            G[i] = keep[i] ? (float)S.green[pg] : 0.0f;
+            B[i] = keep[i] ? (float)bb : 0.0f;
         }
-        apply_stages_n<4>(P, 0, stage_end, R, G, B, err);
+        apply_stages_n<2>(P, 0, stage_end, R, G, B, err);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (!keep[k]) continue;
-            const int x = x0 + 2 * qx + (k & 1), y = y0 + 2 * qy + (k >> 1);
+        for (int i = 0; i < 2; ++i) {
+            if (!keep[i]) continue;
+            const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
             float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
-            o[0] = R[k];
-            o[1] = G[k];
-            o[2] = B[k];
+            o[0] = R[i];
+            o[1] = G[i];
+            o[2] = B[i];
+            if (dirs) dirs[(size_t)(y - oy) * ow + (x - ox)] = S.horiz[(2 * qy + j + 2) * FG_W + 2 * qx + i + 2];
         }
     }
 }
 
 union MenonShared {
-    MenonSmem generic;
-    FastSmem fast;
+    MenonSmemT<double> generic;
+    MenonSmemT<float> generic32;
+    FastSmemT<double> fast;
+    FastSmemT<float> fast32;
 };
+
 
 // One CTA per MN_TW x MN_TH tile of the viewport, tiles anchored at an even
 // sensor coordinate.  Interior tiles take the fast quad path; tiles whose
@@ -554,61 +781,57 @@ union MenonShared {
 __device__ __forceinline__ void menon_cta(unsigned char* smem_raw, const DevRaw& raw, int x0, int y0, int ox,
                                           int oy, int ow, int oh, int layout, int stage_end, const DevProgram& P,
                                           float* __restrict__ out, size_t out_stride, unsigned long long* ties,
-                                          uint32_t& err) {
-    const bool interior = !ties && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay && x0 + MN_TW + 6 <= raw.ax + raw.aw &&
-                          y0 + MN_TH + 6 <= raw.ay + raw.ah;
-    if (interior) {
-        FastSmem& F = reinterpret_cast<MenonShared*>(smem_raw)->fast;
+                                          uint32_t& err, bool exact, uint8_t* dirs) {
+    // binary64 mode with tie counting takes the general path, which counts exact ties
+    const bool interior = !(exact && ties) && x0 - 6 >= raw.ax && y0 - 6 >= raw.ay &&
+                          x0 + MN_TW + 6 <= raw.ax + raw.aw && y0 + MN_TH + 6 <= raw.ay + raw.ah;
+    if (interior && exact) {
+        FastSmemT<double>& F = reinterpret_cast<MenonShared*>(smem_raw)->fast;
         switch (layout) {
-        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
         }
         return;
     }
-    MenonSmem& S = reinterpret_cast<MenonShared*>(smem_raw)->generic;
+    if (interior) {
+        FastSmemT<float>& F = reinterpret_cast<MenonShared*>(smem_raw)->fast32;
+        switch (layout) {
+        case 0: menon_fast<0>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        case 1: menon_fast<1>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        case 2: menon_fast<2>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        default: menon_fast<3>(F, raw, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, ties, dirs); break;
+        }
+        return;
+    }
     MenonCtx c;
     c.x0 = x0;
     c.y0 = y0;
     c.xe = min(c.x0 + MN_TW, ox + ow);
     c.ye = min(c.y0 + MN_TH, oy + oh);
     c.ax = raw.ax; c.ay = raw.ay; c.aw = raw.aw; c.ah = raw.ah;
-    menon_tile(S, raw, c, ties);
-    // 6. final opposite colour at R/B sites, float cast, stage program
-    //    (MenonDemosaic.cpp:162-173).
-    for (int i = threadIdx.x; i < MN_TW * MN_TH; i += MN_THREADS) {
-        const int tx = i % MN_TW, ty = i / MN_TW;
-        const int x = c.x0 + tx, y = c.y0 + ty;
-        if (x < ox || y < oy || x >= ox + ow || y >= oy + oh) continue;
-        const int own = color_of(raw, x, y);
-        const bool horizontal = S.horiz[ty + 2][tx + 2];
-        const int dx = horizontal ? 1 : 0, dy = horizontal ? 0 : 1;
-        double rr = S.red[ty + 1][tx + 1], bb = S.blue[ty + 1][tx + 1];
-        if (own == 2)
-            rr = __dadd_rn(__dadd_rn(bb, pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy)),
-                           -pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy));
-        if (own == 0)
-            bb = __dadd_rn(__dadd_rn(rr, pair_mean<CO_W, -1, -1>(S.blue, c, x, y, dx, dy)),
-                           -pair_mean<CO_W, -1, -1>(S.red, c, x, y, dx, dy));
-        float r = (float)rr, g = (float)S.green[ty + 2][tx + 2], b = (float)bb;
-        apply_stages(P, 0, stage_end, r, g, b, err);
-        float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
-        o[0] = r;
-        o[1] = g;
-        o[2] = b;
+    if (exact) {
+        MenonSmemT<double>& S = reinterpret_cast<MenonShared*>(smem_raw)->generic;
+        menon_tile(S, raw, c, ties);
+        menon_tile_out(S, raw, c, ox, oy, ow, oh, stage_end, P, out, out_stride, err, dirs);
+    } else {
+        MenonSmemT<float>& S = reinterpret_cast<MenonShared*>(smem_raw)->generic32;
+        menon_tile(S, raw, c, ties);
+        menon_tile_out(S, raw, c, ox, oy, ow, oh, stage_end, P, out, out_stride, err, dirs);
     }
 }
 
 __global__ void __launch_bounds__(MN_THREADS, 4)
 menon_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
              const __grid_constant__ DevProgram P, float* __restrict__ out, size_t out_stride,
-             uint32_t* status, unsigned long long* ties) {
+             uint32_t* status, unsigned long long* ties, int exact, uint8_t* dirs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int x0 = (ox & ~1) + blockIdx.x * MN_TW;
     const int y0 = (oy & ~1) + blockIdx.y * MN_TH;
     uint32_t err = 0;
-    menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, ties, err);
+    menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, ties, err, exact != 0,
+              dirs);
     report(status, err);
 }
 
@@ -670,10 +893,12 @@ __device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchP
     const DevRaw& raw = A.images[image];
     const DevProgram& P = A.programs[program];
     if (menon)
-        menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, nullptr, err);
+        menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, nullptr, err,
+                  menon == 1, nullptr);
     else
-        bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw), raw, x0, y0, ox, oy, ow, oh, layout, stage_end,
-                     P, out, out_stride, err);
+        bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw),
+                     reinterpret_cast<float*>(smem_raw + BL_OTILE_OFFSET), raw, x0, y0, ox, oy, ow, oh, layout,
+                     stage_end, P, out, out_stride, err);
 }
 
 __device__ __forceinline__ void prefetch_unit(BatchUnit* dst, const BatchUnit* src) {
@@ -738,7 +963,8 @@ static_assert(BL_THREADS == MN_THREADS, "batched tiles share one block size");
 static_assert(BATCH_MENON_TW == MN_TW && BATCH_MENON_TH == MN_TH && BATCH_BILINEAR_TW == BL_TW &&
                   BATCH_BILINEAR_TH == BL_TH,
               "batch planner tile sizes");
-static_assert(sizeof(MenonShared) >= sizeof(float) * BL_SH * BL_SW, "bilinear tile fits the batch's shared memory");
+static_assert(sizeof(MenonShared) >= BL_OTILE_OFFSET + sizeof(float) * BL_TH * BL_TW * 3,
+              "bilinear tiles fit the batch's shared memory");
 
 static_assert(sizeof(BatchParams) <= 32000, "batch launch parameters exceed the 32 KB kernel parameter limit");
 
@@ -824,20 +1050,23 @@ int quad_layout(const DevRaw& raw) {
     return 0;
 }
 
+// demosaic: 0 bilinear, 1 Menon in binary64 (bit-exact), 2 Menon in binary32
+// with exact directions.  dirs (optional, device, ow x oh) receives the Menon
+// direction of every viewport pixel (1 = horizontal; green sites 1).
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
                             int stage_end, const DevProgram& P, float* out, size_t out_stride,
                             uint32_t* status, unsigned long long* ties, cudaStream_t stream,
-                            uint32_t* launches) {
+                            uint32_t* launches, uint8_t* dirs) {
     if (ow <= 0 || oh <= 0) return cudaSuccess;
     // Menon with a singleton active-area axis is bilinear (RawEngine.cpp:303).
-    if (demosaic == 1 && raw.aw > 1 && raw.ah > 1) {
+    if (demosaic >= 1 && raw.aw > 1 && raw.ah > 1) {
         const size_t smem = sizeof(MenonShared);
         cudaError_t e = cudaFuncSetAttribute(menon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const int gx0 = ox & ~1, gy0 = oy & ~1;
         dim3 grid((ox + ow - gx0 + MN_TW - 1) / MN_TW, (oy + oh - gy0 + MN_TH - 1) / MN_TH);
         menon_kernel<<<grid, MN_THREADS, smem, stream>>>(raw, ox, oy, ow, oh, quad_layout(raw), stage_end, P, out,
-                                                         out_stride, status, ties);
+                                                         out_stride, status, ties, demosaic == 1 ? 1 : 0, dirs);
     } else {
         const int gx0 = ox & ~1, gy0 = oy & ~1;
         dim3 grid((ox + ow - gx0 + BL_TW - 1) / BL_TW, (oy + oh - gy0 + BL_TH - 1) / BL_TH);

@@ -82,29 +82,28 @@ class PointStages(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, wb, exposure, matrix, kx, ky, c0, c1, s_first, s_last):
         x = x.contiguous()
-        p = DiffPointParams()
-        wbl, ml = wb.detach().double().tolist(), matrix.detach().reshape(-1).double().tolist()
-        for i in range(3):
-            p.wb[i] = wbl[i]
-        p.exposure = float(exposure)
-        for i in range(9):
-            p.matrix[i] = ml[i]
+        scalars = torch.cat([wb.detach().reshape(3), exposure.detach().reshape(1), matrix.detach().reshape(9),
+                             s_first.detach().reshape(1), s_last.detach().reshape(1)]).float().contiguous()
         knots = [t.detach().float().contiguous() for t in (kx, ky, c0, c1)]
-        p.knots = kx.numel()
-        p.kx, p.ky, p.c0, p.c1 = (t.data_ptr() for t in knots)
-        p.slope_first, p.slope_last = float(s_first), float(s_last)
         y = torch.empty_like(x)
+        p = PointStages._params(scalars, knots)
         check(lib().re_diff_point_forward(_ptr(x), x.numel() // 3, C.byref(p), _ptr(y), _stream()))
-        ctx.save_for_backward(x, *knots)
-        ctx.p = p
+        ctx.save_for_backward(x, scalars, *knots)
         ctx.n = kx.numel()
         return y
 
     @staticmethod
+    def _params(scalars, knots):
+        p = DiffPointParams()
+        p.scalars = scalars.data_ptr()
+        p.knots = knots[0].numel()
+        p.kx, p.ky, p.c0, p.c1 = (t.data_ptr() for t in knots)
+        return p
+
+    @staticmethod
     def backward(ctx, grad):
-        x, kx, ky, c0, c1 = ctx.saved_tensors
-        p = ctx.p
-        p.kx, p.ky, p.c0, p.c1 = kx.data_ptr(), ky.data_ptr(), c0.data_ptr(), c1.data_ptr()
+        x, scalars, kx, ky, c0, c1 = ctx.saved_tensors
+        p = PointStages._params(scalars, [kx, ky, c0, c1])
         n = ctx.n
         grad = grad.contiguous()
         g = torch.zeros(int(lib().re_diff_point_grad_count(n)), dtype=torch.float64, device=x.device)
@@ -133,23 +132,23 @@ class DetailBoost(torch.autograd.Function):
     def forward(ctx, v, strength, radius: int, eps: float, space: int):
         v = v.contiguous()
         h, w = v.shape[:2]
+        k = strength.detach().float().reshape(1).contiguous()
         out = torch.empty_like(v)
-        check(lib().re_diff_detail_forward(_ptr(v), w, h, radius, eps, float(strength), space, _ptr(out),
-                                           _stream()))
-        ctx.save_for_backward(v)
-        ctx.args = (radius, eps, float(strength), space)
+        check(lib().re_diff_detail_forward(_ptr(v), w, h, radius, eps, _ptr(k), space, _ptr(out), _stream()))
+        ctx.save_for_backward(v, k)
+        ctx.args = (radius, eps, space)
         return out
 
     @staticmethod
     def backward(ctx, grad):
-        (v,) = ctx.saved_tensors
-        radius, eps, k, space = ctx.args
+        v, k = ctx.saved_tensors
+        radius, eps, space = ctx.args
         h, w = v.shape[:2]
         grad = grad.contiguous()
         dv = torch.empty_like(v)
         dk = torch.zeros(1, dtype=torch.float64, device=v.device)
-        check(lib().re_diff_detail_backward(_ptr(v), _ptr(grad), w, h, radius, eps, k, space, _ptr(dv), _ptr(dk),
-                                            _stream()))
+        check(lib().re_diff_detail_backward(_ptr(v), _ptr(grad), w, h, radius, eps, _ptr(k), space, _ptr(dv),
+                                            _ptr(dk), _stream()))
         return dv, dk.float()[0], None, None, None
 
 

@@ -21,7 +21,7 @@ from . import _capi
 from ._capi import (MAX_STAGES, Rect, RawMetadata, RenderDesc, RenderStats, ReError, Stage, check,
                     lib)
 
-BILINEAR, MENON = 0, 1
+BILINEAR, MENON, MENON_FAST = 0, 1, 2   # MENON: binary64, bit-exact; MENON_FAST: binary32, exact directions
 PROPHOTO, REC2020 = 0, 1
 FINAL, PREVIEW = 1, 0
 
@@ -298,6 +298,19 @@ def render_async(image: Image, pipe: Pipeline, viewport, out, device_status, mip
                                     C.c_void_p(device_status.data_ptr()),
                                     C.c_void_p(scratch.data_ptr() if scratch is not None else None),
                                     C.c_void_p(_stream_ptr(stream))))
+
+
+def menon_directions(image: Image, viewport, demosaic: int = MENON, out=None, stream=None):
+    """Menon direction map of a viewport (CUDA uint8, 1 = horizontal; green
+    sites 1) and the number of near-tie decisions (re_menon_directions)."""
+    import torch
+    vp = _rect(viewport)
+    if out is None:
+        out = torch.empty((vp.height, vp.width), dtype=torch.uint8, device="cuda")
+    ties = C.c_uint64()
+    check(lib().re_menon_directions(image.handle, demosaic, vp, C.c_void_p(out.data_ptr()), C.byref(ties),
+                                    C.c_void_p(_stream_ptr(stream))))
+    return out, ties.value
 
 
 def scratch_bytes(image: Image, pipe: Pipeline, viewport, mip: int) -> int:

@@ -22,6 +22,7 @@ def _meta(m, lv):
 
 
 def test_menon_frozen_fixtures_bit_exact(menon_fixtures):
+    """The binary64 policy against the reference's frozen vectors, bit for bit."""
     pipe = render.Pipeline(demosaic=render.MENON)
     for i, (m, lv, samples, expected) in enumerate(menon_fixtures):
         img = render.Image(_meta(m, lv), samples)
@@ -44,6 +45,37 @@ def test_menon_frozen_fixtures_bit_exact(menon_fixtures):
         mask[area[1]:area[1] + area[3], area[0]:area[0] + area[2]] = False
         padded[mask] = 0
         assert bits_equal(render.render(render.Image(_meta(m, lv), padded), pipe, area), exp)
+
+
+def test_menon_binary32_fixtures(menon_fixtures, oracle):
+    """The binary32 policy: every direction decision equals the reference's,
+    demosaic outputs within a few ulp of the frozen vectors, and results
+    independent of the viewport and tile size bit for bit."""
+    pipe = render.Pipeline(demosaic=render.MENON_FAST)
+    for i, (m, lv, samples, expected) in enumerate(menon_fixtures):
+        img = render.Image(_meta(m, lv), samples)
+        area = m[6:10]
+        exp = expected.reshape(area[3], area[2], 3)
+        full = render.render(img, pipe, area)
+        scale = max(1.0, float(np.abs(exp).max()))
+        within_tolerance(full / scale, exp / scale, abs_tol=1e-6, lsb16=False)
+        if area[2] > 1 and area[3] > 1:
+            raw = RawSpec(m[0], m[1], np.asarray(samples, np.uint16), m[2], m[3], m[4], m[5], tuple(area),
+                          tuple(lv[:4]), tuple(lv[4:]))
+            _, want_dirs = oracle.demosaic(raw, area, True, directions=True)
+            for policy in (render.MENON, render.MENON_FAST):
+                got_dirs, _ = render.menon_directions(img, area, policy)
+                assert np.array_equal(got_dirs.cpu().numpy(), want_dirs), (i, policy)
+        roi = (area[0] + area[2] // 3, area[1] + area[3] // 3, max(1, area[2] // 3), max(1, area[3] // 3))
+        crop = full[roi[1] - area[1]:roi[1] - area[1] + roi[3], roi[0] - area[0]:roi[0] - area[0] + roi[2]]
+        assert bits_equal(render.render(img, pipe, roi), crop), f"fixture {i} roi"
+        tile = 37 if i == 92 else 3
+        assembled = np.zeros_like(exp)
+
+        def cb(r, rgb):
+            assembled[r[1] - area[1]:r[1] - area[1] + r[3], r[0] - area[0]:r[0] - area[0] + r[2]] = rgb
+        render.render_tiles(img, pipe, area, tile, cb)
+        assert bits_equal(assembled, full), f"fixture {i} tiled"
 
 
 def _pipeline_from_golden(goldens, name, menon):
@@ -97,7 +129,8 @@ def test_chains_match_reference_renders(goldens, name, menon, exact):
 
 
 def test_random_chains_bit_exact_against_oracle(oracle):
-    """Demosaic + WB + exposure + matrix are bit-exact for any metadata."""
+    """Demosaic + WB + exposure + matrix are bit-exact for any metadata (Menon in
+    its binary64 policy; the binary32 policy within tolerance)."""
     from oracle.oracle import OP_CAMERA_TO_WORKING, OP_EXPOSURE, OP_WB, Op
     rng = np.random.default_rng(11)
     for trial in range(24):
@@ -123,6 +156,12 @@ def test_random_chains_bit_exact_against_oracle(oracle):
         vp = (vx, vy, int(rng.integers(1, ax + aw - vx + 1)), int(rng.integers(1, ay + ah - vy + 1)))
         want = oracle.render_raw(raw, menon, ops, vp)
         assert bits_equal(render.render(img, pipe, vp), want), trial
+        if menon:
+            fast = render.Pipeline(demosaic=render.MENON_FAST).white_balance(*wb).exposure(stops)
+            fast.camera_to_working(cam, 0)
+            got = render.render(img, fast, vp)
+            scale = max(1.0, float(np.abs(want).max()))
+            within_tolerance(got / scale, want / scale, abs_tol=1e-6, lsb16=False)
 
 
 def test_errors_follow_reference_exceptions():
@@ -188,6 +227,19 @@ def test_menon_24mp_properties(oracle):
         want = oracle.render_raw(raw, True, ops, crop)
         got = full[crop[1] - ay:crop[1] - ay + crop[3], crop[0] - ax:crop[0] - ax + crop[2]]
         within_tolerance(got, want)
+        _, want_dirs = oracle.demosaic(raw, crop, True, directions=True)
+        for policy in (render.MENON, render.MENON_FAST):
+            got_dirs, _ = render.menon_directions(img, crop, policy)
+            assert np.array_equal(got_dirs.cpu().numpy(), want_dirs), (crop, policy)
+    # the binary32 policy: decisions taken by the binary64 recheck, tile invariance
+    _, ties = render.menon_directions(img, w.active, render.MENON_FAST)
+    assert 0 <= ties < aw * ah // 2
+    fast = workloads.pipeline_for(w)
+    fast.demosaic = render.MENON_FAST
+    whole = render.render(img, fast, w.active)
+    for q in quads[:2]:
+        part = render.render(img, fast, q)
+        assert bits_equal(part, whole[q[1] - ay:q[1] - ay + q[3], q[0] - ax:q[0] - ax + q[2]])
     assert stats["pixels"] == aw * ah and stats["launches"] >= 1
 
 
