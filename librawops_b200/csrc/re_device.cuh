@@ -68,6 +68,74 @@ __device__ __forceinline__ float normalize_sample(const DevRaw& r, int x, int y)
     return normalize_code(r, s, (float)__ldg(r.samples + (size_t)y * r.stride + x));
 }
 
+// Normalization constants of the four positions of a 2x2 quad whose top-left
+// sample sits at an even sensor coordinate (the photosite of position k =
+// 2*j + i is then fixed by the CFA phase alone).
+struct QuadNorm {
+    float black[4], span[4], rcp[4];
+    unsigned exact;              // bit k: the reciprocal form is exact at position k
+};
+
+__device__ __forceinline__ QuadNorm quad_norm(const DevRaw& r) {
+    QuadNorm q;
+    q.exact = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int s = (int)(((((unsigned)(k >> 1)) + r.phase_y) & 1u) * 2u + ((((unsigned)(k & 1)) + r.phase_x) & 1u));
+        q.black[k] = r.black[s];
+        q.span[k] = r.span[s];
+        q.rcp[k] = r.rcp[s];
+        q.exact |= ((r.rcp_exact >> s) & 1u) << k;
+    }
+    return q;
+}
+
+// normalize_code for quad position k (same arithmetic).
+__device__ __forceinline__ float quad_normalize(const QuadNorm& q, int k, float code) {
+    const float n = __fsub_rn(code, q.black[k]);
+    if ((q.exact >> k) & 1u) {
+        const float q0 = __fmul_rn(n, q.rcp[k]);
+        const float res = __fmaf_rn(-q0, q.span[k], n);
+        return __fmaf_rn(res, q.rcp[k], q0);
+    }
+    return __fdiv_rn(n, q.span[k]);
+}
+
+// Normalized samples of QX x QY quads from the even sensor position (gx0, gy0)
+// into a row-major plane of PW x PH entries whose origin is OFF samples right
+// of and below (gx0, gy0); quad positions outside the plane are skipped.  The
+// caller guarantees every sample of the quads lies inside the sensor buffer.
+// Two samples of a quad row are read as one 32-bit word when the rows are
+// 4-byte aligned.
+template <int QX, int QY, int PW, int PH, int OFF, int THREADS, typename T>
+__device__ __forceinline__ void load_quads(T* plane, const DevRaw& raw, int gx0, int gy0, float* vmax) {
+    const QuadNorm N = quad_norm(raw);
+    const bool words = ((raw.stride & 1u) == 0) && ((reinterpret_cast<uintptr_t>(raw.samples) & 3u) == 0);
+    float m = 0.0f;
+    for (int q = threadIdx.x; q < QX * QY; q += THREADS) {
+        const int qx = q % QX, qy = q / QX;
+        const uint16_t* r0 = raw.samples + (size_t)(gy0 + 2 * qy) * raw.stride + (gx0 + 2 * qx);
+        const uint16_t* r1 = r0 + raw.stride;
+        unsigned c[4];
+        if (words) {
+            const unsigned w0 = __ldg(reinterpret_cast<const unsigned*>(r0));
+            const unsigned w1 = __ldg(reinterpret_cast<const unsigned*>(r1));
+            c[0] = w0 & 0xFFFFu; c[1] = w0 >> 16; c[2] = w1 & 0xFFFFu; c[3] = w1 >> 16;
+        } else {
+            c[0] = __ldg(r0); c[1] = __ldg(r0 + 1); c[2] = __ldg(r1); c[3] = __ldg(r1 + 1);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int px = 2 * qx + (k & 1) - OFF, py = 2 * qy + (k >> 1) - OFF;
+            if (OFF != 0 && (px < 0 || px >= PW || py < 0 || py >= PH)) continue;
+            const float v = quad_normalize(N, k, (float)c[k]);
+            m = fmaxf(m, fabsf(v));
+            plane[py * PW + px] = (T)v;
+        }
+    }
+    if (vmax) *vmax = m;
+}
+
 // MenonDemosaic.cpp:60-66 whole-sample mirror about [origin, origin+size).
 __host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size) {
     if (v >= origin && v < origin + size) return v;

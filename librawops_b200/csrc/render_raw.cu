@@ -120,17 +120,23 @@ __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], float* otile,
                                              int ox, int oy, int ow, int oh, int layout, int stage_end,
                                              const DevProgram& P, float* __restrict__ out, size_t out_stride,
                                              uint32_t& err) {
-    for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
-        const int sx = i % BL_SW, sy = i / BL_SW;
-        const int x = x0 - 1 + sx, y = y0 - 1 + sy;
-        float v = 0.0f;
-        if (x >= raw.ax && x < raw.ax + raw.aw && y >= raw.ay && y < raw.ay + raw.ah)
-            v = normalize_sample(raw, x, y);
-        tile[sy][sx] = v;
+    // interior: the halo's even-aligned quads lie inside the active area
+    const bool interior = x0 - 2 >= raw.ax && y0 - 2 >= raw.ay && x0 + BL_TW + 2 <= raw.ax + raw.aw &&
+                          y0 + BL_TH + 2 <= raw.ay + raw.ah;
+    if (interior) {
+        load_quads<BL_SW / 2 + 1, BL_SH / 2 + 1, BL_SW, BL_SH, 1, BL_THREADS>(&tile[0][0], raw, x0 - 2, y0 - 2,
+                                                                              nullptr);
+    } else {
+        for (int i = threadIdx.x; i < BL_SW * BL_SH; i += BL_THREADS) {
+            const int sx = i % BL_SW, sy = i / BL_SW;
+            const int x = x0 - 1 + sx, y = y0 - 1 + sy;
+            float v = 0.0f;
+            if (x >= raw.ax && x < raw.ax + raw.aw && y >= raw.ay && y < raw.ay + raw.ah)
+                v = normalize_sample(raw, x, y);
+            tile[sy][sx] = v;
+        }
     }
     __syncthreads();
-    const bool interior = x0 - 1 >= raw.ax && y0 - 1 >= raw.ay && x0 + BL_TW + 1 <= raw.ax + raw.aw &&
-                          y0 + BL_TH + 1 <= raw.ay + raw.ah;
     if (interior) {
         switch (layout) {
         case 0: bilinear_fast<0>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
@@ -577,15 +583,9 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         S.smax_bits = 0;
         S.rechecks = 0;
     }
-    // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile
+    // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile, as 2x2 quads
     float local_max = 0.0f;
-#pragma unroll 4
-    for (int i = t; i < FR_W * FR_H; i += MN_THREADS) {
-        const int sx = i % FR_W, sy = i / FR_W;
-        const float v = normalize_sample(raw, x0 - 6 + sx, y0 - 6 + sy);
-        local_max = fmaxf(local_max, fabsf(v));
-        S.raw[i] = (T)v;
-    }
+    load_quads<FR_W / 2, FR_H / 2, FR_W, FR_H, 0, MN_THREADS>(S.raw, raw, x0 - 6, y0 - 6, &local_max);
     if constexpr (F32) {
         for (int o = 16; o; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
         __syncthreads();   // smax_bits and rechecks are zeroed
