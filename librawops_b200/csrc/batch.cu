@@ -10,7 +10,8 @@
 // parameters; the tile records, the reduction tables and the mip scratch live in
 // one device arena owned by the batch.  A launch is a memset of the queue heads
 // and status word plus two kernel launches per group (one group unless the
-// batch holds more than 24 distinct programs or 32 images), optionally
+// batch holds more than 24 distinct programs or 32 images, or both Menon
+// policies, each of which has its own kernel), optionally
 // replayed from a CUDA graph.
 #include <cuda_runtime.h>
 
@@ -228,17 +229,20 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         std::vector<size_t> reqs;
         std::map<const DevRaw*, int> images;
         std::map<const re_render_desc*, int> programs;
+        int policy = 0;          // Menon policy of the group (0: bilinear requests only so far)
     };
     std::vector<GroupPlan> gplans(1);
     for (size_t k : order) {
         GroupPlan* g = &gplans.back();
         const bool new_image = !g->images.count(reqs[k].raw);
         const bool new_program = !g->programs.count(reqs[k].desc);
+        const int policy = reqs[k].menon;
         if ((new_image && g->images.size() == BATCH_IMAGES) ||
-            (new_program && g->programs.size() == BATCH_PROGRAMS)) {
+            (new_program && g->programs.size() == BATCH_PROGRAMS) || (policy && g->policy && policy != g->policy)) {
             gplans.emplace_back();
             g = &gplans.back();
         }
+        if (policy) g->policy = policy;
         if (!g->images.count(reqs[k].raw)) g->images.emplace(reqs[k].raw, (int)g->images.size());
         if (!g->programs.count(reqs[k].desc)) g->programs.emplace(reqs[k].desc, (int)g->programs.size());
         g->reqs.push_back(k);
@@ -364,6 +368,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         A.units = (uint32_t)T.units.size();
         A.runits = (uint32_t)T.runit_task.size();
         A.dispatch = opt.dispatch;
+        A.menon_policy = gplans[gi].policy ? (uint32_t)gplans[gi].policy : 1u;
         A.status = b->head;
         A.queue = b->head + 1 + gi;
         groups[gi].grid = A.dispatch != 1 ? (uint32_t)std::min<uint64_t>(A.units, (uint64_t)sms * opt.ctas_per_sm)

@@ -52,7 +52,8 @@ struct BatchParams {
     const ReduceTask* rtasks;
     const uint32_t* runit_task;
     uint32_t units, runits;
-    uint32_t dispatch, pad;      // 0 persistent queue, 1 one CTA per tile, 2 persistent strided + prefetch
+    uint32_t dispatch;           // 0 persistent queue, 1 one CTA per tile, 2 persistent strided + prefetch
+    uint32_t menon_policy;       // the group's Menon policy (1 binary64, 2 binary32); its kernel has only that path
     uint32_t* queue;             // next unit of this group (persistent queue)
     uint32_t* status;
 };

@@ -884,6 +884,7 @@ __global__ void mip_reduce_kernel(const float* __restrict__ native, int nw, int 
 // next tile's record into shared memory (cp.async) while the current tile
 // renders.  Each tile runs exactly the per-tile code of the single-request
 // kernels, so a batched request's pixels equal its single render bit for bit.
+template <int POLICY>
 __device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchParams& A, const BatchUnit& T,
                                            uint32_t& err) {
     const int image = T.image, program = T.program, x0 = T.x0, y0 = T.y0, ox = T.ox, oy = T.oy, ow = T.ow,
@@ -894,7 +895,7 @@ __device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchP
     const DevProgram& P = A.programs[program];
     if (menon)
         menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, nullptr, err,
-                  menon == 1, nullptr);
+                  POLICY == 1, nullptr);
     else
         bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw),
                      reinterpret_cast<float*>(smem_raw + BL_OTILE_OFFSET), raw, x0, y0, ox, oy, ow, oh, layout,
@@ -910,13 +911,14 @@ __device__ __forceinline__ void prefetch_unit(BatchUnit* dst, const BatchUnit* s
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
+template <int POLICY>
 __global__ void __launch_bounds__(MN_THREADS, 4) batch_render_kernel(const __grid_constant__ BatchParams A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) BatchUnit s_rec[2];
     __shared__ uint32_t s_unit;
     uint32_t err = 0;
     if (A.dispatch == 1) {
-        if (blockIdx.x < A.units) batch_tile(smem_raw, A, A.units_rec[blockIdx.x], err);
+        if (blockIdx.x < A.units) batch_tile<POLICY>(smem_raw, A, A.units_rec[blockIdx.x], err);
     } else if (A.dispatch == 0) {
         for (;;) {
             if (threadIdx.x == 0) s_unit = atomicAdd(A.queue, 1u);
@@ -924,7 +926,7 @@ __global__ void __launch_bounds__(MN_THREADS, 4) batch_render_kernel(const __gri
             const uint32_t u = s_unit;
             __syncthreads();
             if (u >= A.units) break;
-            batch_tile(smem_raw, A, A.units_rec[u], err);
+            batch_tile<POLICY>(smem_raw, A, A.units_rec[u], err);
             __syncthreads();
         }
     } else {
@@ -935,7 +937,7 @@ __global__ void __launch_bounds__(MN_THREADS, 4) batch_render_kernel(const __gri
             __syncthreads();
             const uint32_t next = u + gridDim.x;
             if (next < A.units) prefetch_unit(&s_rec[(i + 1) & 1], &A.units_rec[next]);
-            batch_tile(smem_raw, A, s_rec[i & 1], err);
+            batch_tile<POLICY>(smem_raw, A, s_rec[i & 1], err);
             __syncthreads();
             u = next;
         }
@@ -972,10 +974,10 @@ static_assert(sizeof(BatchParams) <= 32000, "batch launch parameters exceed the 
 cudaError_t launch_batch_group(const BatchParams& A, uint32_t grid, bool reduce, cudaStream_t stream) {
     if (!reduce) {
         const size_t smem = sizeof(MenonShared);
-        cudaError_t e =
-            cudaFuncSetAttribute(batch_render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        auto kernel = A.menon_policy == 2 ? batch_render_kernel<2> : batch_render_kernel<1>;
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        if (A.units && grid) batch_render_kernel<<<grid, MN_THREADS, smem, stream>>>(A);
+        if (A.units && grid) kernel<<<grid, MN_THREADS, smem, stream>>>(A);
     } else if (A.runits) {
         batch_reduce_kernel<<<A.runits, RD_TW * RD_TH, 0, stream>>>(A);
     }

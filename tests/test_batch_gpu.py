@@ -176,3 +176,30 @@ def test_batch_splits_into_launch_groups():
         for k, (out, w) in enumerate(zip(outs, want)):
             assert bits_equal(out.cpu().numpy(), w), (d, k)
     batch.close()
+
+
+def test_batch_mixes_menon_policies():
+    """Requests of both Menon policies (binary64 and binary32) in one batch run
+    in separate launch groups and equal their single renders bit for bit."""
+    images, recipes, tiles = _small_batch(seed=8)
+    imgs = _device_images(images)
+    pipes = []
+    for im, r in zip(images, recipes):
+        pipes.append(workloads.mixed_pipeline(im, r))
+        fast = workloads.mixed_pipeline(im, r)
+        fast.demosaic = render.MENON_FAST if fast.demosaic else 0
+        pipes.append(fast)
+    tiles = [workloads.MixedTile(t.image, 2 * t.recipe + (k % 2), t.viewport, t.mip, t.quality)
+             for k, t in enumerate(tiles)]
+    want = [render.render(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality) for t in tiles]
+    reqs, outs = _requests(imgs, pipes, tiles)
+    batch = render.Batch()
+    for d in (0, 1, 2):
+        for out in outs:
+            out.fill_(float("nan"))
+        batch.plan(reqs, dispatch=d, ctas_per_sm=4, order=1, use_graph=True)
+        batch.launch()
+        batch.status()
+        for k, (out, w) in enumerate(zip(outs, want)):
+            assert bits_equal(out.cpu().numpy(), w), (d, k)
+    batch.close()
