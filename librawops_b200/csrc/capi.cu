@@ -215,6 +215,19 @@ re_status build_program(const re_render_desc* d, DevProgram& P) {
         if (s.kind == RE_STAGE_CURVES && (s.arg > 3 || !d->curves[s.arg]))
             return fail(RE_INVALID_ARGUMENT, "curves stage without a curve set");
         P.st[i] = s;
+        if (s.kind == RE_STAGE_CURVES) {
+            // the master curve's lookup scalars and the channel identities travel
+            // with the stage (kernel parameters), so the device reads only tables
+            const DevCurveSet& h = d->curves[s.arg]->host;
+            float* f = P.st[i].f;
+            f[0] = h.c[0].identity ? 1.0f : 0.0f;
+            f[1] = (float)h.c[0].n;
+            f[2] = (float)h.c[0].ncells;
+            f[3] = h.c[0].xf[0];
+            f[4] = h.c[0].x0c;
+            f[5] = h.c[0].inv_dx;
+            for (int c = 0; c < 3; ++c) f[6 + c] = h.c[c + 1].identity ? 1.0f : 0.0f;
+        }
     }
     for (int k = 0; k < 4; ++k) P.curves[k] = d->curves[k] ? d->curves[k]->dev : nullptr;
     return RE_OK;
@@ -503,17 +516,17 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
             // cell-lookup records: cubic segments in t = (v - x_i)/h, linear ones
             // (and the extrapolations) as y_i + (v - x_i)*slope like ToneOps.cpp:826
             if (interpolation) {
-                d.rec[i] = make_float4(d.xn[i], d.inv_h[i], d.xf[i + 1], 0.0f);
-                d.rcoef[i] = d.coef[i];
+                d.rec[i].a = make_float4(d.xn[i], d.inv_h[i], d.xf[i + 1], 0.0f);
+                d.rec[i].k = d.coef[i];
             } else {
-                d.rec[i] = make_float4(d.xn[i], 1.0f, d.xf[i + 1], 0.0f);
-                d.rcoef[i] = make_float4(d.y[i], d.slope[i], 0.0f, 0.0f);
+                d.rec[i].a = make_float4(d.xn[i], 1.0f, d.xf[i + 1], 0.0f);
+                d.rec[i].k = make_float4(d.y[i], d.slope[i], 0.0f, 0.0f);
             }
         }
-        d.rec[n - 1] = make_float4(d.xn[n - 1], 1.0f, INFINITY, 0.0f);
-        d.rcoef[n - 1] = make_float4(d.y[n - 1], d.slope[n - 2], 0.0f, 0.0f);
-        d.rec[n] = make_float4(d.xn[0], 1.0f, d.xf[0], 0.0f);
-        d.rcoef[n] = make_float4(d.y[0], d.slope[0], 0.0f, 0.0f);
+        d.rec[n - 1].a = make_float4(d.xn[n - 1], 1.0f, INFINITY, 0.0f);
+        d.rec[n - 1].k = make_float4(d.y[n - 1], d.slope[n - 2], 0.0f, 0.0f);
+        d.rec[n].a = make_float4(d.xn[0], 1.0f, d.xf[0], 0.0f);
+        d.rec[n].k = make_float4(d.y[0], d.slope[0], 0.0f, 0.0f);
         // Uniform cells at most half the narrowest segment wide: every cell
         // names the segment one cell to its left (a safe lower start for the
         // device's short forward walk).  Curves needing more than 4096 cells

@@ -152,6 +152,15 @@ __host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size
 // Knot x are rounded UP to float so that `v < xf` equals the reference's
 // double comparison `v < x` for every float v; xeq holds x only when x is a
 // float (else NaN) so that `v == xeq` equals the double equality test.
+// A segment of the cell lookup: where it starts (arithmetic anchor), the scale
+// of t = (v - anchor) * scale, the next knot (RU-rounded, where the next
+// record takes over), and the power basis c0 + t(c1 + t(c2 + t c3)); both
+// halves sit in one aligned 32-byte sector.
+struct __align__(32) CurveRec {
+    float4 a;                 // {anchor, scale, next knot, 0}
+    float4 k;                 // {c0, c1, c2, c3}
+};
+
 struct DevCurve {
     uint32_t n;               // knots
     uint32_t identity;        // every knot has x == y
@@ -169,8 +178,7 @@ struct DevCurve {
     // 0..n-2 are the segments, n-1 the right and n the left linear extrapolation.
     uint32_t ncells;
     float x0c, inv_dx, pad2;
-    float4 rec[258];          // {x anchor, 1/h (1 for linear records), next knot (RU), 0}
-    float4 rcoef[258];        // power basis in t = (v - anchor) * rec.y
+    CurveRec rec[258];        // one 32-byte record per segment / extrapolation
     uint8_t cell_seg[4096];
 };
 

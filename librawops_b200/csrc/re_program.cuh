@@ -44,21 +44,29 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
 // reference's double comparisons for every float sample) finds the segment,
 // and one power-basis polynomial evaluates it.  Extrapolation and linear
 // curves are records of the same form.
-__device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
-    const int n = (int)c->n;
+__device__ __forceinline__ float curve_lookup(const DevCurve* __restrict__ c, int n, int ncells, float xf0, float x0c,
+                                              float inv_dx, float v) {
     int rec;
-    if (v < __ldg(&c->xf[0])) {
+    if (v < xf0) {
         rec = n;
     } else {
-        int cell = __float2int_rz((v - c->x0c) * c->inv_dx);
-        cell = min(max(cell, 0), (int)c->ncells - 1);
+        int cell = __float2int_rz((v - x0c) * inv_dx);
+        cell = min(max(cell, 0), ncells - 1);
         rec = __ldg(&c->cell_seg[cell]);
-        while (rec < n - 1 && v >= __ldg(&c->rec[rec].z)) ++rec;
     }
-    const float4 r = __ldg(&c->rec[rec]);
-    const float4 k = __ldg(&c->rcoef[rec]);
-    const float t = (v - r.x) * r.y;
+    float4 a = __ldg(&c->rec[rec].a);
+    float4 k = __ldg(&c->rec[rec].k);
+    while (rec < n - 1 && v >= a.z) {
+        ++rec;
+        a = __ldg(&c->rec[rec].a);
+        k = __ldg(&c->rec[rec].k);
+    }
+    const float t = (v - a.x) * a.y;
     return k.x + t * (k.y + t * (k.z + t * k.w));
+}
+
+__device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
+    return curve_lookup(c, (int)c->n, (int)c->ncells, __ldg(&c->xf[0]), c->x0c, c->inv_dx, v);
 }
 
 __device__ __forceinline__ float curve_apply(const DevCurve* __restrict__ c, float v) {
@@ -158,37 +166,27 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
     b = v[2];
 }
 
-// Cell-lookup evaluation with the curve's uniform scalars already in registers.
-struct CurveView {
+// The master curve with its lookup scalars from the stage's parameters
+// (f[0] identity, f[1] knots, f[2] cells, f[3] first knot, f[4] cell origin,
+// f[5] 1/cell width; build_program fills them).
+struct MasterCurve {
     const DevCurve* c;
     int n, ncells;
     float xf0, x0c, inv_dx;
     bool identity;
-    __device__ __forceinline__ void load(const DevCurve* curve) {
+    __device__ __forceinline__ void load(const DevCurve* curve, const float* f) {
         c = curve;
-        identity = curve->identity != 0;
-        n = (int)curve->n;
-        ncells = (int)curve->ncells;
-        xf0 = curve->xf[0];
-        x0c = curve->x0c;
-        inv_dx = curve->inv_dx;
+        identity = f[0] != 0.0f;
+        n = (int)f[1];
+        ncells = (int)f[2];
+        xf0 = f[3];
+        x0c = f[4];
+        inv_dx = f[5];
     }
     __device__ __forceinline__ float eval(float v) const {
         if (identity) return v;
         if (!ncells) return curve_map(c, v);
-        int rec;
-        if (v < xf0) {
-            rec = n;
-        } else {
-            int cell = __float2int_rz((v - x0c) * inv_dx);
-            cell = min(max(cell, 0), ncells - 1);
-            rec = __ldg(&c->cell_seg[cell]);
-            while (rec < n - 1 && v >= __ldg(&c->rec[rec].z)) ++rec;
-        }
-        const float4 r = __ldg(&c->rec[rec]);
-        const float4 k = __ldg(&c->rcoef[rec]);
-        const float t = (v - r.x) * r.y;
-        return k.x + t * (k.y + t * (k.z + t * k.w));
+        return curve_lookup(c, n, ncells, xf0, x0c, inv_dx, v);
     }
 };
 
@@ -283,20 +281,18 @@ __device__ __forceinline__ void apply_stages_n(const DevProgram& P, int begin, i
         }
         case RE_STAGE_CURVES: {
             const DevCurveSet* cs = P.curves[st.arg];
-            CurveView m, cr, cg, cb;
-            m.load(&cs->c[0]);
-            cr.load(&cs->c[1]);
-            cg.load(&cs->c[2]);
-            cb.load(&cs->c[3]);
+            MasterCurve m;
+            m.load(&cs->c[0], st.f);
+            const bool id_r = st.f[6] != 0.0f, id_g = st.f[7] != 0.0f, id_b = st.f[8] != 0.0f;
             bool bad = false;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
                 bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
                 const float mr = m.eval(r[i]), mg = m.eval(g[i]), mb = m.eval(b[i]);
                 bad |= !(isfinite(mr) && isfinite(mg) && isfinite(mb));
-                r[i] = cr.eval(mr);
-                g[i] = cg.eval(mg);
-                b[i] = cb.eval(mb);
+                r[i] = id_r ? mr : curve_apply(&cs->c[1], mr);
+                g[i] = id_g ? mg : curve_apply(&cs->c[2], mg);
+                b[i] = id_b ? mb : curve_apply(&cs->c[3], mb);
                 bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
             }
             if (bad) err = max(err, stage_key(s, ST_INVALID));
