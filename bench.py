@@ -331,8 +331,9 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "frame": f"{aw}x{ah} active of {w.width}x{w.height} BGGR stride {w.stride}",
                    "tile": w.tile,
-                   "per_launch": f"{len(tiles)} tile requests of {w.tile} (edge remainders) drained by one "
-                                 "persistent batched launch (CUDA graph)",
+                   "per_launch": f"{len(tiles)} tile requests of {w.tile} (edge remainders) as one batch "
+                                 "(CUDA graph): adjacent requests merge into one render, the autotuner picks "
+                                 "the tile-queue kernel or a plain launch per merged render",
                    "batch_options": tuned,
                    "l2": "inputs+outputs 337 MB > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{world}"},
@@ -346,7 +347,8 @@ def run_ours(args, rank, world, local_rank):
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s", "algorithmic_bytes_per_px": ALGO_BYTES_PER_PX,
-                     "kernel": "batch_render_kernel", "kernel_ms": round(kernel_ms, 5)},
+                     "kernel": "menon_kernel" if tuned["dispatch"] == 3 else "batch_render_kernel",
+                     "kernel_ms": round(kernel_ms, 5)},
         "differentiable": differentiable,
         "cpu_baseline": cpu,
         "e2e": {"value": round(world * pixels / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s",

@@ -270,7 +270,8 @@ typedef struct re_batch_item {
 typedef struct re_batch_options {
     uint32_t dispatch;          /* 0: persistent grid draining an atomic tile queue; 1: one CTA per
                                    tile; 2: persistent grid taking every grid-th tile, prefetching
-                                   the next tile's record while the current one renders */
+                                   the next tile's record while the current one renders; 3: one
+                                   plain render launch per merged render (see re_batch_plan) */
     uint32_t ctas_per_sm;       /* persistent grid = SMs x this (1..4); 0 = 4 */
     uint32_t order;             /* 0: requests in submission order; 1: Menon requests first */
     uint32_t use_graph;         /* nonzero: launches replayed from a CUDA graph */
@@ -278,6 +279,7 @@ typedef struct re_batch_options {
 
 typedef struct re_batch_info {
     uint32_t requests, reduced_requests;
+    uint32_t tasks;             /* renders after merging adjacent requests */
     uint32_t tiles;             /* phase-1 CTA tiles (queue length) */
     uint32_t reduce_blocks;     /* phase-2 blocks */
     uint32_t grid;              /* phase-1 CTAs launched */
@@ -290,9 +292,11 @@ typedef struct re_batch re_batch;
 
 RE_API re_status re_batch_create(re_batch** out);
 RE_API re_status re_batch_destroy(re_batch* batch);
-/* Validates every item like re_render_raw_async, lays out the tile queue and
- * the reduction blocks, uploads them and sizes the mip scratch (held by the
- * batch).  options may be NULL (defaults, or the autotuned choice cached for
+/* Validates every item like re_render_raw_async, merges requests of one
+ * image, description, level and row stride whose viewports tile a rectangle
+ * and whose outputs lie where one render of it would write (the pixels are the
+ * same either way), lays out the tile queue and the reduction blocks, uploads
+ * them and sizes the mip scratch (held by the batch).  options may be NULL (defaults, or the autotuned choice cached for
  * a batch of the same shape). */
 RE_API re_status re_batch_plan(re_batch* batch, const re_batch_item* items, size_t count,
                                const re_batch_options* options);
@@ -307,7 +311,8 @@ RE_API re_status re_batch_launch_per_request(re_batch* batch, void* stream);
 RE_API re_status re_batch_status(re_batch* batch, void* stream);
 RE_API re_status re_batch_info_get(const re_batch* batch, re_batch_info* info);
 /* Times the dispatch choices (queue or strided persistent grids of 2..4
- * CTAs/SM, one CTA per tile; either request order) over `reps` launches of the planned batch and re-plans
+ * CTAs/SM, one CTA per tile, either request order; plain launches per merged
+ * render) over `reps` launches of the planned batch and re-plans
  * with the fastest; the choice is cached for batches of the same shape. */
 RE_API re_status re_batch_autotune(re_batch* batch, uint32_t reps, void* stream, re_batch_options* best);
 

@@ -89,7 +89,8 @@ class BatchOptions(C.Structure):
 
 
 class BatchInfo(C.Structure):
-    _fields_ = [("requests", C.c_uint32), ("reduced_requests", C.c_uint32), ("tiles", C.c_uint32),
+    _fields_ = [("requests", C.c_uint32), ("reduced_requests", C.c_uint32), ("tasks", C.c_uint32),
+                ("tiles", C.c_uint32),
                 ("reduce_blocks", C.c_uint32), ("grid", C.c_uint32), ("native_pixels", C.c_uint64),
                 ("output_pixels", C.c_uint64), ("raw_bytes", C.c_uint64), ("output_bytes", C.c_uint64),
                 ("options", BatchOptions)]

@@ -67,7 +67,9 @@ struct LaunchGroup {
 struct re_batch {
     BatchShape shape{};
     std::vector<re_batch_item> items;
-    std::vector<PerRequest> singles;
+    std::vector<PerRequest> singles;       // the requests as given
+    std::vector<PerRequest> directs;       // the merged renders
+    bool direct = false;                   // dispatch 3: plain launches of the merged renders
     std::vector<LaunchGroup> groups;
     re_batch_options opt{};
     re_batch_info info{};
@@ -125,11 +127,83 @@ void release_graph(re_batch* b) {
     b->graph = nullptr;
 }
 
+// One plain launch sequence per render (demosaic, then the mip reduction).
+re_status launch_singles(re_batch* b, const std::vector<PerRequest>& list, cudaStream_t stream) {
+    uint32_t* status = b->head;
+    if (!list.empty()) BT_CUDA(cudaMemsetAsync(b->head, 0, b->head_words * sizeof(uint32_t), stream));
+    for (const PerRequest& q : list) {
+        const DevProgram& P = q.program;
+        if (!q.mip) {
+            BT_CUDA(launch_demosaic(q.demosaic, q.raw, (int)q.viewport.x, (int)q.viewport.y, (int)q.viewport.width,
+                                    (int)q.viewport.height, (int)P.count, P, q.out, q.out_stride, status, nullptr,
+                                    stream, nullptr));
+            continue;
+        }
+        const size_t nstride = (size_t)q.native.width * 3;
+        BT_CUDA(launch_demosaic(q.demosaic, q.raw, (int)q.native.x, (int)q.native.y, (int)q.native.width,
+                                (int)q.native.height, P.anchor + 1, P, q.scratch, nstride, status, nullptr, stream,
+                                nullptr));
+        BT_CUDA(launch_mip_reduce(q.scratch, (int)q.native.width, (int)q.native.height, nstride, (int)q.mip,
+                                  (int)q.viewport.width, (int)q.viewport.height, P.anchor + 1, (int)P.count, P,
+                                  q.out, q.out_stride, status, stream, nullptr));
+    }
+    return RE_OK;
+}
+
 re_status enqueue(re_batch* b, cudaStream_t stream) {
+    if (b->direct) return launch_singles(b, b->directs, stream);
     BT_CUDA(cudaMemsetAsync(b->head, 0, b->head_words * sizeof(uint32_t), stream));
     for (const LaunchGroup& g : b->groups) BT_CUDA(launch_batch_group(g.params, g.grid, false, stream));
     for (const LaunchGroup& g : b->groups) BT_CUDA(launch_batch_group(g.params, 0, true, stream));
     return RE_OK;
+}
+
+// Requests of one image, description, level and output row stride whose
+// viewports tile a rectangle and whose outputs sit where one render of that
+// rectangle would write them merge into that one render (results do not depend
+// on how a viewport is cut, so the pixels are the same): first along rows,
+// then along columns.
+std::vector<re_batch_item> merge_items(std::vector<re_batch_item> v) {
+    auto same = [](const re_batch_item& a, const re_batch_item& b) {
+        return a.image == b.image && a.desc == b.desc && a.mip == b.mip && a.quality == b.quality &&
+               a.out_row_stride == b.out_row_stride;
+    };
+    auto key = [](const re_batch_item& a) {
+        return std::make_tuple((uintptr_t)a.image, (uintptr_t)a.desc, a.mip, a.quality, a.out_row_stride);
+    };
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool rows = pass == 0;
+        std::sort(v.begin(), v.end(), [&](const re_batch_item& a, const re_batch_item& b) {
+            const auto ka = key(a), kb = key(b);
+            if (ka != kb) return ka < kb;
+            if (rows) return std::make_tuple(a.viewport.y, a.viewport.height, a.viewport.x) <
+                             std::make_tuple(b.viewport.y, b.viewport.height, b.viewport.x);
+            return std::make_tuple(a.viewport.x, a.viewport.width, a.viewport.y) <
+                   std::make_tuple(b.viewport.x, b.viewport.width, b.viewport.y);
+        });
+        std::vector<re_batch_item> out;
+        for (const re_batch_item& it : v) {
+            if (!out.empty()) {
+                re_batch_item& a = out.back();
+                const bool adjacent =
+                    same(a, it) &&
+                    (rows ? (a.viewport.y == it.viewport.y && a.viewport.height == it.viewport.height &&
+                             (uint64_t)a.viewport.x + a.viewport.width == it.viewport.x &&
+                             it.out == a.out + (size_t)a.viewport.width * 3)
+                          : (a.viewport.x == it.viewport.x && a.viewport.width == it.viewport.width &&
+                             (uint64_t)a.viewport.y + a.viewport.height == it.viewport.y &&
+                             it.out == a.out + (size_t)a.viewport.height * a.out_row_stride));
+                if (adjacent) {
+                    if (rows) a.viewport.width += it.viewport.width;
+                    else a.viewport.height += it.viewport.height;
+                    continue;
+                }
+            }
+            out.push_back(it);
+        }
+        v = std::move(out);
+    }
+    return v;
 }
 
 }  // namespace
@@ -166,19 +240,17 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         int menon, layout, stage_end, mip;
         uint32_t tiles_x, tiles;
     };
-    std::vector<Req> reqs;
     re_batch_info info{};
-    for (size_t i = 0; i < count; ++i) {
-        const re_batch_item& it = copy[i];
+    auto describe = [&](const re_batch_item& it, size_t index, Req& r) -> re_status {
         if (!it.image || !it.desc) return fail(RE_INVALID_ARGUMENT, "null render arguments");
-        Req r{};
+        r = Req{};
         re_status s = render_plan(it.image, it.desc, it.viewport, it.mip, it.quality, r.program, r.native, &r.raw);
         if (s) return s;
-        if (!it.viewport.width || !it.viewport.height) continue;
+        if (!it.viewport.width || !it.viewport.height) return RE_OK;
         if (!it.out) return fail(RE_INVALID_ARGUMENT, "null render arguments");
         if (it.out_row_stride < (size_t)it.viewport.width * 3)
             return fail(RE_INVALID_ARGUMENT, "output row stride too small");
-        r.item = i;
+        r.item = index;
         r.desc = it.desc;
         r.mip = (int)it.mip;
         r.menon = it.desc->demosaic >= 1 && r.raw->aw > 1 && r.raw->ah > 1 ? (int)it.desc->demosaic : 0;
@@ -190,12 +262,31 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         r.tiles_x = (uint32_t)(((int)(r.native.x + r.native.width) - gx0 + tw - 1) / tw);
         const uint32_t tiles_y = (uint32_t)(((int)(r.native.y + r.native.height) - gy0 + th - 1) / th);
         r.tiles = r.tiles_x * tiles_y;
-        reqs.push_back(r);
+        return RE_OK;
+    };
+    // the requests as given (validated; the per-request form renders these)
+    std::vector<Req> orig;
+    std::vector<re_batch_item> valid;
+    for (size_t i = 0; i < count; ++i) {
+        Req r;
+        re_status s = describe(copy[i], i, r);
+        if (s) return s;
+        if (!copy[i].viewport.width || !copy[i].viewport.height) continue;
+        orig.push_back(r);
+        valid.push_back(copy[i]);
         info.native_pixels += (uint64_t)r.native.width * r.native.height;
-        info.output_pixels += (uint64_t)it.viewport.width * it.viewport.height;
-        info.reduced_requests += it.mip ? 1 : 0;
+        info.output_pixels += (uint64_t)copy[i].viewport.width * copy[i].viewport.height;
+        info.reduced_requests += copy[i].mip ? 1 : 0;
     }
-    info.requests = (uint32_t)reqs.size();
+    info.requests = (uint32_t)orig.size();
+    // the renders the batch performs: adjacent requests merged
+    const std::vector<re_batch_item> merged = merge_items(valid);
+    std::vector<Req> reqs(merged.size());
+    for (size_t i = 0; i < merged.size(); ++i) {
+        re_status s = describe(merged[i], i, reqs[i]);
+        if (s) return s;
+    }
+    info.tasks = (uint32_t)reqs.size();
     uint64_t tiles = 0, menon_tiles = 0;
     for (const Req& r : reqs) {
         tiles += r.tiles;
@@ -216,7 +307,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         auto t = g_tuned.find(shape);
         if (t != g_tuned.end()) opt = t->second;
     }
-    if (opt.dispatch > 2 || opt.ctas_per_sm > 4 || opt.order > 1)
+    if (opt.dispatch > 3 || opt.ctas_per_sm > 4 || opt.order > 1)
         return fail(RE_INVALID_ARGUMENT, "invalid batch options");
     if (!opt.ctas_per_sm) opt.ctas_per_sm = 4;
     // 3. queue order, then launch groups of at most BATCH_PROGRAMS programs and
@@ -250,11 +341,16 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
     if (gplans.back().reqs.empty()) gplans.pop_back();
     // 4. host tables of every group
     size_t scratch_bytes = 0;
-    std::vector<size_t> scratch_off(reqs.size(), 0);
+    std::vector<size_t> scratch_off(reqs.size(), 0), orig_scratch_off(orig.size(), 0);
     for (size_t k = 0; k < reqs.size(); ++k)
         if (reqs[k].mip) {
             scratch_off[k] = scratch_bytes;
             scratch_bytes += align256((size_t)reqs[k].native.width * reqs[k].native.height * 3 * sizeof(float));
+        }
+    for (size_t k = 0; k < orig.size(); ++k)
+        if (orig[k].mip) {
+            orig_scratch_off[k] = scratch_bytes;
+            scratch_bytes += align256((size_t)orig[k].native.width * orig[k].native.height * 3 * sizeof(float));
         }
     struct GroupTables {
         std::vector<BatchUnit> units;
@@ -268,7 +364,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         GroupTables& T = tabs[gi];
         for (size_t k : gplans[gi].reqs) {
             const Req& r = reqs[k];
-            const re_batch_item& it = copy[r.item];
+            const re_batch_item& it = merged[r.item];
             BatchUnit t{};
             t.image = gplans[gi].images.at(r.raw);
             t.program = gplans[gi].programs.at(r.desc);
@@ -341,6 +437,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
     }
     char* base = b->dev;
     auto scratch_of = [&](size_t k) { return reinterpret_cast<float*>(base + o_scratch + scratch_off[k]); };
+    auto orig_scratch_of = [&](size_t k) { return reinterpret_cast<float*>(base + o_scratch + orig_scratch_off[k]); };
     auto put = [&](size_t at, const void* src, size_t bytes) -> cudaError_t {
         return bytes ? cudaMemcpy(base + at, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
     };
@@ -389,6 +486,28 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
     info.options = opt;
     b->info = info;
     b->shape = shape;
+    // 7. the requests as single-request launches (re_batch_launch_per_request),
+    //    and the merged renders as plain launches (dispatch 3)
+    auto single = [&](const Req& r, const re_batch_item& it, float* scratch) {
+        PerRequest q{};
+        q.raw = *r.raw;
+        q.program = r.program;
+        q.demosaic = it.desc->demosaic;
+        q.mip = it.mip;
+        q.viewport = it.viewport;
+        q.native = r.native;
+        q.out = it.out;
+        q.out_stride = it.out_row_stride;
+        q.scratch = scratch;
+        return q;
+    };
+    b->singles.clear();
+    for (size_t k = 0; k < orig.size(); ++k)
+        b->singles.push_back(single(orig[k], b->items[orig[k].item], orig[k].mip ? orig_scratch_of(k) : nullptr));
+    b->directs.clear();
+    for (size_t k = 0; k < reqs.size(); ++k)
+        b->directs.push_back(single(reqs[k], merged[reqs[k].item], reqs[k].mip ? scratch_of(k) : nullptr));
+    b->direct = opt.dispatch == 3;
     // 6. CUDA graph of the launch sequence
     release_graph(b);
     if (opt.use_graph && !b->groups.empty()) {
@@ -405,49 +524,13 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         b->graph = g;
         BT_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
     }
-    // 7. the same requests as single-request launches (re_batch_launch_per_request)
-    b->singles.clear();
-    for (size_t k = 0; k < reqs.size(); ++k) {
-        const Req& r = reqs[k];
-        const re_batch_item& it = b->items[r.item];
-        PerRequest q{};
-        q.raw = *r.raw;
-        q.program = r.program;
-        q.demosaic = it.desc->demosaic;
-        q.mip = it.mip;
-        q.viewport = it.viewport;
-        q.native = r.native;
-        q.out = it.out;
-        q.out_stride = it.out_row_stride;
-        q.scratch = r.mip ? scratch_of(k) : nullptr;
-        b->singles.push_back(q);
-    }
     b->planned = true;
     return RE_OK;
 }
 
 re_status re_batch_launch_per_request(re_batch* b, void* stream_) {
     if (!b || !b->planned) return fail(RE_INVALID_ARGUMENT, "batch is not planned");
-    cudaStream_t stream = (cudaStream_t)stream_;
-    uint32_t* status = b->head;
-    if (!b->singles.empty()) BT_CUDA(cudaMemsetAsync(b->head, 0, b->head_words * sizeof(uint32_t), stream));
-    for (const PerRequest& q : b->singles) {
-        const DevProgram& P = q.program;
-        if (!q.mip) {
-            BT_CUDA(launch_demosaic(q.demosaic, q.raw, (int)q.viewport.x, (int)q.viewport.y, (int)q.viewport.width,
-                                    (int)q.viewport.height, (int)P.count, P, q.out, q.out_stride, status, nullptr,
-                                    stream, nullptr));
-            continue;
-        }
-        const size_t nstride = (size_t)q.native.width * 3;
-        BT_CUDA(launch_demosaic(q.demosaic, q.raw, (int)q.native.x, (int)q.native.y, (int)q.native.width,
-                                (int)q.native.height, P.anchor + 1, P, q.scratch, nstride, status, nullptr, stream,
-                                nullptr));
-        BT_CUDA(launch_mip_reduce(q.scratch, (int)q.native.width, (int)q.native.height, nstride, (int)q.mip,
-                                  (int)q.viewport.width, (int)q.viewport.height, P.anchor + 1, (int)P.count, P,
-                                  q.out, q.out_stride, status, stream, nullptr));
-    }
-    return RE_OK;
+    return launch_singles(b, b->singles, (cudaStream_t)stream_);
 }
 
 re_status re_batch_launch(re_batch* b, void* stream_) {
@@ -490,6 +573,7 @@ re_status re_batch_autotune(re_batch* b, uint32_t reps, void* stream_, re_batch_
         }
         cands.push_back({1, 4, order, graph});
     }
+    cands.push_back({3, 4, 0, graph});
     cudaEvent_t e0, e1;
     BT_CUDA(cudaEventCreate(&e0));
     BT_CUDA(cudaEventCreate(&e1));

@@ -405,7 +405,7 @@ class Batch:
         i = _capi.BatchInfo()
         check(lib().re_batch_info_get(self.handle, C.byref(i)))
         o = i.options
-        return {"requests": i.requests, "reduced_requests": i.reduced_requests, "tiles": i.tiles,
+        return {"requests": i.requests, "reduced_requests": i.reduced_requests, "tasks": i.tasks, "tiles": i.tiles,
                 "reduce_blocks": i.reduce_blocks, "grid": i.grid, "native_pixels": i.native_pixels,
                 "output_pixels": i.output_pixels, "raw_bytes": i.raw_bytes, "output_bytes": i.output_bytes,
                 "options": {"dispatch": o.dispatch, "ctas_per_sm": o.ctas_per_sm, "order": o.order,

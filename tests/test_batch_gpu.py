@@ -203,3 +203,47 @@ def test_batch_mixes_menon_policies():
         for k, (out, w) in enumerate(zip(outs, want)):
             assert bits_equal(out.cpu().numpy(), w), (d, k)
     batch.close()
+
+
+def test_batch_merges_tiles_of_one_render():
+    """Tiles of one viewport written into one frame (the reference renderer's
+    render_image) merge into one render per viewport; the frame equals the
+    single render under every dispatch choice."""
+    images, recipes, _ = _small_batch(seed=13)
+    imgs = _device_images(images)
+    pipes = [workloads.mixed_pipeline(im, r) for im, r in zip(images, recipes)]
+    frames, reqs, wants = [], [], []
+    for i, img in enumerate(images):
+        ax, ay, aw, ah = img.active
+        for mip, quality in ((0, 1), (1, 0)):
+            s = 1 << mip
+            lw, lh = (aw, ah) if mip == 0 else (-(-aw // s), -(-ah // s))
+            ox0, oy0 = (ax, ay) if mip == 0 else (0, 0)
+            vp = (ox0 + 3, oy0 + 2, lw - 5, lh - 4)
+            frame = torch.full((vp[3], vp[2], 3), float("nan"), device="cuda")
+            frames.append(frame)
+            wants.append(render.render(imgs[i], pipes[i], vp, mip, quality))
+            t = 41
+            for y in range(vp[1], vp[1] + vp[3], t):
+                for x in range(vp[0], vp[0] + vp[2], t):
+                    w_, h_ = min(t, vp[0] + vp[2] - x), min(t, vp[1] + vp[3] - y)
+                    part = frame[y - vp[1]:y - vp[1] + h_, x - vp[0]:x - vp[0] + w_]
+                    reqs.append((imgs[i], pipes[i], (x, y, w_, h_), mip, quality, part))
+    batch = render.Batch()
+    for d in (0, 1, 2, 3):
+        for f in frames:
+            f.fill_(float("nan"))
+        batch.plan(reqs, dispatch=d, ctas_per_sm=4, order=1, use_graph=bool(d % 2))
+        info = batch.info()
+        assert info["requests"] == len(reqs) and info["tasks"] == len(frames), info
+        batch.launch()
+        batch.status()
+        for f, w in zip(frames, wants):
+            assert bits_equal(f.cpu().numpy(), w), d
+    for f in frames:
+        f.fill_(float("nan"))
+    batch.launch_per_request()
+    batch.status()
+    for f, w in zip(frames, wants):
+        assert bits_equal(f.cpu().numpy(), w)
+    batch.close()
