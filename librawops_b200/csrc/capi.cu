@@ -529,8 +529,9 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
         d.rec[n].k = make_float4(d.y[0], d.slope[0], 0.0f, 0.0f);
         // Uniform cells at most half the narrowest segment wide: every cell
         // names the segment one cell to its left (a safe lower start for the
-        // device's short forward walk).  Curves needing more than 4096 cells
-        // keep the binary search.
+        // device's short forward walk) and the knot ending it, so one
+        // comparison nearly always lands on the sample's segment.  Curves
+        // needing more than 4096 cells keep the binary search.
         const double span = x[n - 1] - x[0];
         const double cells = std::ceil(span / (0.5 * min_h));
         d.ncells = 0;
@@ -544,7 +545,8 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
                 const double left = x[0] + (double(c) - 1.0) * dx;
                 uint32_t seg = 0;
                 while (seg + 2 < n && (double)d.xf[seg + 1] <= left) ++seg;
-                d.cell_seg[c] = (uint8_t)seg;
+                d.cell[c].seg = seg;
+                d.cell[c].next = d.xf[seg + 1];
             }
         }
     }

@@ -101,29 +101,38 @@ __device__ __forceinline__ float quad_normalize(const QuadNorm& q, int k, float 
     return __fdiv_rn(n, q.span[k]);
 }
 
+// The four sample codes of the 2x2 quad at the even sensor position (gx, gy);
+// two samples of a quad row are read as one 32-bit word when `words` (rows
+// 4-byte aligned).
+__device__ __forceinline__ void quad_codes(const DevRaw& raw, bool words, int gx, int gy, unsigned (&c)[4]) {
+    const uint16_t* r0 = raw.samples + (size_t)gy * raw.stride + gx;
+    const uint16_t* r1 = r0 + raw.stride;
+    if (words) {
+        const unsigned w0 = __ldg(reinterpret_cast<const unsigned*>(r0));
+        const unsigned w1 = __ldg(reinterpret_cast<const unsigned*>(r1));
+        c[0] = w0 & 0xFFFFu; c[1] = w0 >> 16; c[2] = w1 & 0xFFFFu; c[3] = w1 >> 16;
+    } else {
+        c[0] = __ldg(r0); c[1] = __ldg(r0 + 1); c[2] = __ldg(r1); c[3] = __ldg(r1 + 1);
+    }
+}
+
+__device__ __forceinline__ bool quad_words(const DevRaw& raw) {
+    return ((raw.stride & 1u) == 0) && ((reinterpret_cast<uintptr_t>(raw.samples) & 3u) == 0);
+}
+
 // Normalized samples of QX x QY quads from the even sensor position (gx0, gy0)
 // into a row-major plane of PW x PH entries whose origin is OFF samples right
 // of and below (gx0, gy0); quad positions outside the plane are skipped.  The
 // caller guarantees every sample of the quads lies inside the sensor buffer.
-// Two samples of a quad row are read as one 32-bit word when the rows are
-// 4-byte aligned.
 template <int QX, int QY, int PW, int PH, int OFF, int THREADS, typename T>
 __device__ __forceinline__ void load_quads(T* plane, const DevRaw& raw, int gx0, int gy0, float* vmax) {
     const QuadNorm N = quad_norm(raw);
-    const bool words = ((raw.stride & 1u) == 0) && ((reinterpret_cast<uintptr_t>(raw.samples) & 3u) == 0);
+    const bool words = quad_words(raw);
     float m = 0.0f;
     for (int q = threadIdx.x; q < QX * QY; q += THREADS) {
         const int qx = q % QX, qy = q / QX;
-        const uint16_t* r0 = raw.samples + (size_t)(gy0 + 2 * qy) * raw.stride + (gx0 + 2 * qx);
-        const uint16_t* r1 = r0 + raw.stride;
         unsigned c[4];
-        if (words) {
-            const unsigned w0 = __ldg(reinterpret_cast<const unsigned*>(r0));
-            const unsigned w1 = __ldg(reinterpret_cast<const unsigned*>(r1));
-            c[0] = w0 & 0xFFFFu; c[1] = w0 >> 16; c[2] = w1 & 0xFFFFu; c[3] = w1 >> 16;
-        } else {
-            c[0] = __ldg(r0); c[1] = __ldg(r0 + 1); c[2] = __ldg(r1); c[3] = __ldg(r1 + 1);
-        }
+        quad_codes(raw, words, gx0 + 2 * qx, gy0 + 2 * qy, c);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int px = 2 * qx + (k & 1) - OFF, py = 2 * qy + (k >> 1) - OFF;
@@ -131,6 +140,28 @@ __device__ __forceinline__ void load_quads(T* plane, const DevRaw& raw, int gx0,
             const float v = quad_normalize(N, k, (float)c[k]);
             m = fmaxf(m, fabsf(v));
             plane[py * PW + px] = (T)v;
+        }
+    }
+    if (vmax) *vmax = m;
+}
+
+// The same samples by quad position: planes[k][q] holds position k = 2*j + i
+// of quad q (row-major over the QX x QY quads).
+template <int QX, int QY, int THREADS, typename T>
+__device__ __forceinline__ void load_quad_planes(T (*planes)[QX * QY], const DevRaw& raw, int gx0, int gy0,
+                                                 float* vmax) {
+    const QuadNorm N = quad_norm(raw);
+    const bool words = quad_words(raw);
+    float m = 0.0f;
+    for (int q = threadIdx.x; q < QX * QY; q += THREADS) {
+        const int qx = q % QX, qy = q / QX;
+        unsigned c[4];
+        quad_codes(raw, words, gx0 + 2 * qx, gy0 + 2 * qy, c);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float v = quad_normalize(N, k, (float)c[k]);
+            m = fmaxf(m, fabsf(v));
+            planes[k][q] = (T)v;
         }
     }
     if (vmax) *vmax = m;
@@ -148,10 +179,6 @@ __host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size
 
 // ---------------------------------------------------------------- curves
 
-// One ExtendedCurves curve prepared for float32 evaluation (ToneOps.cpp:795-832).
-// Knot x are rounded UP to float so that `v < xf` equals the reference's
-// double comparison `v < x` for every float v; xeq holds x only when x is a
-// float (else NaN) so that `v == xeq` equals the double equality test.
 // A segment of the cell lookup: where it starts (arithmetic anchor), the scale
 // of t = (v - anchor) * scale, the next knot (RU-rounded, where the next
 // record takes over), and the power basis c0 + t(c1 + t(c2 + t c3)); both
@@ -161,6 +188,18 @@ struct __align__(32) CurveRec {
     float4 k;                 // {c0, c1, c2, c3}
 };
 
+// A cell of the uniform lookup grid: a segment at or below every sample that
+// falls in the cell, and the RU-rounded knot where that segment ends (a sample
+// at or above it starts one segment later).
+struct __align__(8) CurveCell {
+    float next;
+    uint32_t seg;
+};
+
+// One ExtendedCurves curve prepared for float32 evaluation (ToneOps.cpp:795-832).
+// Knot x are rounded UP to float so that `v < xf` equals the reference's
+// double comparison `v < x` for every float v; xeq holds x only when x is a
+// float (else NaN) so that `v == xeq` equals the double equality test.
 struct DevCurve {
     uint32_t n;               // knots
     uint32_t identity;        // every knot has x == y
@@ -173,13 +212,13 @@ struct DevCurve {
     float slope[256];         // segment slopes (linear segments and extrapolation)
     float4 coef[256];         // power-basis cubic per segment: c0 + t(c1 + t(c2 + t c3))
     float inv_h[256];         // 1 / (x[i+1] - x[i])
-    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none),
-    // each naming a segment at or below every sample that falls in it; records
-    // 0..n-2 are the segments, n-1 the right and n the left linear extrapolation.
+    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none);
+    // records 0..n-2 are the segments, n-1 the right and n the left linear
+    // extrapolation.
     uint32_t ncells;
     float x0c, inv_dx, pad2;
     CurveRec rec[258];        // one 32-byte record per segment / extrapolation
-    uint8_t cell_seg[4096];
+    CurveCell cell[4096];
 };
 
 struct DevCurveSet {

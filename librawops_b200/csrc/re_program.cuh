@@ -39,34 +39,46 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
     return k.x + t * (k.y + t * (k.z + t * k.w));
 }
 
-// Cell lookup (DevCurve::ncells > 0): the cell gives a segment at or below
-// the sample, a short walk over the RU-rounded knots (which equals the
-// reference's double comparisons for every float sample) finds the segment,
-// and one power-basis polynomial evaluates it.  Extrapolation and linear
-// curves are records of the same form.
-__device__ __forceinline__ float curve_lookup(const DevCurve* __restrict__ c, int n, int ncells, float xf0, float x0c,
-                                              float inv_dx, float v) {
-    int rec;
-    if (v < xf0) {
-        rec = n;
-    } else {
-        int cell = __float2int_rz((v - x0c) * inv_dx);
+// Cell lookup (DevCurve::ncells > 0) of M samples at once: the cell gives a
+// segment at or below the sample and the knot ending it, one comparison steps
+// over that knot, a short walk over the RU-rounded knots (which equals the
+// reference's double comparisons for every float sample) covers the rare
+// sample further right, and one power-basis polynomial evaluates the segment.
+// Extrapolation and linear curves are records of the same form.  The loads of
+// all M samples are issued before any of them is used.
+template <int M>
+__device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, int n, int ncells, float xf0,
+                                               float x0c, float inv_dx, float* v) {
+    int rec[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        int cell = __float2int_rz((v[i] - x0c) * inv_dx);
         cell = min(max(cell, 0), ncells - 1);
-        rec = __ldg(&c->cell_seg[cell]);
+        const uint2 e = __ldg(reinterpret_cast<const uint2*>(&c->cell[cell]));
+        rec[i] = v[i] < xf0 ? n : (int)e.y + (v[i] >= __uint_as_float(e.x) ? 1 : 0);
     }
-    float4 a = __ldg(&c->rec[rec].a);
-    float4 k = __ldg(&c->rec[rec].k);
-    while (rec < n - 1 && v >= a.z) {
-        ++rec;
-        a = __ldg(&c->rec[rec].a);
-        k = __ldg(&c->rec[rec].k);
+    float t[M];
+    {
+        float4 a[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) a[i] = __ldg(&c->rec[rec[i]].a);
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            while (rec[i] < n - 1 && v[i] >= a[i].z) a[i] = __ldg(&c->rec[++rec[i]].a);
+            t[i] = (v[i] - a[i].x) * a[i].y;
+        }
     }
-    const float t = (v - a.x) * a.y;
-    return k.x + t * (k.y + t * (k.z + t * k.w));
+    float4 k[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) k[i] = __ldg(&c->rec[rec[i]].k);
+#pragma unroll
+    for (int i = 0; i < M; ++i) v[i] = k[i].x + t[i] * (k[i].y + t[i] * (k[i].z + t[i] * k[i].w));
 }
 
 __device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
-    return curve_lookup(c, (int)c->n, (int)c->ncells, __ldg(&c->xf[0]), c->x0c, c->inv_dx, v);
+    float x[1] = {v};
+    curve_lookup_n<1>(c, (int)c->n, (int)c->ncells, __ldg(&c->xf[0]), c->x0c, c->inv_dx, x);
+    return x[0];
 }
 
 __device__ __forceinline__ float curve_apply(const DevCurve* __restrict__ c, float v) {
@@ -183,10 +195,16 @@ struct MasterCurve {
         x0c = f[4];
         inv_dx = f[5];
     }
-    __device__ __forceinline__ float eval(float v) const {
-        if (identity) return v;
-        if (!ncells) return curve_map(c, v);
-        return curve_lookup(c, n, ncells, xf0, x0c, inv_dx, v);
+    // maps v[0..M) in place
+    template <int M>
+    __device__ __forceinline__ void eval_n(float* v) const {
+        if (identity) return;
+        if (!ncells) {
+#pragma unroll
+            for (int i = 0; i < M; ++i) v[i] = curve_map(c, v[i]);
+            return;
+        }
+        curve_lookup_n<M>(c, n, ncells, xf0, x0c, inv_dx, v);
     }
 };
 
@@ -194,7 +212,9 @@ struct MasterCurve {
 // outside, so each stage's constants are read once and its arithmetic runs
 // over N independent pixels.  Per pixel the operations and their order are
 // exactly apply_stages'.
-template <int N>
+// CHUNK: master-curve lookups kept in flight together (more hides the table
+// loads' latency, fewer keeps registers free).
+template <int N, int CHUNK = 3>
 __device__ __forceinline__ void apply_stages_n(const DevProgram& P, int begin, int end, float (&r)[N],
                                                float (&g)[N], float (&b)[N], uint32_t& err) {
     for (int s = begin; s < end; ++s) {
@@ -285,10 +305,21 @@ __device__ __forceinline__ void apply_stages_n(const DevProgram& P, int begin, i
             m.load(&cs->c[0], st.f);
             const bool id_r = st.f[6] != 0.0f, id_g = st.f[7] != 0.0f, id_b = st.f[8] != 0.0f;
             bool bad = false;
+            // master curve over the 3N channel values, CHUNK lookups in flight
+            float mv[3 * N];
 #pragma unroll
             for (int i = 0; i < N; ++i) {
                 bad |= !(isfinite(r[i]) && isfinite(g[i]) && isfinite(b[i]));
-                const float mr = m.eval(r[i]), mg = m.eval(g[i]), mb = m.eval(b[i]);
+                mv[3 * i] = r[i];
+                mv[3 * i + 1] = g[i];
+                mv[3 * i + 2] = b[i];
+            }
+            static_assert((3 * N) % CHUNK == 0, "channel values split into whole chunks");
+#pragma unroll
+            for (int j = 0; j < 3 * N; j += CHUNK) m.eval_n<CHUNK>(mv + j);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const float mr = mv[3 * i], mg = mv[3 * i + 1], mb = mv[3 * i + 2];
                 bad |= !(isfinite(mr) && isfinite(mg) && isfinite(mb));
                 r[i] = id_r ? mr : curve_apply(&cs->c[1], mr);
                 g[i] = id_g ? mg : curve_apply(&cs->c[2], mg);

@@ -491,10 +491,14 @@ __device__ __forceinline__ void menon_tile_out(MenonSmemT<T>& S, const DevRaw& r
 //
 // Tiles whose r=6 raw footprint lies inside the active area need no mirroring
 // and no zero extension, and with an even tile origin the CFA colour of each
-// position of a 2x2 quad is a compile-time constant (template L = the Bayer
-// layout seen from the quad's top-left).  Each thread then works on whole
-// quads with constant shared-memory offsets: chroma/gradients only at the two
-// non-green sites, greens copied, every neighbour a single shared load.
+// position k = 2*j + i of a 2x2 quad is a compile-time constant (template L =
+// the Bayer layout seen from the quad's top-left).  Every plane is stored by
+// quad position: one dense row-major plane of quads per position, so the
+// neighbour (dx, dy) of a sample is a compile-time position and quad offset,
+// consecutive threads touch consecutive elements (no shared-memory bank
+// conflicts), and chroma, gradients and directions are kept only at the two
+// non-green positions A (first row, column ax(L)) and B (second row, column
+// 1 - ax(L)), red and blue only at the two green positions.
 //
 // T = double: the reference's arithmetic, in binary64, in the reference's
 // order (bit-exact outputs).  T = float: the same steps in binary32 (outputs
@@ -507,57 +511,83 @@ __device__ __forceinline__ void menon_tile_out(MenonSmemT<T>& S, const DevRaw& r
 // reference's classifier in binary64 (a second pass over a list of such
 // sites); every other site's binary32 decision equals the reference's.
 
-constexpr int FR_W = MN_TW + 12, FR_H = MN_TH + 12;   // raw, full resolution, origin (-6,-6)
-constexpr int QW = (MN_TW + 8) / 2, QH = (MN_TH + 8) / 2;  // quad grid of the r=4 planes, origin (-4,-4)
+constexpr int RQW = (MN_TW + 12) / 2, RQH = (MN_TH + 12) / 2;  // raw planes: quads of the r=6 region, origin (-6,-6)
+constexpr int RQN = RQW * RQH;
+constexpr int QW = (MN_TW + 8) / 2, QH = (MN_TH + 8) / 2;      // chroma planes: quads of the r=4 region, origin (-4,-4)
 constexpr int QN = QW * QH;
-constexpr int FG_W = MN_TW + 4, FG_H = MN_TH + 4;     // green horiz red blue, full resolution, origin (-2,-2)
-constexpr int CLS_N = (QW - 2) * (QH - 2);             // quads of the r=2 region
+constexpr int GQW = QW - 2, GQH = QH - 2;                      // green, direction, red, blue: r=2 region, origin (-2,-2)
+constexpr int GQN = GQW * GQH;
+constexpr int MN_WARPS = MN_THREADS / 32;
+static_assert(MN_TW == 32 && MN_TH == 2 * MN_WARPS,
+              "epilogue mapping: warp w renders rows w and w + MN_TH/2, each lane two pixels of one row");
 
-// The two non-green sites of a quad: A in the quad's first row at column
-// ax(L), B in its second row at column 1 - ax(L).  Chroma-stage planes keep
-// one value per quad and class (consecutive quads are consecutive elements, so
-// a warp's accesses are bank-conflict free), halving their footprint.
+// Column of the first row's non-green position (A); B sits in the second row
+// at the other column.  Green positions: G0 = (1 - ax, 0), G1 = (ax, 1).
 __host__ __device__ constexpr int ng_col(int l) { return l < 2 ? 0 : 1; }
+__host__ __device__ constexpr int floor_half(int v) { return v >= 0 ? v / 2 : -((1 - v) / 2); }
+// Quad position of the sample (dx, dy) away from position (i, j) of a quad.
+__host__ __device__ constexpr int pos_at(int i, int j, int dx, int dy) { return ((j + dy) & 1) * 2 + ((i + dx) & 1); }
+// Its quad, as an offset on a grid of W quads per row.
+__host__ __device__ constexpr int quad_at(int i, int j, int dx, int dy, int W) {
+    return floor_half(j + dy) * W + floor_half(i + dx);
+}
 
 enum { GH_A, GH_B, GV_A, GV_B, CH_A, CH_B, CV_A, CV_B, DH_A, DH_B, DV_A, DV_B, NG_PLANES };
 
 template <typename T>
 struct FastSmemT {
-    T raw[FR_H * FR_W];
-    T ng[NG_PLANES][QN];        // red and blue reuse planes 0..5 in the last stages
-    T green[FG_H * FG_W];
-    uint8_t horiz[FG_H * FG_W];
+    T raw[4][RQN];               // normalized samples by quad position, r = 6
+    T ng[NG_PLANES][QN];         // chroma stage at A and B, r = 4; later red/blue
+    T green[2][GQN];             // interpolated green at A and B, r = 2
+    uint8_t horiz[2][GQN];       // direction at A and B, r = 2
     unsigned smax_bits;          // max |sample| of the footprint (float bits)
     unsigned rechecks;           // entries of `recheck`
-    uint16_t recheck[2 * CLS_N]; // near-tie sites: quad of the r=2 region * 2 + (class B)
+    uint16_t recheck[2 * GQN];   // near-tie sites: quad of the r=2 region * 2 + (site B)
 };
 using FastSmem = FastSmemT<double>;
-static_assert(2 * FG_W * FG_H <= 6 * QN, "red/blue must fit in the dead chroma planes");
+constexpr int FAST_RB_PLANES = 3;   // ng planes holding red and blue at G0, G1 (4 * GQN values)
+static_assert(4 * GQN <= FAST_RB_PLANES * QN, "red/blue must fit in the dead chroma planes");
 
-
-// MenonDemosaic.cpp:112-115 five-tap directional green at raw index r (stride d).
-template <typename T>
-__device__ __forceinline__ T five(const T* r, int d) {
-    return r_sub(r_add(half_sum(r[-d], r[d]), r_mul(T(0.5), r[0])), r_mul(T(0.25), r_add(r[-2 * d], r[2 * d])));
+// Raw sample (DX, DY) away from position (I, J) of raw quad rq.
+template <int I, int J, int DX, int DY, typename T>
+__device__ __forceinline__ T raw_q(const T (*raw)[RQN], int rq) {
+    return raw[pos_at(I, J, DX, DY)][rq + quad_at(I, J, DX, DY, RQW)];
 }
 
-// The reference's classifier at one non-green site, in binary64 from the
-// binary32 samples, terms in its order (MenonDemosaic.cpp:120-147): chroma
-// C = s - five-tap green, gradients |C(p) - C(p + 2 along the axis)|,
-// horizontal iff v >= h.  raw points at the site (row stride FR_W).
-__device__ __forceinline__ bool exact_horizontal(const float* raw) {
-    auto five_d = [](const float* r, int d) {
-        return dsub(dadd(__dmul_rn(0.5, dadd((double)r[-d], (double)r[d])), __dmul_rn(0.5, (double)r[0])),
-                    __dmul_rn(0.25, dadd((double)r[-2 * d], (double)r[2 * d])));
+// MenonDemosaic.cpp:112-115 five-tap directional green at position (I, J)
+// along (DX, DY).
+template <int I, int J, int DX, int DY, typename T>
+__device__ __forceinline__ T five_q(const T (*raw)[RQN], int rq) {
+    return five_tap<T>(raw_q<I, J, -2 * DX, -2 * DY>(raw, rq), raw_q<I, J, -DX, -DY>(raw, rq),
+                       raw[2 * J + I][rq], raw_q<I, J, DX, DY>(raw, rq), raw_q<I, J, 2 * DX, 2 * DY>(raw, rq));
+}
+
+// Interpolated green at the non-green sample (DX, DY) away from position
+// (I, J) of r=2 quad k (plane 0 holds A, plane 1 B: a non-green position's
+// row picks its plane).
+template <int I, int J, int DX, int DY, typename T>
+__device__ __forceinline__ T green_q(const T (*green)[GQN], int k) {
+    return green[pos_at(I, J, DX, DY) >> 1][k + quad_at(I, J, DX, DY, GQW)];
+}
+
+// The reference's classifier at non-green position (I, J) of raw quad rq, in
+// binary64 from the binary32 samples, terms in its order
+// (MenonDemosaic.cpp:120-147): chroma C = s - five-tap green, gradients
+// |C(p) - C(p + 2 along the axis)|, horizontal iff v >= h.
+template <int I, int J>
+__device__ __forceinline__ bool exact_horizontal_q(const float (*raw)[RQN], int rq) {
+    auto at = [&](int dx, int dy) -> double {
+        return (double)raw[pos_at(I, J, dx, dy)][rq + quad_at(I, J, dx, dy, RQW)];
+    };
+    auto five_d = [&](int x, int y, int dx, int dy) {
+        return dsub(dadd(__dmul_rn(0.5, dadd(at(x - dx, y - dy), at(x + dx, y + dy))), __dmul_rn(0.5, at(x, y))),
+                    __dmul_rn(0.25, dadd(at(x - 2 * dx, y - 2 * dy), at(x + 2 * dx, y + 2 * dy))));
     };
     auto dh = [&](int x, int y) {
-        const float* a = raw + y * FR_W + x;
-        return fabs(dsub(dsub((double)a[0], five_d(a, 1)), dsub((double)a[2], five_d(a + 2, 1))));
+        return fabs(dsub(dsub(at(x, y), five_d(x, y, 1, 0)), dsub(at(x + 2, y), five_d(x + 2, y, 1, 0))));
     };
     auto dv = [&](int x, int y) {
-        const float* a = raw + y * FR_W + x;
-        return fabs(dsub(dsub((double)a[0], five_d(a, FR_W)),
-                         dsub((double)a[2 * FR_W], five_d(a + 2 * FR_W, FR_W))));
+        return fabs(dsub(dsub(at(x, y), five_d(x, y, 0, 1)), dsub(at(x, y + 2), five_d(x, y + 2, 0, 1))));
     };
     double h = 0.0, v = 0.0;
     h = dadd(h, dh(0, 2));                    v = dadd(v, dv(2, 0));
@@ -569,6 +599,56 @@ __device__ __forceinline__ bool exact_horizontal(const float* raw) {
     h = dadd(h, dh(0, -2));                   v = dadd(v, dv(-2, 0));
     h = dadd(h, dh(-2, -2));                  v = dadd(v, dv(-2, -2));
     return v >= h;
+}
+
+// MenonDemosaic.cpp:151-161 red and blue at green position (I, J) of raw quad
+// rq / r=2 quad k: the row's non-green neighbours carry that colour along the
+// row, the other colour comes from the column.
+template <int L, int I, int J, typename T>
+__device__ __forceinline__ void rb_at_green(const FastSmemT<T>& S, int rq, int k, T& rr, T& bb) {
+    constexpr bool red_h = pat(L, (J << 1) | (I ^ 1)) == 0;
+    constexpr int rx = red_h ? 1 : 0, ry = red_h ? 0 : 1;   // red axis
+    constexpr int bx = 1 - rx, by = 1 - ry;                 // blue axis
+    const T g = S.raw[2 * J + I][rq];
+    rr = r_sub(r_add(g, half_sum(raw_q<I, J, -rx, -ry>(S.raw, rq), raw_q<I, J, rx, ry>(S.raw, rq))),
+               half_sum(green_q<I, J, -rx, -ry>(S.green, k), green_q<I, J, rx, ry>(S.green, k)));
+    bb = r_sub(r_add(g, half_sum(raw_q<I, J, -bx, -by>(S.raw, rq), raw_q<I, J, bx, by>(S.raw, rq))),
+               half_sum(green_q<I, J, -bx, -by>(S.green, k), green_q<I, J, bx, by>(S.green, k)));
+}
+
+// Row J of output quad (r=2 quad k, raw quad rq): both pixels' RGB after the
+// opposite colour at the R/B site (MenonDemosaic.cpp:162-173), and their
+// directions.  rb = red at G0, G1 then blue at G0, G1 (GQN each).
+template <int L, int J, typename T>
+__device__ __forceinline__ void fast_row(const FastSmemT<T>& S, const T* rb, int rq, int k, T (&rr)[2], T (&gg)[2],
+                                         T (&bb)[2], bool (&hz)[2]) {
+    constexpr int AX = ng_col(L);
+    constexpr int NI = J == 0 ? AX : 1 - AX;   // column of this row's non-green position
+    constexpr int GI = 1 - NI;
+    constexpr int own = pat(L, 2 * J + NI);     // 0 red or 2 blue
+    // green position of this row
+    rr[GI] = rb[J * GQN + k];
+    bb[GI] = rb[(2 + J) * GQN + k];
+    gg[GI] = S.raw[2 * J + GI][rq];
+    hz[GI] = true;
+    // non-green position: its neighbours along the direction are green
+    // positions, of this row's kind along the row and of the other row's kind
+    // along the column
+    const bool h = S.horiz[J][k];
+    const T* red = rb + (h ? J : 1 - J) * GQN;
+    const T* blue = red + 2 * GQN;
+    const int om = k + (h ? quad_at(NI, J, -1, 0, GQW) : quad_at(NI, J, 0, -1, GQW));
+    const int op = k + (h ? quad_at(NI, J, 1, 0, GQW) : quad_at(NI, J, 0, 1, GQW));
+    const T s = S.raw[2 * J + NI][rq];
+    if (own == 2) {
+        bb[NI] = s;
+        rr[NI] = r_sub(r_add(s, half_sum(red[om], red[op])), half_sum(blue[om], blue[op]));
+    } else {
+        rr[NI] = s;
+        bb[NI] = r_sub(r_add(s, half_sum(blue[om], blue[op])), half_sum(red[om], red[op]));
+    }
+    gg[NI] = S.green[J][k];
+    hz[NI] = h;
 }
 
 template <int L, typename T>
@@ -583,35 +663,35 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         S.smax_bits = 0;
         S.rechecks = 0;
     }
-    // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile, as 2x2 quads
+    // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile, by quad position
     float local_max = 0.0f;
-    load_quads<FR_W / 2, FR_H / 2, FR_W, FR_H, 0, MN_THREADS>(S.raw, raw, x0 - 6, y0 - 6, &local_max);
+    load_quad_planes<RQW, RQH, MN_THREADS>(S.raw, raw, x0 - 6, y0 - 6, &local_max);
     if constexpr (F32) {
         for (int o = 16; o; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
         __syncthreads();   // smax_bits and rechecks are zeroed
         if ((t & 31) == 0) atomicMax(&S.smax_bits, __float_as_uint(local_max));
     }
     __syncthreads();
-    // 2. directional green and chroma at the two non-green sites of every quad
-    //    of the r=4 region (MenonDemosaic.cpp:107-119)
+    // 2. directional green and chroma at A and B of every quad of the r=4
+    //    region (MenonDemosaic.cpp:107-119)
 #pragma unroll 2
     for (int q = t; q < QN; q += MN_THREADS) {
         const int qx = q % QW, qy = q / QW;
-        const T* ra = S.raw + (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
-        const T* rb = S.raw + (2 * qy + 3) * FR_W + 2 * qx + BX + 2;
-        const T ha = five(ra, 1), va = five(ra, FR_W);
-        const T hb = five(rb, 1), vb = five(rb, FR_W);
+        const int rq = (qy + 1) * RQW + qx + 1;
+        const T sa = S.raw[AX][rq], sb = S.raw[2 + BX][rq];
+        const T ha = five_q<AX, 0, 1, 0>(S.raw, rq), va = five_q<AX, 0, 0, 1>(S.raw, rq);
+        const T hb = five_q<BX, 1, 1, 0>(S.raw, rq), vb = five_q<BX, 1, 0, 1>(S.raw, rq);
         S.ng[GH_A][q] = ha;
         S.ng[GV_A][q] = va;
-        S.ng[CH_A][q] = r_sub(ra[0], ha);
-        S.ng[CV_A][q] = r_sub(ra[0], va);
+        S.ng[CH_A][q] = r_sub(sa, ha);
+        S.ng[CV_A][q] = r_sub(sa, va);
         S.ng[GH_B][q] = hb;
         S.ng[GV_B][q] = vb;
-        S.ng[CH_B][q] = r_sub(rb[0], hb);
-        S.ng[CV_B][q] = r_sub(rb[0], vb);
+        S.ng[CH_B][q] = r_sub(sb, hb);
+        S.ng[CV_B][q] = r_sub(sb, vb);
     }
     __syncthreads();
-    // 3. forward chroma gradients (MenonDemosaic.cpp:120-125): the same-class
+    // 3. forward chroma gradients (MenonDemosaic.cpp:120-125): the same-position
     //    neighbour two pixels right is the next quad, two pixels down the next row
 #pragma unroll 2
     for (int q = t; q < QN; q += MN_THREADS) {
@@ -627,18 +707,18 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
     }
     __syncthreads();
     // 4. classifier and green (MenonDemosaic.cpp:130-147) for the quads of the r=2
-    //    region, terms in the reference's order; (-1,+-1) offsets land on the other class
+    //    region, terms in the reference's order; (-1,+-1) offsets land on the other position
     const float band_abs = F32 ? 640.0f * 5.9604644775390625e-8f * __uint_as_float(S.smax_bits) : 0.0f;
 #pragma unroll 2
-    for (int k = t; k < CLS_N; k += MN_THREADS) {
-        const int qx = k % (QW - 2) + 1, qy = k / (QW - 2) + 1;
+    for (int k = t; k < GQN; k += MN_THREADS) {
+        const int qx = k % GQW + 1, qy = k / GQW + 1;
         const int q = qy * QW + qx;
         const T* dhA = S.ng[DH_A];
         const T* dhB = S.ng[DH_B];
         const T* dvA = S.ng[DV_A];
         const T* dvB = S.ng[DV_B];
         const T three = T(3);
-        // A site: other-class (B) quads at column offsets -(1-AX) / +AX
+        // A site: B quads at column offsets -(1-AX) / +AX
         T h = 0, v = 0;
         h = r_add(h, dhA[q + QW]);               v = r_add(v, dvA[q + 1]);
         h = r_add(h, dhA[q + QW - 1]);           v = r_add(v, dvA[q - QW + 1]);
@@ -650,7 +730,7 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         h = r_add(h, dhA[q - QW - 1]);           v = r_add(v, dvA[q - QW - 1]);
         const bool hzA = v >= h;
         if (F32 && near_tie(h, v, band_abs)) S.recheck[atomicAdd(&S.rechecks, 1u)] = (uint16_t)(2 * k);
-        // B site: other-class (A) quads at column offsets -AX / +(1-AX)
+        // B site: A quads at column offsets -AX / +(1-AX)
         h = 0;
         v = 0;
         h = r_add(h, dhB[q + QW]);               v = r_add(v, dvB[q + 1]);
@@ -663,19 +743,10 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         h = r_add(h, dhB[q - QW - 1]);           v = r_add(v, dvB[q - QW - 1]);
         const bool hzB = v >= h;
         if (F32 && near_tie(h, v, band_abs)) S.recheck[atomicAdd(&S.rechecks, 1u)] = (uint16_t)(2 * k + 1);
-        // full-resolution green/direction on the r=2 grid (origin -2)
-        const int ga = (2 * qy - 2) * FG_W + 2 * qx - 2 + AX;          // A site
-        const int gb = (2 * qy - 1) * FG_W + 2 * qx - 2 + BX;          // B site
-        const int g0 = (2 * qy - 2) * FG_W + 2 * qx - 2 + BX;          // green in row 0
-        const int g1 = (2 * qy - 1) * FG_W + 2 * qx - 2 + AX;          // green in row 1
-        S.horiz[ga] = hzA;
-        S.horiz[gb] = hzB;
-        S.horiz[g0] = 1;
-        S.horiz[g1] = 1;
-        S.green[ga] = hzA ? S.ng[GH_A][q] : S.ng[GV_A][q];
-        S.green[gb] = hzB ? S.ng[GH_B][q] : S.ng[GV_B][q];
-        S.green[g0] = S.raw[(2 * qy + 2) * FR_W + 2 * qx + 2 + BX];
-        S.green[g1] = S.raw[(2 * qy + 3) * FR_W + 2 * qx + 2 + AX];
+        S.horiz[0][k] = hzA;
+        S.horiz[1][k] = hzB;
+        S.green[0][k] = hzA ? S.ng[GH_A][q] : S.ng[GV_A][q];
+        S.green[1][k] = hzB ? S.ng[GH_B][q] : S.ng[GV_B][q];
     }
     __syncthreads();
     if constexpr (F32) {
@@ -684,84 +755,78 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         if (n) {
             for (unsigned e = t; e < n; e += MN_THREADS) {
                 const int code = S.recheck[e];
-                const int k = code >> 1, cls = code & 1;
-                const int qx = k % (QW - 2) + 1, qy = k / (QW - 2) + 1;
-                const int q = qy * QW + qx;
-                const int site = cls ? (2 * qy + 3) * FR_W + 2 * qx + BX + 2 : (2 * qy + 2) * FR_W + 2 * qx + AX + 2;
-                const bool hz = exact_horizontal(S.raw + site);
-                const int g = cls ? (2 * qy - 1) * FG_W + 2 * qx - 2 + BX : (2 * qy - 2) * FG_W + 2 * qx - 2 + AX;
-                S.horiz[g] = hz;
-                S.green[g] = hz ? S.ng[cls ? GH_B : GH_A][q] : S.ng[cls ? GV_B : GV_A][q];
+                const int k = code >> 1, site = code & 1;
+                const int qx = k % GQW, qy = k / GQW;
+                const int rq = (qy + 2) * RQW + qx + 2;
+                const int q = (qy + 1) * QW + qx + 1;
+                const bool hz = site ? exact_horizontal_q<BX, 1>(S.raw, rq) : exact_horizontal_q<AX, 0>(S.raw, rq);
+                S.horiz[site][k] = hz;
+                S.green[site][k] = hz ? S.ng[site ? GH_B : GH_A][q] : S.ng[site ? GV_B : GV_A][q];
             }
             if (ties && t == 0) atomicAdd(ties, (unsigned long long)n);
             __syncthreads();
         }
     }
-    // 5. red and blue on the r=1 ring (MenonDemosaic.cpp:151-161); chroma planes are dead
-    T* red = S.ng[0];
-    T* blue = S.ng[0] + FG_W * FG_H;
+    // 5. red and blue at the green positions of the r=1 ring (MenonDemosaic.cpp:151-161);
+    //    the chroma planes are dead.  rb: red at G0, G1, then blue at G0, G1.
+    T* rb = S.ng[0];
 #pragma unroll 2
-    for (int q = t; q < (FG_W / 2) * (FG_H / 2); q += MN_THREADS) {
-        const int qx = q % (FG_W / 2), qy = q / (FG_W / 2);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = k & 1, j = k >> 1;
-            const int gx = 2 * qx + i, gy = 2 * qy + j;
-            if (gx == 0 || gx == FG_W - 1 || gy == 0 || gy == FG_H - 1) continue;
-            const int pg = gy * FG_W + gx;
-            const int pr = (gy + 4) * FR_W + gx + 4;
-            const int own = pat(L, k);
-            T rr = 0, bb = 0;
-            if (own == 0) rr = S.raw[pr];
-            if (own == 2) bb = S.raw[pr];
-            if (own == 1) {
-                const bool red_h = pat(L, (j << 1) | (i ^ 1)) == 0;   // colour of the row's non-green
-                const int dr = red_h ? 1 : FR_W, dg = red_h ? 1 : FG_W;
-                const int br = red_h ? FR_W : 1, bg = red_h ? FG_W : 1;
-                const T g = S.green[pg];
-                rr = r_sub(r_add(g, half_sum(S.raw[pr - dr], S.raw[pr + dr])),
-                           half_sum(S.green[pg - dg], S.green[pg + dg]));
-                bb = r_sub(r_add(g, half_sum(S.raw[pr - br], S.raw[pr + br])),
-                           half_sum(S.green[pg - bg], S.green[pg + bg]));
-            }
-            red[pg] = rr;
-            blue[pg] = bb;
+    for (int k = t; k < GQN; k += MN_THREADS) {
+        const int qx = k % GQW, qy = k / GQW;
+        const int rq = (qy + 2) * RQW + qx + 2;
+        // relative pixel of the quad's top-left: (2 qx - 2, 2 qy - 2)
+        const int px0 = 2 * qx - 2 + BX, py0 = 2 * qy - 2;   // G0
+        const int px1 = 2 * qx - 2 + AX, py1 = 2 * qy - 1;   // G1
+        if (px0 >= -1 && px0 <= MN_TW && py0 >= -1 && py0 <= MN_TH) {
+            T rr, bb;
+            rb_at_green<L, BX, 0>(S, rq, k, rr, bb);
+            rb[k] = rr;
+            rb[2 * GQN + k] = bb;
+        }
+        if (px1 >= -1 && px1 <= MN_TW && py1 >= -1 && py1 <= MN_TH) {
+            T rr, bb;
+            rb_at_green<L, AX, 1>(S, rq, k, rr, bb);
+            rb[GQN + k] = rr;
+            rb[3 * GQN + k] = bb;
         }
     }
     __syncthreads();
-    // 6. opposite colour at R/B sites, float cast (MenonDemosaic.cpp:162-173), then the
-    //    fused stages over one row pair of a quad per thread (every thread busy)
-    for (int u = t; u < (MN_TW / 2) * MN_TH; u += MN_THREADS) {
-        const int q = u >> 1, j = u & 1;
-        const int qx = q % (MN_TW / 2), qy = q / (MN_TW / 2);
+    // 6. opposite colour at R/B sites and float cast (MenonDemosaic.cpp:162-173),
+    //    then the fused stages.  Warp w renders rows w and w + MN_TH/2 (the same
+    //    quad row parity, so the row's layout is warp-uniform), a lane two
+    //    adjacent pixels of one row.
+    {
+        const int w = t >> 5, lane = t & 31;
+        const int row = w + (MN_TH / 2) * (lane >> 4);
+        const int qx = lane & 15, qy = row >> 1;
+        const int k = (qy + 1) * GQW + qx + 1;
+        const int rq = (qy + 3) * RQW + qx + 3;
+        T rr[2], gg[2], bb[2];
+        bool hz[2];
+        if (w & 1) fast_row<L, 1>(S, rb, rq, k, rr, gg, bb, hz);
+        else fast_row<L, 0>(S, rb, rq, k, rr, gg, bb, hz);
+        const int y = y0 + row;
         float R[2], G[2], B[2];
         bool keep[2];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-            const int k = 2 * j + i;
-            const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
-            const int pg = (2 * qy + j + 2) * FG_W + 2 * qx + i + 2;
-            const int own = pat(L, k);
-            const int d = S.horiz[pg] ? 1 : FG_W;
-            T rr = red[pg], bb = blue[pg];
-            if (own == 2) rr = r_sub(r_add(bb, half_sum(red[pg - d], red[pg + d])), half_sum(blue[pg - d], blue[pg + d]));
-            if (own == 0) bb = r_sub(r_add(rr, half_sum(blue[pg - d], blue[pg + d])), half_sum(red[pg - d], red[pg + d]));
+            const int x = x0 + 2 * qx + i;
             keep[i] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
             // pixels outside the viewport enter the stages as zeros (never written)
-            R[i] = keep[i] ? (float)rr : 0.0f;
-            G[i] = keep[i] ? (float)S.green[pg] : 0.0f;
-            B[i] = keep[i] ? (float)bb : 0.0f;
+            R[i] = keep[i] ? (float)rr[i] : 0.0f;
+            G[i] = keep[i] ? (float)gg[i] : 0.0f;
+            B[i] = keep[i] ? (float)bb[i] : 0.0f;
         }
         apply_stages_n<2>(P, 0, stage_end, R, G, B, err);
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             if (!keep[i]) continue;
-            const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
+            const int x = x0 + 2 * qx + i;
             float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
             o[0] = R[i];
             o[1] = G[i];
             o[2] = B[i];
-            if (dirs) dirs[(size_t)(y - oy) * ow + (x - ox)] = S.horiz[(2 * qy + j + 2) * FG_W + 2 * qx + i + 2];
+            if (dirs) dirs[(size_t)(y - oy) * ow + (x - ox)] = hz[i];
         }
     }
 }

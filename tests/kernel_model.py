@@ -185,14 +185,29 @@ def model_render(meta, samples, viewport, fast=True):
     return out
 
 
+def _floor_half(v):
+    return v // 2
+
+
+def _pos_at(i, j, dx, dy):
+    return ((j + dy) & 1) * 2 + ((i + dx) & 1)
+
+
+def _quad_at(i, j, dx, dy, w):
+    return _floor_half(j + dy) * w + _floor_half(i + dx)
+
+
 def _fast_tile(meta, sample, color, x0, y0, viewport, out):
-    """The interior quad path (menon_fast in render_raw.cu): class-packed chroma
-    planes on the quad grid, full-resolution green/red/blue, the kernel's strides
-    and neighbour offsets."""
+    """The interior quad path (menon_fast in render_raw.cu): every plane stored
+    by quad position (raw at all four positions, chroma/gradients/green/
+    directions at the non-green positions A and B, red/blue at the green
+    positions G0 and G1), the kernel's strides, neighbour offsets and the
+    epilogue's warp/lane mapping."""
     ox, oy, ow, oh = viewport
-    RW, RH, GW, GH = TW + 12, TH + 12, TW + 4, TH + 4
+    RQW, RQH = (TW + 12) // 2, (TH + 12) // 2
     QW, QH = (TW + 8) // 2, (TH + 8) // 2
-    QN = QW * QH
+    GQW, GQH = QW - 2, QH - 2
+    RQN, QN, GQN = RQW * RQH, QW * QH, GQW * GQH
     lay = [color(x0 + (k & 1), y0 + (k >> 1)) for k in range(4)]
     AX = 0 if lay[0] != 1 else 1          # column of the first row's non-green
     BX = 1 - AX
@@ -200,27 +215,33 @@ def _fast_tile(meta, sample, color, x0, y0, viewport, out):
     def flat(n):
         return Plane(n, 1, 0, 0)
 
-    raw = flat(RW * RH)
+    raw = [flat(RQN) for _ in range(4)]
     ng = {name: flat(QN) for name in ("ghA", "ghB", "gvA", "gvB", "chA", "chB", "cvA", "cvB",
                                       "dhA", "dhB", "dvA", "dvB")}
-    green, horiz = flat(GW * GH), flat(GW * GH)
-    for i in range(RW * RH):
-        raw.set(i, 0, sample(x0 - 6 + i % RW, y0 - 6 + i // RW))
+    green, horiz = [flat(GQN), flat(GQN)], [flat(GQN), flat(GQN)]
+    for q in range(RQN):
+        qx, qy = q % RQW, q // RQW
+        for k in range(4):
+            raw[k].set(q, 0, sample(x0 - 6 + 2 * qx + (k & 1), y0 - 6 + 2 * qy + (k >> 1)))
     half = lambda a, b: 0.5 * (a + b)
-    R = lambda i: raw.get(i, 0)
 
-    def five(i, d):
-        return (half(R(i - d), R(i + d)) + 0.5 * R(i)) - 0.25 * (R(i - 2 * d) + R(i + 2 * d))
+    def R(i, j, dx, dy, rq):
+        return raw[_pos_at(i, j, dx, dy)].get(rq + _quad_at(i, j, dx, dy, RQW), 0)
+
+    def five(i, j, dx, dy, rq):
+        return ((half(R(i, j, -dx, -dy, rq), R(i, j, dx, dy, rq)) + 0.5 * R(i, j, 0, 0, rq))
+                - 0.25 * (R(i, j, -2 * dx, -2 * dy, rq) + R(i, j, 2 * dx, 2 * dy, rq)))
 
     for q in range(QN):
         qx, qy = q % QW, q // QW
-        ra = (2 * qy + 2) * RW + 2 * qx + AX + 2
-        rb = (2 * qy + 3) * RW + 2 * qx + BX + 2
-        ha, va, hb, vb = five(ra, 1), five(ra, RW), five(rb, 1), five(rb, RW)
+        rq = (qy + 1) * RQW + qx + 1
+        sa, sb = R(AX, 0, 0, 0, rq), R(BX, 1, 0, 0, rq)
+        ha, va = five(AX, 0, 1, 0, rq), five(AX, 0, 0, 1, rq)
+        hb, vb = five(BX, 1, 1, 0, rq), five(BX, 1, 0, 1, rq)
         ng["ghA"].set(q, 0, ha); ng["gvA"].set(q, 0, va)
-        ng["chA"].set(q, 0, R(ra) - ha); ng["cvA"].set(q, 0, R(ra) - va)
+        ng["chA"].set(q, 0, sa - ha); ng["cvA"].set(q, 0, sa - va)
         ng["ghB"].set(q, 0, hb); ng["gvB"].set(q, 0, vb)
-        ng["chB"].set(q, 0, R(rb) - hb); ng["cvB"].set(q, 0, R(rb) - vb)
+        ng["chB"].set(q, 0, sb - hb); ng["cvB"].set(q, 0, sb - vb)
     G = lambda name, i: ng[name].get(i, 0)
     for q in range(QN):
         qx, qy = q % QW, q // QW
@@ -230,8 +251,8 @@ def _fast_tile(meta, sample, color, x0, y0, viewport, out):
         if qy < QH - 1:
             ng["dvA"].set(q, 0, abs(G("cvA", q) - G("cvA", q + QW)))
             ng["dvB"].set(q, 0, abs(G("cvB", q) - G("cvB", q + QW)))
-    for k in range((QW - 2) * (QH - 2)):
-        qx, qy = k % (QW - 2) + 1, k // (QW - 2) + 1
+    for k in range(GQN):
+        qx, qy = k % GQW + 1, k // GQW + 1
         q = qy * QW + qx
         termsA = [(("dhA", q + QW), ("dvA", q + 1), 1), (("dhA", q + QW - 1), ("dvA", q - QW + 1), 1),
                   (("dhB", q - BX), ("dvB", q - QW + AX), 1), (("dhA", q), ("dvA", q), 3),
@@ -241,57 +262,62 @@ def _fast_tile(meta, sample, color, x0, y0, viewport, out):
                   (("dhA", q + QW - AX), ("dvA", q + BX), 1), (("dhB", q), ("dvB", q), 3),
                   (("dhB", q - 1), ("dvB", q - QW), 3), (("dhA", q - AX), ("dvA", q - AX), 1),
                   (("dhB", q - QW), ("dvB", q - 1), 1), (("dhB", q - QW - 1), ("dvB", q - QW - 1), 1)]
-        hz = []
-        for terms in (termsA, termsB):
+        for site, terms in enumerate((termsA, termsB)):
             h = v = 0.0
             for (hn, hi), (vn, vi), w in terms:
                 h += w * G(hn, hi)
                 v += w * G(vn, vi)
-            hz.append(v >= h)
-        ga = (2 * qy - 2) * GW + 2 * qx - 2 + AX
-        gb = (2 * qy - 1) * GW + 2 * qx - 2 + BX
-        g0 = (2 * qy - 2) * GW + 2 * qx - 2 + BX
-        g1 = (2 * qy - 1) * GW + 2 * qx - 2 + AX
-        horiz.set(ga, 0, float(hz[0])); horiz.set(gb, 0, float(hz[1]))
-        horiz.set(g0, 0, 1.0); horiz.set(g1, 0, 1.0)
-        green.set(ga, 0, G("ghA", q) if hz[0] else G("gvA", q))
-        green.set(gb, 0, G("ghB", q) if hz[1] else G("gvB", q))
-        green.set(g0, 0, R((2 * qy + 2) * RW + 2 * qx + 2 + BX))
-        green.set(g1, 0, R((2 * qy + 3) * RW + 2 * qx + 2 + AX))
-    red, blue = flat(GW * GH), flat(GW * GH)
-    for q in range((GW // 2) * (GH // 2)):
-        qx, qy = q % (GW // 2), q // (GW // 2)
-        for k in range(4):
-            i, j = k & 1, k >> 1
-            gx, gy = 2 * qx + i, 2 * qy + j
-            if gx == 0 or gx == GW - 1 or gy == 0 or gy == GH - 1:
+            hz = v >= h
+            horiz[site].set(k, 0, float(hz))
+            green[site].set(k, 0, G("ghA" if site == 0 else "ghB", q) if hz else G("gvA" if site == 0 else "gvB", q))
+
+    def Gn(i, j, dx, dy, k):
+        p = _pos_at(i, j, dx, dy)
+        assert p in (AX, 2 + BX), "green_q reads a non-green position"
+        return green[p >> 1].get(k + _quad_at(i, j, dx, dy, GQW), 0)
+
+    rb = [flat(GQN) for _ in range(4)]      # red G0, red G1, blue G0, blue G1
+    for k in range(GQN):
+        qx, qy = k % GQW, k // GQW
+        rq = (qy + 2) * RQW + qx + 2
+        for gi, (i, j) in enumerate(((BX, 0), (AX, 1))):
+            px, py = 2 * qx - 2 + i, 2 * qy - 2 + j
+            if not (-1 <= px <= TW and -1 <= py <= TH):
                 continue
-            pg = gy * GW + gx
-            pr = (gy + 4) * RW + gx + 4
-            rr = bb = 0.0
-            if lay[k] == 0:
-                rr = R(pr)
-            if lay[k] == 2:
-                bb = R(pr)
-            if lay[k] == 1:
-                red_h = lay[(j << 1) | (i ^ 1)] == 0
-                dr, dg = (1, 1) if red_h else (RW, GW)
-                br, bg = (RW, GW) if red_h else (1, 1)
-                g = green.get(pg, 0)
-                rr = (g + half(R(pr - dr), R(pr + dr))) - half(green.get(pg - dg, 0), green.get(pg + dg, 0))
-                bb = (g + half(R(pr - br), R(pr + br))) - half(green.get(pg - bg, 0), green.get(pg + bg, 0))
-            red.set(pg, 0, rr); blue.set(pg, 0, bb)
-    for q in range((TW // 2) * (TH // 2)):
-        qx, qy = q % (TW // 2), q // (TW // 2)
-        for k in range(4):
-            i, j = k & 1, k >> 1
-            x, y = x0 + 2 * qx + i, y0 + 2 * qy + j
-            pg = (2 * qy + j + 2) * GW + 2 * qx + i + 2
-            d = 1 if horiz.get(pg, 0) else GW
-            rr, bb = red.get(pg, 0), blue.get(pg, 0)
-            if lay[k] == 2:
-                rr = (bb + half(red.get(pg - d, 0), red.get(pg + d, 0))) - half(blue.get(pg - d, 0), blue.get(pg + d, 0))
-            if lay[k] == 0:
-                bb = (rr + half(blue.get(pg - d, 0), blue.get(pg + d, 0))) - half(red.get(pg - d, 0), red.get(pg + d, 0))
+            red_h = lay[(j << 1) | (i ^ 1)] == 0
+            rx, ry = (1, 0) if red_h else (0, 1)
+            bx, by = 1 - rx, 1 - ry
+            g = R(i, j, 0, 0, rq)
+            rr = (g + half(R(i, j, -rx, -ry, rq), R(i, j, rx, ry, rq))) - half(Gn(i, j, -rx, -ry, k), Gn(i, j, rx, ry, k))
+            bb = (g + half(R(i, j, -bx, -by, rq), R(i, j, bx, by, rq))) - half(Gn(i, j, -bx, -by, k), Gn(i, j, bx, by, k))
+            rb[gi].set(k, 0, rr)
+            rb[2 + gi].set(k, 0, bb)
+    for t in range(256):
+        w, lane = t >> 5, t & 31
+        row = w + (TH // 2) * (lane >> 4)
+        qx, qy = lane & 15, row >> 1
+        j = w & 1
+        assert row & 1 == j
+        k = (qy + 1) * GQW + qx + 1
+        rq = (qy + 3) * RQW + qx + 3
+        ni = AX if j == 0 else BX
+        gi = 1 - ni
+        px = {}
+        # green position of the row
+        px[gi] = (rb[j].get(k, 0), R(gi, j, 0, 0, rq), rb[2 + j].get(k, 0))
+        hz = horiz[j].get(k, 0) != 0
+        plane = j if hz else 1 - j
+        om = k + (_quad_at(ni, j, -1, 0, GQW) if hz else _quad_at(ni, j, 0, -1, GQW))
+        op = k + (_quad_at(ni, j, 1, 0, GQW) if hz else _quad_at(ni, j, 0, 1, GQW))
+        red, blue = rb[plane], rb[2 + plane]
+        s = R(ni, j, 0, 0, rq)
+        if lay[2 * j + ni] == 2:
+            rr = (s + half(red.get(om, 0), red.get(op, 0))) - half(blue.get(om, 0), blue.get(op, 0))
+            px[ni] = (rr, green[j].get(k, 0), s)
+        else:
+            bb = (s + half(blue.get(om, 0), blue.get(op, 0))) - half(red.get(om, 0), red.get(op, 0))
+            px[ni] = (s, green[j].get(k, 0), bb)
+        for i in range(2):
+            x, y = x0 + 2 * qx + i, y0 + row
             if ox <= x < ox + ow and oy <= y < oy + oh:
-                out[y - oy, x - ox] = (rr, green.get(pg, 0), bb)
+                out[y - oy, x - ox] = px[i]
