@@ -513,40 +513,65 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
             d.inv_h[i] = (float)(1.0 / h);
             d.coef[i] = make_float4((float)y[i], (float)(3 * (p0 - y[i])), (float)(3 * (y[i] - 2 * p0 + p1)),
                                     (float)(y[i + 1] - y[i] + 3 * (p0 - p1)));
-            // cell-lookup records: cubic segments in t = (v - x_i)/h, linear ones
-            // (and the extrapolations) as y_i + (v - x_i)*slope like ToneOps.cpp:826
+            // cell-lookup records in s = v - x_i: cubic segments with the power
+            // basis of t = s/h rescaled in binary64, linear ones (and the
+            // extrapolations) as y_i + s*slope like ToneOps.cpp:826
+            d.anchor[i] = d.xn[i];
             if (interpolation) {
-                d.rec[i].a = make_float4(d.xn[i], d.inv_h[i], d.xf[i + 1], 0.0f);
-                d.rec[i].k = d.coef[i];
+                const double r = 1.0 / h;
+                d.e[0][i] = (float)y[i];
+                d.e[1][i] = (float)(3 * (p0 - y[i]) * r);
+                d.e[2][i] = (float)(3 * (y[i] - 2 * p0 + p1) * r * r);
+                d.e[3][i] = (float)((y[i + 1] - y[i] + 3 * (p0 - p1)) * r * r * r);
             } else {
-                d.rec[i].a = make_float4(d.xn[i], 1.0f, d.xf[i + 1], 0.0f);
-                d.rec[i].k = make_float4(d.y[i], d.slope[i], 0.0f, 0.0f);
+                d.e[0][i] = d.y[i];
+                d.e[1][i] = d.slope[i];
+                d.e[2][i] = 0.0f;
+                d.e[3][i] = 0.0f;
             }
         }
-        d.rec[n - 1].a = make_float4(d.xn[n - 1], 1.0f, INFINITY, 0.0f);
-        d.rec[n - 1].k = make_float4(d.y[n - 1], d.slope[n - 2], 0.0f, 0.0f);
-        d.rec[n].a = make_float4(d.xn[0], 1.0f, d.xf[0], 0.0f);
-        d.rec[n].k = make_float4(d.y[0], d.slope[0], 0.0f, 0.0f);
-        // Uniform cells at most half the narrowest segment wide: every cell
-        // names the segment one cell to its left (a safe lower start for the
-        // device's short forward walk) and the knot ending it, so one
-        // comparison nearly always lands on the sample's segment.  Curves
-        // needing more than 4096 cells keep the binary search.
+        auto linear_rec = [&](uint32_t r, uint32_t knot, float s) {
+            d.anchor[r] = d.xn[knot];
+            d.e[0][r] = d.y[knot];
+            d.e[1][r] = s;
+            d.e[2][r] = 0.0f;
+            d.e[3][r] = 0.0f;
+        };
+        linear_rec(n - 1, n - 1, d.slope[n - 2]);
+        linear_rec(n, 0, d.slope[0]);
+        // Uniform cells at most a quarter of the narrowest segment wide: every
+        // cell names the segment one cell to its left and the knot ending it.
+        // A float sample's computed cell is within one of its true cell, so the
+        // samples reaching a cell span at most three cells -- less than any
+        // segment -- and one comparison with that knot finds the sample's
+        // segment; each cell is checked for this below.  Curves needing more
+        // than 4096 cells keep the binary search.
         const double span = x[n - 1] - x[0];
-        const double cells = std::ceil(span / (0.5 * min_h));
+        const double cells = std::ceil(span / (0.25 * min_h));
         d.ncells = 0;
         if (cells >= 1 && cells <= 4096) {
             const uint32_t nc = (uint32_t)cells;
             const double dx = span / nc;
-            d.ncells = nc;
-            d.x0c = d.xn[0];
-            d.inv_dx = (float)(1.0 / dx);
+            // record of a sample at or above the first knot: knots 1..n-1 at or below it
+            auto rec_of = [&](double u) {
+                uint32_t r = 0;
+                while (r + 1 < n && (double)d.xf[r + 1] <= u) ++r;
+                return r;
+            };
+            bool ok = true;
             for (uint32_t c = 0; c < nc; ++c) {
                 const double left = x[0] + (double(c) - 1.0) * dx;
                 uint32_t seg = 0;
                 while (seg + 2 < n && (double)d.xf[seg + 1] <= left) ++seg;
                 d.cell[c].seg = seg;
                 d.cell[c].next = d.xf[seg + 1];
+                const uint32_t hi = c + 2 >= nc ? n - 1 : rec_of(x[0] + (double(c) + 2.0) * dx);
+                if (hi > seg + 1) ok = false;
+            }
+            if (ok) {
+                d.ncells = nc;
+                d.x0c = d.xn[0];
+                d.inv_dx = (float)(1.0 / dx);
             }
         }
     }

@@ -179,18 +179,11 @@ __host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size
 
 // ---------------------------------------------------------------- curves
 
-// A segment of the cell lookup: where it starts (arithmetic anchor), the scale
-// of t = (v - anchor) * scale, the next knot (RU-rounded, where the next
-// record takes over), and the power basis c0 + t(c1 + t(c2 + t c3)); both
-// halves sit in one aligned 32-byte sector.
-struct __align__(32) CurveRec {
-    float4 a;                 // {anchor, scale, next knot, 0}
-    float4 k;                 // {c0, c1, c2, c3}
-};
-
 // A cell of the uniform lookup grid: a segment at or below every sample that
 // falls in the cell, and the RU-rounded knot where that segment ends (a sample
 // at or above it starts one segment later).
+constexpr int CURVE_RECS = 288;   // 258 records, padded to whole cache lines
+
 struct __align__(8) CurveCell {
     float next;
     uint32_t seg;
@@ -212,12 +205,15 @@ struct DevCurve {
     float slope[256];         // segment slopes (linear segments and extrapolation)
     float4 coef[256];         // power-basis cubic per segment: c0 + t(c1 + t(c2 + t c3))
     float inv_h[256];         // 1 / (x[i+1] - x[i])
-    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none);
-    // records 0..n-2 are the segments, n-1 the right and n the left linear
-    // extrapolation.
+    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none).
+    // Record r (0..n-2 the segments, n-1 the right and n the left linear
+    // extrapolation) is p(s) = e0 + s(e1 + s(e2 + s e3)), s = v - anchor[r];
+    // each field is its own 128-byte aligned array, so a warp's gather of one
+    // field over a short curve touches a single cache line.
     uint32_t ncells;
     float x0c, inv_dx, pad2;
-    CurveRec rec[258];        // one 32-byte record per segment / extrapolation
+    alignas(128) float anchor[CURVE_RECS];
+    alignas(128) float e[4][CURVE_RECS];
     CurveCell cell[4096];
 };
 

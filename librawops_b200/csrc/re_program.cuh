@@ -40,12 +40,12 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
 }
 
 // Cell lookup (DevCurve::ncells > 0) of M samples at once: the cell gives a
-// segment at or below the sample and the knot ending it, one comparison steps
-// over that knot, a short walk over the RU-rounded knots (which equals the
-// reference's double comparisons for every float sample) covers the rare
-// sample further right, and one power-basis polynomial evaluates the segment.
-// Extrapolation and linear curves are records of the same form.  The loads of
-// all M samples are issued before any of them is used.
+// segment at or below the sample and the knot ending it, one comparison with
+// that knot finds the sample's segment (the host sized the cells for it; the
+// RU-rounded knots make the float comparison equal the reference's double
+// one), and one power-basis polynomial evaluates the segment.  Extrapolation
+// and linear curves are records of the same form.  The loads of all M samples
+// are issued before any of them is used.
 template <int M>
 __device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, int n, int ncells, float xf0,
                                                float x0c, float inv_dx, float* v) {
@@ -57,22 +57,20 @@ __device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, i
         const uint2 e = __ldg(reinterpret_cast<const uint2*>(&c->cell[cell]));
         rec[i] = v[i] < xf0 ? n : (int)e.y + (v[i] >= __uint_as_float(e.x) ? 1 : 0);
     }
-    float t[M];
-    {
-        float4 a[M];
+    float s[M], e0[M], e1[M], e2[M], e3[M];
 #pragma unroll
-        for (int i = 0; i < M; ++i) a[i] = __ldg(&c->rec[rec[i]].a);
-#pragma unroll
-        for (int i = 0; i < M; ++i) {
-            while (rec[i] < n - 1 && v[i] >= a[i].z) a[i] = __ldg(&c->rec[++rec[i]].a);
-            t[i] = (v[i] - a[i].x) * a[i].y;
-        }
+    for (int i = 0; i < M; ++i) {
+        s[i] = __ldg(&c->anchor[rec[i]]);
+        e0[i] = __ldg(&c->e[0][rec[i]]);
+        e1[i] = __ldg(&c->e[1][rec[i]]);
+        e2[i] = __ldg(&c->e[2][rec[i]]);
+        e3[i] = __ldg(&c->e[3][rec[i]]);
     }
-    float4 k[M];
 #pragma unroll
-    for (int i = 0; i < M; ++i) k[i] = __ldg(&c->rec[rec[i]].k);
-#pragma unroll
-    for (int i = 0; i < M; ++i) v[i] = k[i].x + t[i] * (k[i].y + t[i] * (k[i].z + t[i] * k[i].w));
+    for (int i = 0; i < M; ++i) {
+        const float d = v[i] - s[i];
+        v[i] = e0[i] + d * (e1[i] + d * (e2[i] + d * e3[i]));
+    }
 }
 
 __device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
