@@ -98,7 +98,7 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], float*
             G[k] = keep[k] ? rgb[1] : 0.0f;
             B[k] = keep[k] ? rgb[2] : 0.0f;
         }
-        apply_stages_n<4>(P, 0, stage_end, R, G, B, err);
+        apply_stages_n<4, 6>(P, 0, stage_end, R, G, B, err);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             float* o = otile + (2 * qy + (k >> 1)) * (BL_TW * 3) + (2 * qx + (k & 1)) * 3;

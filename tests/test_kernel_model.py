@@ -9,7 +9,8 @@ from kernel_model import model_render
 from oracle.oracle import RawSpec
 
 CASES = [(2, 2, None), (3, 5, None), (5, 3, None), (2, 9, None), (33, 17, None), (40, 20, (1, 1, 37, 17)),
-         (64, 34, None), (37, 19, (2, 1, 33, 17)), (90, 50, (1, 0, 87, 49))]
+         (64, 34, None), (37, 19, (2, 1, 33, 17)), (90, 50, (1, 0, 87, 49)),
+         (80, 84, (1, 3, 77, 79))]
 
 
 @pytest.mark.parametrize("w,h,act", CASES)
