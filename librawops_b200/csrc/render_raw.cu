@@ -818,15 +818,42 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
             B[i] = keep[i] ? (float)bb[i] : 0.0f;
         }
         apply_stages_n<2>(P, 0, stage_end, R, G, B, err);
+        // The tile's row span inside the viewport and 16-byte aligned (the
+        // same for every thread of the block): adjacent lanes pair up, and the
+        // pair's four pixels (48 bytes) leave as three aligned 16-byte stores --
+        // the even lane's own first four floats plus its last two and the odd
+        // lane's first two, the odd lane's last four.  Otherwise single floats.
+        const bool wide = x0 >= ox && x0 + MN_TW <= ox + ow && ((x0 - ox) & 3) == 0 && (out_stride & 3) == 0 &&
+                          (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        if (wide) {
+            const float p0 = __shfl_down_sync(0xffffffffu, R[0], 1);
+            const float p1 = __shfl_down_sync(0xffffffffu, G[0], 1);
+            if (y >= oy && y < oy + oh) {
+                float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x0 - ox) * 3 + 6 * qx;
+                if ((qx & 1) == 0) {
+                    reinterpret_cast<float4*>(o)[0] = make_float4(R[0], G[0], B[0], R[1]);
+                    reinterpret_cast<float4*>(o)[1] = make_float4(G[1], B[1], p0, p1);
+                } else {
+                    *reinterpret_cast<float4*>(o + 2) = make_float4(B[0], R[1], G[1], B[1]);
+                }
+            }
+        } else {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            if (!keep[i]) continue;
-            const int x = x0 + 2 * qx + i;
-            float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
-            o[0] = R[i];
-            o[1] = G[i];
-            o[2] = B[i];
-            if (dirs) dirs[(size_t)(y - oy) * ow + (x - ox)] = hz[i];
+            for (int i = 0; i < 2; ++i) {
+                if (!keep[i]) continue;
+                const int x = x0 + 2 * qx + i;
+                float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x - ox) * 3;
+                o[0] = R[i];
+                o[1] = G[i];
+                o[2] = B[i];
+            }
+        }
+        if (dirs) {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int x = x0 + 2 * qx + i;
+                if (keep[i]) dirs[(size_t)(y - oy) * ow + (x - ox)] = hz[i];
+            }
         }
     }
 }
