@@ -536,7 +536,7 @@ enum { GH_A, GH_B, GV_A, GV_B, CH_A, CH_B, CV_A, CV_B, DH_A, DH_B, DV_A, DV_B, N
 
 template <typename T>
 struct FastSmemT {
-    T raw[4][RQN];               // normalized samples by quad position, r = 6
+    float raw[4][RQN];           // normalized samples by quad position, r = 6 (binary32 values, widened on use)
     T ng[NG_PLANES][QN];         // chroma stage at A and B, r = 4; later red/blue
     T green[2][GQN];             // interpolated green at A and B, r = 2
     uint8_t horiz[2][GQN];       // direction at A and B, r = 2
@@ -549,17 +549,17 @@ constexpr int FAST_RB_PLANES = 3;   // ng planes holding red and blue at G0, G1 
 static_assert(4 * GQN <= FAST_RB_PLANES * QN, "red/blue must fit in the dead chroma planes");
 
 // Raw sample (DX, DY) away from position (I, J) of raw quad rq.
-template <int I, int J, int DX, int DY, typename T>
-__device__ __forceinline__ T raw_q(const T (*raw)[RQN], int rq) {
-    return raw[pos_at(I, J, DX, DY)][rq + quad_at(I, J, DX, DY, RQW)];
+template <typename T, int I, int J, int DX, int DY>
+__device__ __forceinline__ T raw_q(const float (*raw)[RQN], int rq) {
+    return (T)raw[pos_at(I, J, DX, DY)][rq + quad_at(I, J, DX, DY, RQW)];
 }
 
 // MenonDemosaic.cpp:112-115 five-tap directional green at position (I, J)
 // along (DX, DY).
-template <int I, int J, int DX, int DY, typename T>
-__device__ __forceinline__ T five_q(const T (*raw)[RQN], int rq) {
-    return five_tap<T>(raw_q<I, J, -2 * DX, -2 * DY>(raw, rq), raw_q<I, J, -DX, -DY>(raw, rq),
-                       raw[2 * J + I][rq], raw_q<I, J, DX, DY>(raw, rq), raw_q<I, J, 2 * DX, 2 * DY>(raw, rq));
+template <typename T, int I, int J, int DX, int DY>
+__device__ __forceinline__ T five_q(const float (*raw)[RQN], int rq) {
+    return five_tap<T>(raw_q<T, I, J, -2 * DX, -2 * DY>(raw, rq), raw_q<T, I, J, -DX, -DY>(raw, rq),
+                       (T)raw[2 * J + I][rq], raw_q<T, I, J, DX, DY>(raw, rq), raw_q<T, I, J, 2 * DX, 2 * DY>(raw, rq));
 }
 
 // Interpolated green at the non-green sample (DX, DY) away from position
@@ -609,10 +609,10 @@ __device__ __forceinline__ void rb_at_green(const FastSmemT<T>& S, int rq, int k
     constexpr bool red_h = pat(L, (J << 1) | (I ^ 1)) == 0;
     constexpr int rx = red_h ? 1 : 0, ry = red_h ? 0 : 1;   // red axis
     constexpr int bx = 1 - rx, by = 1 - ry;                 // blue axis
-    const T g = S.raw[2 * J + I][rq];
-    rr = r_sub(r_add(g, half_sum(raw_q<I, J, -rx, -ry>(S.raw, rq), raw_q<I, J, rx, ry>(S.raw, rq))),
+    const T g = (T)S.raw[2 * J + I][rq];
+    rr = r_sub(r_add(g, half_sum(raw_q<T, I, J, -rx, -ry>(S.raw, rq), raw_q<T, I, J, rx, ry>(S.raw, rq))),
                half_sum(green_q<I, J, -rx, -ry>(S.green, k), green_q<I, J, rx, ry>(S.green, k)));
-    bb = r_sub(r_add(g, half_sum(raw_q<I, J, -bx, -by>(S.raw, rq), raw_q<I, J, bx, by>(S.raw, rq))),
+    bb = r_sub(r_add(g, half_sum(raw_q<T, I, J, -bx, -by>(S.raw, rq), raw_q<T, I, J, bx, by>(S.raw, rq))),
                half_sum(green_q<I, J, -bx, -by>(S.green, k), green_q<I, J, bx, by>(S.green, k)));
 }
 
@@ -629,7 +629,7 @@ __device__ __forceinline__ void fast_row(const FastSmemT<T>& S, const T* rb, int
     // green position of this row
     rr[GI] = rb[J * GQN + k];
     bb[GI] = rb[(2 + J) * GQN + k];
-    gg[GI] = S.raw[2 * J + GI][rq];
+    gg[GI] = (T)S.raw[2 * J + GI][rq];
     hz[GI] = true;
     // non-green position: its neighbours along the direction are green
     // positions, of this row's kind along the row and of the other row's kind
@@ -639,7 +639,7 @@ __device__ __forceinline__ void fast_row(const FastSmemT<T>& S, const T* rb, int
     const T* blue = red + 2 * GQN;
     const int om = k + (h ? quad_at(NI, J, -1, 0, GQW) : quad_at(NI, J, 0, -1, GQW));
     const int op = k + (h ? quad_at(NI, J, 1, 0, GQW) : quad_at(NI, J, 0, 1, GQW));
-    const T s = S.raw[2 * J + NI][rq];
+    const T s = (T)S.raw[2 * J + NI][rq];
     if (own == 2) {
         bb[NI] = s;
         rr[NI] = r_sub(r_add(s, half_sum(red[om], red[op])), half_sum(blue[om], blue[op]));
@@ -678,9 +678,9 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
     for (int q = t; q < QN; q += MN_THREADS) {
         const int qx = q % QW, qy = q / QW;
         const int rq = (qy + 1) * RQW + qx + 1;
-        const T sa = S.raw[AX][rq], sb = S.raw[2 + BX][rq];
-        const T ha = five_q<AX, 0, 1, 0>(S.raw, rq), va = five_q<AX, 0, 0, 1>(S.raw, rq);
-        const T hb = five_q<BX, 1, 1, 0>(S.raw, rq), vb = five_q<BX, 1, 0, 1>(S.raw, rq);
+        const T sa = (T)S.raw[AX][rq], sb = (T)S.raw[2 + BX][rq];
+        const T ha = five_q<T, AX, 0, 1, 0>(S.raw, rq), va = five_q<T, AX, 0, 0, 1>(S.raw, rq);
+        const T hb = five_q<T, BX, 1, 1, 0>(S.raw, rq), vb = five_q<T, BX, 1, 0, 1>(S.raw, rq);
         S.ng[GH_A][q] = ha;
         S.ng[GV_A][q] = va;
         S.ng[CH_A][q] = r_sub(sa, ha);
