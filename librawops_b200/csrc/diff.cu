@@ -304,27 +304,45 @@ constexpr int BOX_CHUNK = 64;
 
 // out[p][y][x] = sum of in[p][y][x-r..x+r] clipped.  One CTA per (plane, row,
 // segment of BOX_SEG columns): the segment and its halo are staged in shared
-// memory with coalesced loads, then each thread sums its window from there.
-constexpr int BOX_SEG = 256, BOX_MAX_R = 64;
-__global__ void __launch_bounds__(BOX_SEG) box_rows_kernel(const double* __restrict__ in, double* __restrict__ out,
-                                                           GfGeom g, int planes) {
-    __shared__ double seg[BOX_SEG + 2 * BOX_MAX_R];
+// memory with coalesced loads; each thread then slides a window over
+// BOX_RUN consecutive outputs (one full window sum, then one entering and one
+// leaving sample per step).  Entry i of the staged row sits at i + i / BOX_RUN,
+// so the threads' stride-BOX_RUN reads fall in distinct banks.
+constexpr int BOX_THREADS = 256, BOX_RUN = 8, BOX_SEG = BOX_THREADS * BOX_RUN, BOX_MAX_R = 64;
+constexpr int BOX_STAGE = BOX_SEG + 2 * BOX_MAX_R;
+__device__ __forceinline__ int box_slot(int i) { return i + i / BOX_RUN; }
+__global__ void __launch_bounds__(BOX_THREADS) box_rows_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                               GfGeom g, int planes) {
+    __shared__ double seg[BOX_STAGE + BOX_STAGE / BOX_RUN + 1];
     const int x0 = blockIdx.x * BOX_SEG, y = blockIdx.y, p = blockIdx.z;
     const double* row = in + p * g.plane + (size_t)y * g.w;
     const int n = BOX_SEG + 2 * g.r;
-    for (int i = threadIdx.x; i < n; i += BOX_SEG) {
+    for (int i = threadIdx.x; i < n; i += BOX_THREADS) {
         const int x = x0 - g.r + i;
-        seg[i] = (x >= 0 && x < g.w) ? row[x] : 0.0;
+        seg[box_slot(i)] = (x >= 0 && x < g.w) ? row[x] : 0.0;
     }
     __syncthreads();
-    const int x = x0 + (int)threadIdx.x;
-    if (x >= g.w) return;
+    const int i0 = (int)threadIdx.x * BOX_RUN;   // first output of this thread, relative to x0
+    if (x0 + i0 >= g.w) return;
     double s = 0;
-    for (int j = 0; j <= 2 * g.r; ++j) s += seg[threadIdx.x + j];
-    out[p * g.plane + (size_t)y * g.w + x] = s;
+    for (int j = 0; j <= 2 * g.r; ++j) s += seg[box_slot(i0 + j)];
+    double* o = out + p * g.plane + (size_t)y * g.w + x0 + i0;
+    o[0] = s;
+#pragma unroll
+    for (int k = 1; k < BOX_RUN; ++k) {
+        if (x0 + i0 + k >= g.w) break;
+        s += seg[box_slot(i0 + k + 2 * g.r)];
+        s -= seg[box_slot(i0 + k - 1)];
+        o[k] = s;
+    }
 }
 
-// out[p][y][x] = sum of in[p][y-r..y+r][x] clipped; one thread per (plane, column, chunk of rows)
+// out[p][y][x] = sum of in[p][y-r..y+r][x] clipped; one thread per (plane,
+// column, chunk of rows), a sliding sum down the chunk.  The rows entering and
+// leaving the window are fetched BOX_STEP at a time before any is added, so a
+// thread keeps that many loads in flight; the additions run in the order of a
+// row-by-row slide.
+constexpr int BOX_STEP = 8;
 __global__ void box_cols_kernel(const double* __restrict__ in, double* __restrict__ out, GfGeom g, int planes) {
     const int chunks = (g.h + BOX_CHUNK - 1) / BOX_CHUNK;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -336,11 +354,21 @@ __global__ void box_cols_kernel(const double* __restrict__ in, double* __restric
     const int y0 = chunk * BOX_CHUNK, y1 = min(y0 + BOX_CHUNK, g.h);
     double s = 0;
     for (int j = max(0, y0 - g.r); j <= min(g.h - 1, y0 + g.r); ++j) s += col[(size_t)j * g.w];
-    for (int y = y0; y < y1; ++y) {
-        ocol[(size_t)y * g.w] = s;
-        const int add = y + 1 + g.r, sub = y - g.r;
-        if (add < g.h) s += col[(size_t)add * g.w];
-        if (sub >= 0) s -= col[(size_t)sub * g.w];
+    for (int y = y0; y < y1; y += BOX_STEP) {
+        double add[BOX_STEP], sub[BOX_STEP];
+#pragma unroll
+        for (int k = 0; k < BOX_STEP; ++k) {
+            const int a = y + k + 1 + g.r, b = y + k - g.r;
+            add[k] = (y + k < y1 && a < g.h) ? col[(size_t)a * g.w] : 0.0;
+            sub[k] = (y + k < y1 && b >= 0) ? col[(size_t)b * g.w] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < BOX_STEP; ++k) {
+            if (y + k >= y1) break;
+            ocol[(size_t)(y + k) * g.w] = s;
+            if (y + k + 1 + g.r < g.h) s += add[k];
+            if (y + k - g.r >= 0) s -= sub[k];
+        }
     }
 }
 
@@ -506,7 +534,7 @@ YW weights(uint32_t space) {
 }
 
 void box(const double* in, double* tmp, double* out, const GfGeom& g, int planes, cudaStream_t s) {
-    box_rows_kernel<<<dim3((g.w + BOX_SEG - 1) / BOX_SEG, g.h, planes), BOX_SEG, 0, s>>>(in, tmp, g, planes);
+    box_rows_kernel<<<dim3((g.w + BOX_SEG - 1) / BOX_SEG, g.h, planes), BOX_THREADS, 0, s>>>(in, tmp, g, planes);
     dim3 grid((g.w + 127) / 128, (g.h + BOX_CHUNK - 1) / BOX_CHUNK, planes);
     box_cols_kernel<<<grid, 128, 0, s>>>(tmp, out, g, planes);
 }
