@@ -111,11 +111,11 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, window="timed region"):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        window = self.lines[getattr(self, "first", 0):getattr(self, "last", len(self.lines)) + 1]
-        for line in window:
+        sampled = self.lines[getattr(self, "first", 0):getattr(self, "last", len(self.lines)) + 1]
+        for line in sampled:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -128,16 +128,20 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0, "window": window}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 class CpuReference:
     """The reference's own CPU implementation of the workload: the reference
-    library built from its sources (oracle/_ref), driven through its
-    TileScheduler with one worker per host core; the C oracle port (one thread)
-    when that library is absent."""
+    library built from its sources (oracle/_ref), driven through its own
+    TileScheduler with one worker per host core.  The RawImage, the node chain
+    and the scheduler are built once, outside the timing; a timed render
+    submits the frame's render tiles (tile 512: 96 requests for the
+    6000x4000 frame), waits for them and assembles the frame -- the work a
+    reference caller repeats per frame.  When that library is absent, the C
+    oracle port renders the frame on one thread."""
 
     def __init__(self, workload):
         from oracle.oracle import (OP_CAMERA_TO_WORKING, OP_CURVES_EXT, OP_DISPLAY_TAG, OP_SRGB_ENCODE,
@@ -151,33 +155,33 @@ class CpuReference:
                     Op(OP_CURVES_EXT, curves_params(1, w.curve)), Op(OP_WORKING_TO_SRGB), Op(OP_DISPLAY_TAG),
                     Op(OP_SRGB_ENCODE)]
         self.cores = os.cpu_count() or 1
+        self.out = np.zeros((w.active[3], w.active[2], 3), np.float32)
         if reference_available():
-            self.impl, self.kind, self.threads = Reference(), "reference", min(self.cores, 64)
+            self.kind, self.threads = "reference", min(self.cores, 64)
+            self.session = Reference().session(self.raw, True, self.ops, self.threads)
         else:
-            self.impl, self.kind, self.threads = Oracle(), "port", 1
+            self.kind, self.threads = "port", 1
+            self.oracle = Oracle()
             self.ops = [o for o in self.ops if o.code != OP_DISPLAY_TAG]
 
-    def strip(self, rows):
-        ax, ay, aw, ah = self.w.active
-        return (ax, ay + ah // 2 - rows // 2, aw, rows)
-
-    def render_seconds(self, rows):
-        s = self.strip(rows)
+    def frame_seconds(self):
         t0 = time.perf_counter()
         if self.kind == "reference":
-            self.impl.render_raw(self.raw, True, self.ops, s, tile=self.w.tile, scheduled_workers=self.threads)
+            self.session.render(self.w.active, tile=self.w.tile, out=self.out)
         else:
-            self.impl.render_raw(self.raw, True, self.ops, s)
+            self.out = self.oracle.render_raw(self.raw, True, self.ops, self.w.active)
         return time.perf_counter() - t0
 
-    def rate(self, rows, repeats):
-        self.render_seconds(8)
-        times = [self.render_seconds(rows) for _ in range(repeats)]
-        return rows * self.w.active[2] / statistics.median(times) / 1e6
+    def rate(self, repeats):
+        self.frame_seconds()
+        times = [self.frame_seconds() for _ in range(repeats)]
+        return self.w.pixels / statistics.median(times) / 1e6
 
-    def sample_text(self, rows, repeats):
-        s = self.strip(rows)
-        return f"{s[2]}x{s[3]} strip of the frame, tile {self.w.tile}, median of {repeats}"
+    def sample_text(self, repeats, stat="median"):
+        ax, ay, aw, ah = self.w.active
+        how = (f"its TileScheduler, {self.threads} workers, tile {self.w.tile}" if self.kind == "reference"
+               else "the C port, one thread")
+        return f"the whole {aw}x{ah} frame through {how}; setup outside the timing; {stat} of {repeats} frames"
 
 
 def run_reference(args, rank):
@@ -185,20 +189,20 @@ def run_reference(args, rank):
     if rank != 0:
         return
     ref = CpuReference(workloads.menon_24mp())
-    # each step is a bounded strip of the frame, sized so that the whole run
-    # stays near a minute of host time
-    rows = max(2, min(400, int(40000 / max(1, args.steps + args.warmup))))
+    # one step renders the whole frame, as the GPU arm's step does
     for _ in range(args.warmup):
-        ref.render_seconds(rows)
-    t = [ref.render_seconds(rows) for _ in range(args.steps)]
-    value = rows * ref.w.active[2] * len(t) / sum(t) / 1e6
+        ref.frame_seconds()
+    t = [ref.frame_seconds() for _ in range(args.steps)]
+    value = ref.w.pixels * len(t) / sum(t) / 1e6
     line = {"metric": METRIC, "value": round(value, 3), "unit": "Mpix/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(t) / len(t), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": ref.w.name, "sample_rows_per_step": rows, "tile": ref.w.tile},
+            "config": {"workload": ref.w.name, "tile": ref.w.tile,
+                       "frame": f"{ref.w.active[2]}x{ref.w.active[3]} active of {ref.w.width}x{ref.w.height} "
+                                f"BGGR stride {ref.w.stride}"},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": ref.threads, "kind": ref.kind,
-                             "sample": ref.sample_text(rows, args.steps)},
+                             "sample": ref.sample_text(args.steps, "mean")},
             "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -241,12 +245,22 @@ def run_ours(args, rank, world, local_rank):
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clocks = ClockSampler(local_rank).start()
+    # The timed region is short (K steps of well under a millisecond), shorter
+    # than the sampler's interval.  Untimed steps run for half a second right
+    # before it, inside the sampled window, so the clock record covers the GPU
+    # under this load: the reported window is that soak plus the timed steps.
+    clocks.mark()
+    soak_end = time.time() + 0.5
+    with torch.cuda.stream(stream):
+        while time.time() < soak_end:
+            for _ in range(20):
+                step()
+            torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t_begin = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
-    clocks.mark()
     t_begin.record(stream)
     for i in range(args.steps):
         starts[i].record(stream)
@@ -280,6 +294,12 @@ def run_ours(args, rank, world, local_rank):
     whole_ms = timed(lambda: render.render_async(img, pipe, w.active, out, status, stream=stream), reps)
     render.status_from_device(int(status.item()))
     mixed = _mixed_batch(render, workloads, torch, dev, stream, reps=max(3, min(args.steps, 20)))
+    peak, peak_kind = _peaks()
+    configs = _config_legs(render, workloads, torch, dev, stream, peak, reps=max(3, min(args.steps, 10)))
+    try:
+        scheduler = _scheduler_leg(workloads)
+    except Exception as e:   # no host compiler
+        scheduler = {"error": str(e)[-300:]}
     differentiable = _differentiable(torch, dev, reps=3)
 
     # end-to-end through the public API: each step uploads its Bayer frame from
@@ -340,8 +360,8 @@ def run_ours(args, rank, world, local_rank):
     traffic = _traffic_from_profile()
     try:
         ref = CpuReference(w)
-        cpu = {"value": round(ref.rate(200, 3), 3), "unit": "Mpix/s", "cores": ref.threads, "kind": ref.kind,
-               "sample": ref.sample_text(200, 3)}
+        cpu = {"value": round(ref.rate(3), 3), "unit": "Mpix/s", "cores": ref.threads, "kind": ref.kind,
+               "sample": ref.sample_text(3)}
     except Exception as e:  # the checker libraries are missing
         cpu = {"value": None, "unit": "Mpix/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
     line = {
@@ -361,21 +381,121 @@ def run_ours(args, rank, world, local_rank):
             "per_tile_mpix_s": round(pixels / (per_tile_ms * 1e-3) / 1e6, 2),
             "speedup": round(per_tile_ms / ms_per_step, 3),
             "single_launch_whole_frame_mpix_s": round(pixels / (whole_ms * 1e-3) / 1e6, 2),
-            "mixed_batch": mixed},
+            "mixed_batch": mixed,
+            "mixed_batch_through_tile_scheduler": scheduler},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s", "algorithmic_bytes_per_px": ALGO_BYTES_PER_PX,
                      "kernel": "menon_kernel" if tuned["dispatch"] == 3 else "batch_render_kernel",
                      "kernel_ms": round(kernel_ms, 5)},
+        "configs": configs,
         "differentiable": differentiable,
         "cpu_baseline": cpu,
         "e2e": {"value": round(world * pixels / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s",
                 "h2d_bytes_per_step": int(samples_host.nbytes), "d2h_bytes_per_step": int(pixels * 12)},
         "gpu_launches": args.steps,
-        "clocks": clocks.summary(),
+        "clocks": clocks.summary("0.5 s of untimed steps immediately before the timed steps, and the timed "
+                                 "steps"),
     }
     print(json.dumps(line), flush=True)
+
+
+def _scheduler_leg(workloads):
+    """The mixed batch submitted through the drop-in C++ TileScheduler
+    (tests/cpp/scheduler_driver.cpp, compiled against include/ and the
+    library): wall time of all requests through Renderer::render_image one at
+    a time vs through the scheduler's batched waves, host and device tiles,
+    every tile checked bit-equal to the direct render."""
+    import tempfile
+    lib_dir = os.path.join(ROOT, "librawops_b200", "_lib")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "scheduler_driver")
+        subprocess.run(["g++", "-std=c++20", "-O2", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "scheduler_driver.cpp"), "-L", lib_dir,
+                        "-lrawengine_b200", f"-Wl,-rpath,{lib_dir}", "-pthread", "-o", exe], check=True)
+        images, recipes, tiles = workloads.mixed_batch()
+        spec = os.path.join(tmp, "spec.txt")
+        workloads.write_scheduler_spec(spec, images, recipes, tiles)
+        p = subprocess.run([exe, spec, "2"], capture_output=True, text=True, timeout=900)
+        if p.returncode != 0:
+            return {"error": (p.stdout + p.stderr)[-500:]}
+        r = json.loads(p.stdout.strip().splitlines()[-1])
+    r["speedup_host_tiles"] = round(r["per_request_s"] / r["scheduler_host_s"], 3)
+    r["speedup_device_tiles"] = round(r["per_request_s"] / r["scheduler_device_s"], 3)
+    return r
+
+
+def _per_launch_ms(torch, stream, fn, reps, flush=None):
+    """Mean device time of one call of `fn` (CUDA events on `stream` around
+    each call), after three untimed calls; `flush` (untimed, between calls)
+    evicts L2 when a call's inputs and outputs fit in it."""
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            fn()
+        times = []
+        for _ in range(reps):
+            if flush is not None:
+                flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            times.append((e0, e1))
+    torch.cuda.synchronize()
+    return statistics.mean(a.elapsed_time(b) for a, b in times)
+
+
+def _roofline_leg(ms, pixels, bytes_per_px, peak, **extra):
+    achieved = bytes_per_px * pixels / (ms * 1e-3) / 1e9
+    leg = {"ms": round(ms, 5), "mpix_s": round(pixels / (ms * 1e-3) / 1e6, 1),
+           "algorithmic_bytes_per_px": bytes_per_px, "achieved_gb_s": round(achieved, 1),
+           "frac": round(achieved / peak, 4)}
+    leg.update(extra)
+    return leg
+
+
+def _config_legs(render, workloads, torch, dev, stream, peak, reps):
+    """The other configurations, each kernel timed by CUDA events against the
+    HBM roofline: the bilinear render to float32 linear ProPhoto (1024x768,
+    and a 6000x4000 instance of the same generator and recipe), the guided
+    filter on the 6000x4000 raster at r 8/32 x eps 1e-3/1e-2, and box local
+    statistics at r 16."""
+    from librawops_b200 import synthetic
+    legs = {}
+    flush_buf = torch.empty(64 << 20, dtype=torch.float32, device=dev)   # 256 MB > L2
+
+    def flush():
+        flush_buf.zero_()
+
+    for w in (workloads.bilinear_1mp(), workloads.bilinear_1mp(width=6000, height=4000, seed=5)):
+        meta = render.Metadata(w.width, w.height, w.stride, w.pattern, *w.phase, w.active, w.black,
+                               (w.white,) * 4)
+        img = render.Image(meta, torch.from_numpy(w.samples().reshape(-1).view(np.int16)).to(dev))
+        pipe = workloads.pipeline_for(w)
+        out = torch.empty((w.active[3], w.active[2], 3), dtype=torch.float32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        small = w.pixels * 14 < (126 << 20)
+        ms = _per_launch_ms(torch, stream, lambda: render.render_async(img, pipe, w.active, out, status,
+                                                                     stream=stream),
+                            reps, flush if small else None)
+        render.status_from_device(int(status.item()))
+        legs[f"bilinear_linear_prophoto_{w.width}x{w.height}"] = _roofline_leg(
+            ms, w.pixels, 14, peak, kernel="bilinear_kernel",
+            l2="L2 flushed between launches" if small else "inputs+outputs > L2")
+        img.close()
+    rgb = torch.from_numpy(synthetic.raster(6000, 4000, seed=3)).to(dev)
+    px = 6000 * 4000
+    gf_out = torch.empty_like(rgb)
+    for radius in (8, 32):
+        for eps in (1e-3, 1e-2):
+            ms = _per_launch_ms(torch, stream, lambda: render.guided_filter(rgb, radius, eps, out=gf_out,
+                                                                          stream=stream), reps)
+            legs[f"guided_filter_6000x4000_r{radius}_eps{eps:g}"] = _roofline_leg(ms, px, 24, peak,
+                                                                                 kernel="guided filter")
+    ms = _per_launch_ms(torch, stream, lambda: render.local_statistics(rgb, 16, stream=stream), reps)
+    legs["local_statistics_6000x4000_r16"] = _roofline_leg(ms, px, 36, peak, kernel="local statistics")
+    return legs
 
 
 def _mixed_batch(render, workloads, torch, dev, stream, reps):

@@ -141,9 +141,27 @@ private:
 
 enum class RenderPriority { Background = 0, Normal = 1, Interactive = 2 };
 
-// Queued requests run in priority order, FIFO within a priority; each worker
-// thread renders on its own CUDA stream.  Throws length_error when the pending
-// budget is full; cancellation is checked before and between tiles.
+// A render result left in device memory (no counterpart in the reference,
+// whose results are host tiles): bounds.height rows of bounds.width * 3
+// interleaved float32 RGB values, contiguous, on the device that was current
+// when the scheduler was created.  The memory stays valid while any copy of
+// the DeviceTile (or of its rgb pointer) lives.
+struct DeviceTile {
+    Rect bounds;
+    std::shared_ptr<const float> rgb;
+    ImageDescriptor descriptor = ImageDescriptor::camera_linear();
+    RAWENGINE_API Tile to_host() const;   // copies the pixels into a host Tile
+};
+
+// Queued requests are taken in priority order, FIFO within a priority, and
+// rendered in waves: a dispatch lane takes every pending request it can hold
+// at once, renders the requests whose chains are a RAW source under point
+// nodes as ONE batched device render (a persistent kernel over all of their
+// tiles), renders any other request through its node, and resolves the
+// futures.  `workers` is the number of lanes (1..64); each lane has its own
+// CUDA stream, so waves of different lanes overlap.  Throws length_error when
+// the pending budget is full; cancellation is checked before a wave is
+// rendered and again before its result is delivered.
 class RAWENGINE_API TileScheduler final {
 public:
     TileScheduler(std::size_t workers, std::size_t max_pending);
@@ -163,10 +181,25 @@ public:
                                     Rect viewport, RenderPriority priority = RenderPriority::Interactive,
                                     std::uint32_t tile_size = 256,
                                     std::shared_ptr<CancellationToken> cancellation = nullptr);
+    // The same request with the result left in device memory (no
+    // counterpart in the reference): no device-to-host copy is made.
+    std::future<DeviceTile> submit_device(std::shared_ptr<const Node> output, Rect source_bounds,
+                                          RenderRequest request, RenderPriority priority = RenderPriority::Normal,
+                                          std::shared_ptr<CancellationToken> cancellation = nullptr);
+    std::future<DeviceTile> submit_latest_device(std::string group, std::shared_ptr<const Node> output,
+                                                 Rect source_bounds, RenderRequest request,
+                                                 RenderPriority priority = RenderPriority::Interactive,
+                                                 std::shared_ptr<CancellationToken> cancellation = nullptr);
+    struct Stats {
+        std::uint64_t waves = 0;            // waves rendered
+        std::uint64_t batched_requests = 0; // requests rendered inside a batched device render
+        std::uint64_t node_requests = 0;    // requests rendered through their node
+        std::uint64_t unbatchable_requests = 0;  // node requests whose chain is not a RAW point chain
+        std::uint64_t batch_fallbacks = 0;  // waves whose batched render failed and were re-rendered per request
+        std::string last_fallback;          // the error text of the last such failure
+    };
+    Stats stats() const;
 private:
-    std::future<Tile> submit_request(std::string group, std::shared_ptr<const Node> output, Rect source_bounds,
-                                     RenderRequest request, RenderPriority priority,
-                                     std::shared_ptr<CancellationToken> cancellation);
     struct Impl;
     std::unique_ptr<Impl> impl_;
 };

@@ -183,6 +183,19 @@ struct Tile {
     ImageDescriptor descriptor = ImageDescriptor::camera_linear();
 };
 
+// The ICC profile and conversion policy an encoded-raster source node reports
+// (RawEngine.hpp:212-219 of the reference).  No node of this library has one;
+// the type exists so that nodes written against the reference's Node
+// interface compile unchanged.
+struct IccProfileIdentity {
+    std::array<std::uint8_t, 32> profile_sha256{};
+    std::string intent = "relative_colorimetric";
+    bool black_point_compensation = false;
+    std::string engine = "lcms2-core";
+    std::string engine_version = "2.19.1";
+    bool operator==(const IccProfileIdentity&) const = default;
+};
+
 struct RawDemosaicIdentity {
     std::string algorithm = "rawengine.bilinear";
     std::uint32_t processing_version = 1;
@@ -212,6 +225,11 @@ public:
         if (level.mip == 0 && level.quality == RenderQuality::Final) return input_region(output, source_bounds);
         throw std::invalid_argument("node has no mapping for this render level");
     }
+    // Identity hooks of the reference's Node (RawEngine.hpp:263-268).  The
+    // device executor does not consult them; they return no identity unless a
+    // subclass overrides them.
+    virtual std::optional<IccProfileIdentity> input_icc_identity() const { return std::nullopt; }
+    virtual std::optional<std::array<std::uint8_t, 32>> source_fingerprint() const { return std::nullopt; }
     virtual std::optional<Rect> source_bounds() const { return std::nullopt; }
     virtual std::optional<RawDemosaicIdentity> raw_demosaic_identity() const { return std::nullopt; }
 };

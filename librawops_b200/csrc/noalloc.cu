@@ -85,7 +85,9 @@ size_t re_render_raw_reduced_noalloc_max_native_pixels(void) { return kNoAllocMa
 
 re_status re_render_raw_reduced_noalloc(const re_image* image, const re_render_desc* desc, re_rect viewport,
                                         uint32_t mip, float* out, size_t out_row_stride, void* stream_) {
-    if (!image || !desc || !out) {
+    // Same argument rules as re_render_raw: a null output is accepted for an
+    // empty viewport, which renders nothing.
+    if (!image || !desc || (!out && viewport.width && viewport.height)) {
         set_last_error("null render arguments");
         return RE_INVALID_ARGUMENT;
     }

@@ -1129,153 +1129,420 @@ void analyze_local_rgb(const ImageGraph& graph, const RenderRequest& request, co
 
 // ----------------------------------------------------------- TileScheduler
 
-// The queue semantics of TileScheduler.cpp:19-304: priority then FIFO, a
-// pending budget (length_error) in which queued requests of the caller's
-// supersession group do not count, a new group request cancelling the group's
-// running request and failing its queued ones, destruction failing pending
-// requests and waiting for running ones.  Queued jobs live in one ordered map
-// keyed by (descending priority, arrival), with a per-group count; each worker
-// thread renders on its own CUDA stream, so requests on different workers
-// overlap on the device.
+namespace {
+
+// A request whose chain is a RAW source under point nodes only, lowered to the
+// fused render the executor would launch for it (Executor::eval_raw): the
+// device image and the render description.  Returns false for any other chain
+// (spatial, geometry, raster or caller nodes), and for chains the executor
+// must reject, so that the error comes from the executor as it would for a
+// direct render.
+struct RawLowering {
+    const re_image* image = nullptr;
+    re_render_desc desc{};
+};
+
+bool lower_raw_chain(const Node& node, RenderLevel level, RawLowering& out) {
+    if (!node.supports_level(level)) return false;
+    std::vector<const PointNode*> chain;
+    const Node* cur = &node;
+    while (auto* p = dynamic_cast<const PointNode*>(cur)) {
+        chain.push_back(p);
+        cur = p->input().get();
+    }
+    auto* raw = dynamic_cast<const RawUnpackNode*>(cur);
+    if (!raw) return false;
+    std::reverse(chain.begin(), chain.end());
+    int anchor = -1;
+    for (int i = (int)chain.size() - 1; i >= 0 && level.mip; --i)
+        if (dynamic_cast<const CameraToWorkingNode*>(chain[i])) {
+            anchor = i;
+            break;
+        }
+    StageList sl;
+    sl.desc.demosaic = raw->menon() ? 1u : 0u;
+    sl.desc.anchor = -1;
+    try {
+        for (int i = 0; i < (int)chain.size(); ++i) add_stage(sl, chain[i], i == anchor, level);
+        if (level.mip && sl.desc.anchor < 0) return false;
+        out.image = raw->image().device().handle;
+    } catch (...) {
+        return false;
+    }
+    out.desc = sl.desc;
+    return true;
+}
+
+// Canonical bytes of a render description, so that requests with equal
+// recipes share one device program inside a batch.
+std::string desc_key(const re_render_desc& d) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    put(&d.demosaic, sizeof d.demosaic);
+    put(&d.anchor, sizeof d.anchor);
+    put(&d.count, sizeof d.count);
+    for (uint32_t i = 0; i < d.count && i < RE_MAX_STAGES; ++i) {
+        put(&d.stages[i].kind, sizeof(uint32_t));
+        put(&d.stages[i].arg, sizeof(uint32_t));
+        put(d.stages[i].f, sizeof d.stages[i].f);
+    }
+    put(d.curves, sizeof d.curves);
+    return k;
+}
+
+// Device memory handed out in DeviceTiles: freed stream-ordered on the legacy
+// default stream once the last tile that points into it is released.
+std::shared_ptr<float> device_block(size_t bytes, cudaStream_t s) {
+    float* p = nullptr;
+    if (bytes) check_cuda(cudaMallocAsync((void**)&p, bytes, s), "scheduler output");
+    return std::shared_ptr<float>(p, [](float* q) {
+        if (q) cudaFreeAsync(q, nullptr);
+    });
+}
+
+}  // namespace
+
+Tile DeviceTile::to_host() const {
+    Tile t{bounds, std::vector<float>((size_t)bounds.width * bounds.height * 3), descriptor};
+    if (!t.rgb.empty())
+        check_cuda(cudaMemcpy(t.rgb.data(), rgb.get(), t.rgb.size() * sizeof(float), cudaMemcpyDeviceToHost),
+                   "device tile download");
+    return t;
+}
+
+// Pending requests sit in one ordered map keyed by (descending priority,
+// arrival), with a count per supersession group for the budget rule.  Lanes
+// take WAVES: everything pending (up to a request and byte limit) in key order.
+// Taken requests stay listed as in flight until their futures resolve, so that
+// a newer request of their group can cancel them.
 struct TileScheduler::Impl {
-    struct Job {
-        std::shared_ptr<const Node> output;
+    struct Request {
+        std::shared_ptr<const Node> node;
         Rect source_bounds;
         RenderRequest request;
-        std::shared_ptr<CancellationToken> cancellation;
+        std::shared_ptr<CancellationToken> token;
         std::string group;
-        std::promise<Tile> result;
-    };
-    using Key = std::pair<int, uint64_t>;  // (-priority, arrival)
+        bool device = false;
+        std::promise<Tile> host_result;
+        std::promise<DeviceTile> device_result;
 
-    Impl(size_t workers, size_t budget) : budget(budget) {
-        if (!workers || workers > 64 || !budget)
+        bool cancelled() const { return token && token->is_cancelled(); }
+        void fail(std::exception_ptr e) {
+            if (device) device_result.set_exception(e);
+            else host_result.set_exception(e);
+        }
+        uint64_t bytes() const { return (uint64_t)request.viewport.width * request.viewport.height * 12; }
+    };
+    using RequestPtr = std::shared_ptr<Request>;
+    using Order = std::pair<int, uint64_t>;
+
+    static constexpr size_t kWaveRequests = 8192;
+    static constexpr uint64_t kWaveBytes = 3ull << 30;   // device outputs of one wave
+
+    struct Lane {
+        cudaStream_t stream = nullptr;   // batched renders and their copies
+        re_batch* batch = nullptr;
+        std::thread thread;
+    };
+
+    Impl(size_t lanes, size_t budget) : budget_(budget) {
+        if (!lanes || lanes > 64 || !budget)
             throw std::invalid_argument("scheduler needs 1-64 workers and a pending budget");
+        if (cudaGetDevice(&device_) != cudaSuccess) device_ = 0;   // lanes then report the error per request
+        lanes_.resize(lanes);
         try {
-            for (size_t i = 0; i < workers; ++i) threads.emplace_back([this] { work(); });
+            for (Lane& lane : lanes_) lane.thread = std::thread([this, &lane] { run_lane(lane); });
         } catch (...) {
-            shutdown();
+            close();   // joins the lanes that did start
             throw;
         }
     }
-    ~Impl() { shutdown(); }
 
-    void shutdown() {
+    ~Impl() { close(); }
+
+    // Fails every pending request with RenderCancelled, lets each lane finish
+    // the wave it holds, and joins the lanes.
+    void close() {
+        std::vector<RequestPtr> dropped;
         {
-            std::lock_guard<std::mutex> lock(mutex);
-            stopping = true;
-            for (auto& [key, job] : queued) job->result.set_exception(std::make_exception_ptr(RenderCancelled()));
-            queued.clear();
-            group_count.clear();
-            latest.clear();
+            std::lock_guard<std::mutex> lock(mu_);
+            closing_ = true;
+            for (auto& entry : pending_) dropped.push_back(std::move(entry.second));
+            pending_.clear();
+            pending_in_group_.clear();
         }
-        ready.notify_all();
-        for (auto& t : threads)
-            if (t.joinable()) t.join();
+        for (auto& r : dropped) r->fail(std::make_exception_ptr(RenderCancelled()));
+        wake_.notify_all();
+        for (Lane& lane : lanes_)
+            if (lane.thread.joinable()) lane.thread.join();
     }
 
-    std::shared_ptr<Job> take() {
-        std::unique_lock<std::mutex> lock(mutex);
-        ready.wait(lock, [&] { return stopping || !queued.empty(); });
-        if (queued.empty()) return nullptr;
-        auto job = std::move(queued.begin()->second);
-        queued.erase(queued.begin());
-        if (!job->group.empty()) --group_count[job->group];
-        return job;
-    }
-
-    void work() {
-        while (auto job = take()) {
-            std::optional<Tile> tile;
-            std::exception_ptr failure;
-            try {
-                if (job->cancellation && job->cancellation->is_cancelled()) throw RenderCancelled();
-                tile = Renderer().render_image(*job->output, job->source_bounds, job->request, job->cancellation.get());
-            } catch (...) {
-                failure = std::current_exception();
-            }
-            std::lock_guard<std::mutex> lock(mutex);
-            if (!failure && job->cancellation && job->cancellation->is_cancelled())
-                failure = std::make_exception_ptr(RenderCancelled());
-            if (failure) job->result.set_exception(failure);
-            else job->result.set_value(std::move(*tile));
-            if (!job->group.empty()) {
-                auto it = latest.find(job->group);
-                if (it != latest.end() && it->second.lock() == job->cancellation) latest.erase(it);
-            }
-        }
-    }
-
-    void enqueue(std::shared_ptr<Job> job, RenderPriority priority) {
+    // Adds a request (the budget and supersession rules of TileScheduler.cpp:122-160).
+    void add(RequestPtr r, RenderPriority priority) {
+        std::vector<RequestPtr> superseded;
         {
-            std::lock_guard<std::mutex> lock(mutex);
-            const size_t replaced = job->group.empty() ? 0 : group_count[job->group];
-            if (queued.size() - replaced >= budget) throw std::length_error("scheduler pending request budget is full");
-            if (!job->group.empty()) {
-                if (auto it = latest.find(job->group); it != latest.end())
-                    if (auto running = it->second.lock()) running->cancel();
-                for (auto it = queued.begin(); it != queued.end();) {
-                    if (it->second->group != job->group) {
+            std::lock_guard<std::mutex> lock(mu_);
+            const size_t replaceable = r->group.empty() ? 0 : count_in_group(r->group);
+            if (pending_.size() - replaceable >= budget_)
+                throw std::length_error("scheduler pending request budget is full");
+            if (!r->group.empty()) {
+                for (auto it = pending_.begin(); it != pending_.end();) {
+                    if (it->second->group == r->group) {
+                        if (it->second->token) it->second->token->cancel();
+                        superseded.push_back(std::move(it->second));
+                        it = pending_.erase(it);
+                    } else {
                         ++it;
-                        continue;
                     }
-                    it->second->cancellation->cancel();
-                    it->second->result.set_exception(std::make_exception_ptr(RenderCancelled()));
-                    it = queued.erase(it);
                 }
-                group_count[job->group] = 1;
-                latest[job->group] = job->cancellation;
+                for (const RequestPtr& f : in_flight_)
+                    if (f->group == r->group && f->token) f->token->cancel();
+                pending_in_group_[r->group] = 1;
             }
-            queued.emplace(Key{-(int)priority, arrivals++}, std::move(job));
+            pending_.emplace(Order{-(int)priority, next_arrival_++}, std::move(r));
         }
-        ready.notify_one();
+        for (auto& s : superseded) s->fail(std::make_exception_ptr(RenderCancelled()));
+        wake_.notify_one();
     }
 
-    const size_t budget;
-    std::mutex mutex;
-    std::condition_variable ready;
-    std::map<Key, std::shared_ptr<Job>> queued;
-    std::map<std::string, size_t> group_count;
-    std::map<std::string, std::weak_ptr<CancellationToken>> latest;
-    std::vector<std::thread> threads;
-    uint64_t arrivals = 0;
-    bool stopping = false;
+    Stats stats() const {
+        std::lock_guard<std::mutex> lock(mu_);
+        return stats_;
+    }
+
+private:
+    size_t count_in_group(const std::string& g) const {
+        auto it = pending_in_group_.find(g);
+        return it == pending_in_group_.end() ? 0 : it->second;
+    }
+
+    // Blocks until requests are pending (or the scheduler closes: empty wave).
+    std::vector<RequestPtr> take_wave() {
+        std::unique_lock<std::mutex> lock(mu_);
+        wake_.wait(lock, [&] { return closing_ || !pending_.empty(); });
+        std::vector<RequestPtr> wave;
+        uint64_t bytes = 0;
+        while (!pending_.empty() && wave.size() < kWaveRequests) {
+            const RequestPtr& next = pending_.begin()->second;
+            if (!wave.empty() && bytes + next->bytes() > kWaveBytes) break;
+            bytes += next->bytes();
+            if (!next->group.empty()) --pending_in_group_[next->group];
+            in_flight_.push_back(next);
+            wave.push_back(next);
+            pending_.erase(pending_.begin());
+        }
+        if (!wave.empty()) ++stats_.waves;
+        return wave;
+    }
+
+    void retire(const std::vector<RequestPtr>& wave) {
+        std::lock_guard<std::mutex> lock(mu_);
+        for (const RequestPtr& r : wave) {
+            auto it = std::find(in_flight_.begin(), in_flight_.end(), r);
+            if (it != in_flight_.end()) in_flight_.erase(it);
+        }
+    }
+
+    void run_lane(Lane& lane) {
+        cudaSetDevice(device_);
+        if (cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking) != cudaSuccess) lane.stream = nullptr;
+        if (re_batch_create(&lane.batch) != RE_OK) lane.batch = nullptr;
+        for (;;) {
+            std::vector<RequestPtr> wave = take_wave();
+            if (wave.empty()) break;
+            render_wave(lane, wave);
+            retire(wave);
+        }
+        if (lane.batch) re_batch_destroy(lane.batch);
+        if (lane.stream) cudaStreamDestroy(lane.stream);
+    }
+
+    // One request through its node on this thread's executor stream, exactly
+    // as Renderer::render_image would render it.
+    void render_one(Request& r) {
+        try {
+            if (r.cancelled()) throw RenderCancelled();
+            if (!r.device) {
+                Tile t = Renderer().render_image(*r.node, r.source_bounds, r.request, r.token.get());
+                if (r.cancelled()) throw RenderCancelled();
+                r.host_result.set_value(std::move(t));
+                return;
+            }
+            validate_request(*r.node, r.source_bounds, r.request, r.token.get());
+            cudaStream_t s = thread_stream();
+            DeviceTile d{r.request.viewport, nullptr, r.node->output_descriptor()};
+            const Rect vp = r.request.viewport;
+            const size_t row = (size_t)vp.width * 3;
+            auto block = device_block(row * vp.height * sizeof(float), s);
+            if (dynamic_cast<const DeviceNode*>(r.node.get())) {
+                Executor ex{s, r.token.get()};
+                DevPtr img = ex.eval(*r.node, vp, r.request.level);
+                if (vp.width && vp.height)
+                    check_cuda(cudaMemcpy2DAsync(block.get(), row * sizeof(float), img->data,
+                                                 img->stride * sizeof(float), row * sizeof(float), vp.height,
+                                                 cudaMemcpyDeviceToDevice, s),
+                               "device tile");
+            } else {
+                Tile t = Renderer().render_image(*r.node, r.source_bounds, r.request, r.token.get());
+                if (!t.rgb.empty())
+                    check_cuda(cudaMemcpyAsync(block.get(), t.rgb.data(), t.rgb.size() * sizeof(float),
+                                               cudaMemcpyHostToDevice, s),
+                               "device tile");
+            }
+            check_cuda(cudaStreamSynchronize(s), "device tile");
+            if (r.cancelled()) throw RenderCancelled();
+            d.rgb = block;
+            r.device_result.set_value(std::move(d));
+        } catch (...) {
+            r.fail(std::current_exception());
+        }
+    }
+
+    void render_wave(Lane& lane, const std::vector<RequestPtr>& wave) {
+        // 1. split: cancelled requests fail now; RAW point chains join the batch
+        std::vector<Request*> batched, by_node;
+        std::vector<RawLowering> lowered;
+        lowered.reserve(wave.size());
+        for (const RequestPtr& r : wave) {
+            if (r->cancelled()) {
+                r->fail(std::make_exception_ptr(RenderCancelled()));
+                continue;
+            }
+            RawLowering L;
+            const Rect vp = r->request.viewport;
+            const bool batchable = lane.batch && lane.stream && vp.width && vp.height &&
+                                   dynamic_cast<const DeviceNode*>(r->node.get()) &&
+                                   lower_raw_chain(*r->node, r->request.level, L);
+            if (batchable) {
+                lowered.push_back(L);
+                batched.push_back(r.get());
+            } else {
+                by_node.push_back(r.get());
+            }
+        }
+        // 2. one output block for the batch; requests with equal recipes share a program
+        bool launched = false;
+        std::shared_ptr<float> block;
+        std::vector<size_t> offset(batched.size());
+        std::map<std::string, const re_render_desc*> programs;
+        if (!batched.empty()) {
+            size_t floats = 0;
+            for (size_t i = 0; i < batched.size(); ++i) {
+                offset[i] = floats;
+                const Rect vp = batched[i]->request.viewport;
+                floats += ((size_t)vp.width * vp.height * 3 + 63) & ~(size_t)63;
+            }
+            std::vector<re_batch_item> items(batched.size());
+            try {
+                block = device_block(floats * sizeof(float), lane.stream);
+                for (size_t i = 0; i < batched.size(); ++i) {
+                    const Request& r = *batched[i];
+                    const re_render_desc*& shared = programs[desc_key(lowered[i].desc)];
+                    if (!shared) shared = &lowered[i].desc;
+                    items[i] = re_batch_item{lowered[i].image, shared, to_re(r.request.viewport),
+                                             r.request.level.mip, (uint32_t)r.request.level.quality,
+                                             block.get() + offset[i], (size_t)r.request.viewport.width * 3};
+                }
+                re_batch_options opt{};
+                opt.dispatch = 2;
+                opt.ctas_per_sm = 4;
+                opt.order = 1;
+                opt.use_graph = 0;
+                launched = re_batch_plan(lane.batch, items.data(), items.size(), &opt) == RE_OK &&
+                           re_batch_launch(lane.batch, lane.stream) == RE_OK;
+                if (!launched) note_fallback(std::string("batch plan/launch: ") + re_last_error());
+            } catch (const std::exception& e) {
+                launched = false;
+                note_fallback(std::string("batch outputs: ") + e.what());
+            }
+        }
+        // 3. the other requests render through their nodes while the batch runs
+        //    (statistics are updated before any future of the wave resolves)
+        count(0, by_node.size(), by_node.size());
+        for (Request* r : by_node) render_one(*r);
+        // 4. deliver the batch; if it failed as a whole, each request renders
+        //    alone so that it gets its own error, as a direct render reports it
+        if (launched && re_batch_status(lane.batch, lane.stream) != RE_OK) {
+            launched = false;
+            note_fallback(std::string("batch status: ") + re_last_error());
+        }
+        if (!launched) {
+            count(0, batched.size(), 0);
+            for (Request* r : batched) render_one(*r);
+        } else {
+            count(batched.size(), 0, 0);
+            deliver(lane, batched, block, offset);
+        }
+    }
+
+    void count(size_t batched, size_t node, size_t unbatchable) {
+        std::lock_guard<std::mutex> lock(mu_);
+        stats_.batched_requests += batched;
+        stats_.node_requests += node;
+        stats_.unbatchable_requests += unbatchable;
+    }
+
+    void note_fallback(const std::string& why) {
+        std::lock_guard<std::mutex> lock(mu_);
+        ++stats_.batch_fallbacks;
+        stats_.last_fallback = why;
+    }
+
+    void deliver(Lane& lane, const std::vector<Request*>& batched, const std::shared_ptr<float>& block,
+                 const std::vector<size_t>& offset) {
+        std::vector<Tile> host(batched.size());
+        bool copied = true;
+        for (size_t i = 0; i < batched.size(); ++i) {
+            const Request& r = *batched[i];
+            if (r.device) continue;
+            host[i] = Tile{r.request.viewport,
+                           std::vector<float>((size_t)r.request.viewport.width * r.request.viewport.height * 3),
+                           r.node->output_descriptor()};
+            copied = copied && cudaMemcpyAsync(host[i].rgb.data(), block.get() + offset[i],
+                                               host[i].rgb.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                               lane.stream) == cudaSuccess;
+        }
+        copied = copied && cudaStreamSynchronize(lane.stream) == cudaSuccess;
+        for (size_t i = 0; i < batched.size(); ++i) {
+            Request& r = *batched[i];
+            if (!copied) {
+                r.fail(std::make_exception_ptr(std::runtime_error("scheduler result download failed")));
+            } else if (r.cancelled()) {
+                r.fail(std::make_exception_ptr(RenderCancelled()));
+            } else if (r.device) {
+                // the tile shares the wave's block (aliasing pointer)
+                r.device_result.set_value(DeviceTile{r.request.viewport,
+                                                     std::shared_ptr<const float>(block, block.get() + offset[i]),
+                                                     r.node->output_descriptor()});
+            } else {
+                r.host_result.set_value(std::move(host[i]));
+            }
+        }
+    }
+
+    const size_t budget_;
+    int device_ = 0;
+    mutable std::mutex mu_;
+    std::condition_variable wake_;
+    std::map<Order, RequestPtr> pending_;
+    std::map<std::string, size_t> pending_in_group_;
+    std::vector<RequestPtr> in_flight_;
+    std::vector<Lane> lanes_;
+    uint64_t next_arrival_ = 0;
+    bool closing_ = false;
+    Stats stats_;
 };
 
 TileScheduler::TileScheduler(std::size_t workers, std::size_t max_pending)
     : impl_(std::make_unique<Impl>(workers, max_pending)) {}
 TileScheduler::~TileScheduler() = default;
 
-std::future<Tile> TileScheduler::submit(std::shared_ptr<const Node> output, Rect source_bounds, RenderRequest request,
-                                        RenderPriority priority, std::shared_ptr<CancellationToken> cancellation) {
-    return submit_request({}, std::move(output), source_bounds, request, priority, std::move(cancellation));
-}
-std::future<Tile> TileScheduler::submit(std::shared_ptr<const Node> output, Rect source_bounds, Rect viewport,
-                                        RenderPriority priority, std::uint32_t tile_size,
-                                        std::shared_ptr<CancellationToken> cancellation) {
-    return submit(std::move(output), source_bounds, RenderRequest{viewport, tile_size, {}}, priority,
-                  std::move(cancellation));
-}
-std::future<Tile> TileScheduler::submit_latest(std::string group, std::shared_ptr<const Node> output,
-                                               Rect source_bounds, RenderRequest request, RenderPriority priority,
-                                               std::shared_ptr<CancellationToken> cancellation) {
-    if (group.empty()) throw std::invalid_argument("latest request group is empty");
-    if (!cancellation) cancellation = std::make_shared<CancellationToken>();
-    return submit_request(std::move(group), std::move(output), source_bounds, request, priority,
-                          std::move(cancellation));
-}
-std::future<Tile> TileScheduler::submit_latest(std::string group, std::shared_ptr<const Node> output,
-                                               Rect source_bounds, Rect viewport, RenderPriority priority,
-                                               std::uint32_t tile_size,
-                                               std::shared_ptr<CancellationToken> cancellation) {
-    return submit_latest(std::move(group), std::move(output), source_bounds, RenderRequest{viewport, tile_size, {}},
-                         priority, std::move(cancellation));
-}
+TileScheduler::Stats TileScheduler::stats() const { return impl_->stats(); }
 
-// TileScheduler.cpp:205-236
-std::future<Tile> TileScheduler::submit_request(std::string group, std::shared_ptr<const Node> output,
-                                                Rect source_bounds, RenderRequest request, RenderPriority priority,
-                                                std::shared_ptr<CancellationToken> cancellation) {
+namespace {
+// TileScheduler.cpp:205-236: the argument checks of a scheduled request.
+void validate_scheduled(const std::shared_ptr<const Node>& output, Rect source_bounds, const RenderRequest& request,
+                        RenderPriority priority) {
     const Rect vp = request.viewport;
     const bool native = level_any_native(request.level);
     const bool reduced = level_reduced(request.level);
@@ -1287,15 +1554,67 @@ std::future<Tile> TileScheduler::submit_request(std::string group, std::shared_p
         !source_bounds.width || !source_bounds.height || (int)priority < 0 || (int)priority > 2 ||
         !addressable(source_bounds) || !contains(bounds, vp))
         throw std::invalid_argument("invalid scheduled render request");
-    auto job = std::make_shared<Impl::Job>();
-    job->output = std::move(output);
-    job->source_bounds = source_bounds;
-    job->request = request;
-    job->cancellation = std::move(cancellation);
-    job->group = std::move(group);
-    auto result = job->result.get_future();
-    impl_->enqueue(std::move(job), priority);
-    return result;
+}
+}  // namespace
+
+std::future<Tile> TileScheduler::submit(std::shared_ptr<const Node> output, Rect source_bounds, RenderRequest request,
+                                        RenderPriority priority, std::shared_ptr<CancellationToken> cancellation) {
+    validate_scheduled(output, source_bounds, request, priority);
+    auto r = std::make_shared<Impl::Request>();
+    *r = Impl::Request{std::move(output), source_bounds, request, std::move(cancellation), {}, false, {}, {}};
+    auto f = r->host_result.get_future();
+    impl_->add(std::move(r), priority);
+    return f;
+}
+std::future<Tile> TileScheduler::submit(std::shared_ptr<const Node> output, Rect source_bounds, Rect viewport,
+                                        RenderPriority priority, std::uint32_t tile_size,
+                                        std::shared_ptr<CancellationToken> cancellation) {
+    return submit(std::move(output), source_bounds, RenderRequest{viewport, tile_size, {}}, priority,
+                  std::move(cancellation));
+}
+std::future<Tile> TileScheduler::submit_latest(std::string group, std::shared_ptr<const Node> output,
+                                               Rect source_bounds, RenderRequest request, RenderPriority priority,
+                                               std::shared_ptr<CancellationToken> cancellation) {
+    if (group.empty()) throw std::invalid_argument("latest request group is empty");
+    validate_scheduled(output, source_bounds, request, priority);
+    if (!cancellation) cancellation = std::make_shared<CancellationToken>();
+    auto r = std::make_shared<Impl::Request>();
+    *r = Impl::Request{std::move(output), source_bounds, request, std::move(cancellation), std::move(group), false,
+                       {}, {}};
+    auto f = r->host_result.get_future();
+    impl_->add(std::move(r), priority);
+    return f;
+}
+std::future<Tile> TileScheduler::submit_latest(std::string group, std::shared_ptr<const Node> output,
+                                               Rect source_bounds, Rect viewport, RenderPriority priority,
+                                               std::uint32_t tile_size,
+                                               std::shared_ptr<CancellationToken> cancellation) {
+    return submit_latest(std::move(group), std::move(output), source_bounds, RenderRequest{viewport, tile_size, {}},
+                         priority, std::move(cancellation));
+}
+std::future<DeviceTile> TileScheduler::submit_device(std::shared_ptr<const Node> output, Rect source_bounds,
+                                                     RenderRequest request, RenderPriority priority,
+                                                     std::shared_ptr<CancellationToken> cancellation) {
+    validate_scheduled(output, source_bounds, request, priority);
+    auto r = std::make_shared<Impl::Request>();
+    *r = Impl::Request{std::move(output), source_bounds, request, std::move(cancellation), {}, true, {}, {}};
+    auto f = r->device_result.get_future();
+    impl_->add(std::move(r), priority);
+    return f;
+}
+std::future<DeviceTile> TileScheduler::submit_latest_device(std::string group, std::shared_ptr<const Node> output,
+                                                            Rect source_bounds, RenderRequest request,
+                                                            RenderPriority priority,
+                                                            std::shared_ptr<CancellationToken> cancellation) {
+    if (group.empty()) throw std::invalid_argument("latest request group is empty");
+    validate_scheduled(output, source_bounds, request, priority);
+    if (!cancellation) cancellation = std::make_shared<CancellationToken>();
+    auto r = std::make_shared<Impl::Request>();
+    *r = Impl::Request{std::move(output), source_bounds, request, std::move(cancellation), std::move(group), true,
+                       {}, {}};
+    auto f = r->device_result.get_future();
+    impl_->add(std::move(r), priority);
+    return f;
 }
 
 }  // namespace rawengine

@@ -753,6 +753,12 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
         // the near-tie sites, re-decided by the reference's binary64 classifier
         const unsigned n = S.rechecks;
         if (n) {
+            // Rechecks are also made for halo sites that a neighbouring tile
+            // renders; only the sites of this tile's own output are counted, so
+            // every output site is counted once per render.
+            const int cx0 = max(x0, ox), cx1 = min(x0 + MN_TW, ox + ow);
+            const int cy0 = max(y0, oy), cy1 = min(y0 + MN_TH, oy + oh);
+            unsigned own = 0;
             for (unsigned e = t; e < n; e += MN_THREADS) {
                 const int code = S.recheck[e];
                 const int k = code >> 1, site = code & 1;
@@ -762,8 +768,10 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
                 const bool hz = site ? exact_horizontal_q<BX, 1>(S.raw, rq) : exact_horizontal_q<AX, 0>(S.raw, rq);
                 S.horiz[site][k] = hz;
                 S.green[site][k] = hz ? S.ng[site ? GH_B : GH_A][q] : S.ng[site ? GV_B : GV_A][q];
+                const int px = x0 + 2 * qx - 2 + (site ? BX : AX), py = y0 + 2 * qy - 2 + site;
+                own += px >= cx0 && px < cx1 && py >= cy0 && py < cy1;
             }
-            if (ties && t == 0) atomicAdd(ties, (unsigned long long)n);
+            if (ties && own) atomicAdd(ties, (unsigned long long)own);
             __syncthreads();
         }
     }

@@ -205,3 +205,23 @@ def mixed_pipeline(image: MixedImage, recipe: MixedRecipe):
         p.working_to_srgb()
         p.srgb_encode()
     return p
+
+
+def write_scheduler_spec(path: str, images, recipes, tiles) -> None:
+    """The mixed batch as the text spec read by the C++ scheduler driver
+    (tests/cpp/scheduler_driver.cpp): image, recipe and tile lines.  A recipe
+    without a tone curve (the extended-curve recipes) gets the default tone
+    shoulder 0.25 and gamma 1 in the C++ chain."""
+    with open(path, "w") as f:
+        for im in images:
+            f.write("image %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d\n" % (
+                im.width, im.height, im.stride, im.pattern, im.phase[0], im.phase[1], *im.active, *im.black,
+                im.white, im.demosaic, im.seed))
+        for r in recipes:
+            shoulder, gamma = r.tone if r.tone is not None else (0.25, 1.0)
+            knots = r.curve or []
+            f.write("recipe %r %r %r %r %s %r %r %d %s\n" % (
+                r.wb[0], r.wb[1], r.wb[2], r.stops, " ".join(repr(float(v)) for v in np.asarray(r.camera_to_xyz).reshape(9)),
+                shoulder, gamma, len(knots), " ".join("%r %r" % (x, y) for x, y in knots)))
+        for t in tiles:
+            f.write("tile %d %d %d %d %d %d %d %d\n" % (t.image, t.recipe, *t.viewport, t.mip, t.quality))

@@ -457,6 +457,11 @@ class Reference:
                                                f64p, u32p, C.c_uint32, C.c_uint32, u32p]
         L.refshim_raster_input_region.argtypes = [C.c_uint32, C.c_uint32, C.c_int, i32p, C.c_int, f64p,
                                                   u32p, C.c_uint32, C.c_uint32, u32p]
+        L.refshim_session_create.restype = C.c_void_p
+        L.refshim_session_create.argtypes = [u32p, u16p, u16p, C.c_size_t, C.c_int, i32p, C.c_int, f64p,
+                                             C.c_uint32]
+        L.refshim_session_render.argtypes = [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, f32p]
+        L.refshim_session_destroy.argtypes = [C.c_void_p]
         L.refshim_local_statistics.argtypes = [f32p, u32p, u32p, u32p, C.c_uint32, C.c_int, f64p, f64p,
                                                u32p]
         L.refshim_guided_filter.argtypes = [f32p, u32p, u32p, u32p, C.c_uint32, C.c_double, C.c_int,
@@ -485,6 +490,11 @@ class Reference:
         else:
             self._check(self.lib.refshim_render_raw(*args, None))
         return out
+
+    def session(self, raw: RawSpec, menon: bool, ops, workers: int) -> "RefSession":
+        """A reference render session (RawImage, node chain and TileScheduler
+        built once); its render() only submits the tiles and waits."""
+        return RefSession(self, raw, menon, ops, workers)
 
     def raw_bounds(self, raw: RawSpec, menon: bool, ops):
         codes, params = flatten_ops(ops)
@@ -551,6 +561,37 @@ class Reference:
             _ptr(tile, C.c_float), _ptr(self._u32(needed), C.c_uint32), _ptr(o, C.c_uint32),
             _ptr(self._u32(image), C.c_uint32), radius, eps, space, _ptr(out, C.c_float)))
         return out
+
+
+class RefSession:
+    """refshim_session_*: setup outside the timed calls."""
+
+    def __init__(self, ref: Reference, raw: RawSpec, menon: bool, ops, workers: int):
+        codes, params = flatten_ops(ops)
+        self.ref = ref
+        self.samples = np.ascontiguousarray(raw.samples, dtype=np.uint16)
+        self.handle = ref.lib.refshim_session_create(
+            _ptr(raw.meta_words(), C.c_uint32), _ptr(raw.level_words(), C.c_uint16),
+            _ptr(self.samples, C.c_uint16), self.samples.size, int(menon), _ptr(codes, C.c_int32), len(ops),
+            _ptr(params, C.c_double), workers)
+        if not self.handle:
+            raise OracleError(10, ref.lib.refshim_last_error().decode())
+
+    def render(self, viewport, tile=256, mip=0, quality=1, out=None):
+        vp = Reference._u32(viewport)
+        if out is None:
+            out = np.zeros((int(vp[3]), int(vp[2]), 3), np.float32)
+        self.ref._check(self.ref.lib.refshim_session_render(self.handle, _ptr(vp, C.c_uint32), tile, mip, quality,
+                                                            _ptr(out, C.c_float)))
+        return out
+
+    def close(self):
+        if self.handle:
+            self.ref.lib.refshim_session_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
 
 
 def reference_available() -> bool:

@@ -337,3 +337,66 @@ int refshim_guided_filter(const float* rgb, const std::uint32_t* needed,
 }
 
 } // extern "C"
+
+namespace {
+
+// A reference render session for timing: the RawImage, the node chain and a
+// TileScheduler with `workers` threads are built once by
+// refshim_session_create; refshim_session_render then only submits one
+// TileScheduler request per render tile of the viewport (the reference
+// renderer's row-major cut, RawEngine.cpp:1399-1411), waits for them and
+// copies each tile into `out` -- the work a caller of the reference repeats
+// per frame.
+struct RefSession {
+    std::shared_ptr<const Node> node;
+    Rect bounds;
+    std::unique_ptr<TileScheduler> scheduler;
+};
+
+} // namespace
+
+extern "C" {
+
+
+void* refshim_session_create(const std::uint32_t* meta, const std::uint16_t* levels,
+                             const std::uint16_t* samples, std::size_t count, int demosaic,
+                             const std::int32_t* ops, int nops, const double* params,
+                             std::uint32_t workers) {
+    RefSession* out = nullptr;
+    const int st = guarded([&] {
+        auto s = std::make_unique<RefSession>();
+        s->node = build_chain(raw_source(meta, levels, samples, count, demosaic, s->bounds), s->bounds, ops,
+                              nops, params);
+        s->scheduler = std::make_unique<TileScheduler>(workers, 1u << 20);
+        out = s.release();
+    });
+    return st ? nullptr : out;
+}
+
+int refshim_session_render(void* session, const std::uint32_t* viewport, std::uint32_t tile_size,
+                           std::uint32_t mip, std::uint32_t quality, float* out) {
+    return guarded([&] {
+        auto* s = static_cast<RefSession*>(session);
+        const Rect vp{viewport[0], viewport[1], viewport[2], viewport[3]};
+        std::vector<std::future<Tile>> futures;
+        for (std::uint64_t y = vp.y; y < std::uint64_t(vp.y) + vp.height; y += tile_size)
+            for (std::uint64_t x = vp.x; x < std::uint64_t(vp.x) + vp.width; x += tile_size) {
+                const Rect r{std::uint32_t(x), std::uint32_t(y),
+                             std::uint32_t(std::min<std::uint64_t>(tile_size, vp.x + std::uint64_t(vp.width) - x)),
+                             std::uint32_t(std::min<std::uint64_t>(tile_size, vp.y + std::uint64_t(vp.height) - y))};
+                futures.push_back(s->scheduler->submit(
+                    s->node, s->bounds, RenderRequest{r, tile_size, {mip, static_cast<RenderQuality>(quality)}}));
+            }
+        for (auto& f : futures) {
+            const auto t = f.get();
+            for (std::uint32_t row = 0; row < t.bounds.height; ++row)
+                std::memcpy(out + ((std::size_t(t.bounds.y - vp.y + row) * vp.width) + (t.bounds.x - vp.x)) * 3,
+                            t.rgb.data() + std::size_t(row) * t.bounds.width * 3,
+                            std::size_t(t.bounds.width) * 3 * sizeof(float));
+        }
+    });
+}
+
+void refshim_session_destroy(void* session) { delete static_cast<RefSession*>(session); }
+
+} // extern "C"

@@ -105,6 +105,13 @@ public:
         for (size_t i = 0; i < t.rgb.size(); i += 3) std::copy(px_.begin(), px_.end(), t.rgb.begin() + i);
         return t;
     }
+    // The reference's identity hooks, overridden as a reference user would.
+    std::optional<IccProfileIdentity> input_icc_identity() const override { return std::nullopt; }
+    std::optional<std::array<std::uint8_t, 32>> source_fingerprint() const override {
+        std::array<std::uint8_t, 32> f{};
+        f[0] = 0x5a;
+        return f;
+    }
 private:
     std::array<float, 3> px_;
 };
@@ -342,6 +349,10 @@ int run_render(const std::string& dir) {
         for (size_t i = 0; ok && i < t.rgb.size(); i += 3)
             ok = t.rgb[i] == 0.25f * 2.0f && t.rgb[i + 1] == 0.5f && t.rgb[i + 2] == 0.75f * 0.5f;
         check(ok, "foreign_node_uploaded");
+        const Node& base = *c;
+        check(!base.input_icc_identity() && base.source_fingerprint() && (*base.source_fingerprint())[0] == 0x5a &&
+                  !WhiteBalanceNode(c, 1.0f, 1.0f, 1.0f).source_fingerprint(),
+              "node_identity_hooks");
         auto w = std::make_shared<WhiteBalanceNode>(std::make_shared<WrongDescriptorNode>(), 1.0f, 1.0f, 1.0f);
         expect_throw<std::domain_error>([&] { w->render({0, 0, 2, 2}); }, "foreign_wrong_descriptor_domain_error");
     }

@@ -1,6 +1,7 @@
 """Regenerates the committed golden fixtures under tests/golden/ (run in a
-checkout that has the reference at REF, default /root/reference, and the
-reference library built by `make -C oracle ref`).
+checkout that has the reference at $REF -- by default a directory named
+"reference" beside this checkout -- and the reference library built by
+`make -C oracle ref`).
 
 * menon_native_base_v1.npz -- the reference's own frozen Menon vectors
   (tests/reference/raw/menon_native_base_v1.bin, format documented in its
@@ -30,7 +31,7 @@ from oracle.oracle import (OP_CAMERA_TO_WORKING, OP_CUBIC_RESIZE, OP_CURVES_EXT,
                            curves_params)
 from librawops_b200 import synthetic, workloads  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def menon_fixtures():

@@ -21,8 +21,9 @@ pytestmark = pytest.mark.gpu
 
 def _noalloc(img, pipe, viewport, mip, out):
     d = pipe.desc()
+    ptr, stride = (None, 0) if out is None else (C.c_void_p(out.data_ptr()), out.stride(0))
     _capi.check(_capi.lib().re_render_raw_reduced_noalloc(
-        img.handle, C.byref(d), _capi.Rect(*viewport), mip, C.c_void_p(out.data_ptr()), out.stride(0), None))
+        img.handle, C.byref(d), _capi.Rect(*viewport), mip, ptr, stride, None))
 
 
 def test_noalloc_reduced_render_matches_allocating_render():
@@ -50,3 +51,5 @@ def test_noalloc_reduced_render_matches_allocating_render():
     with pytest.raises(_capi.ReError) as e:
         _noalloc(big, pipe, (0, 0, 1200, 800), 1, out)
     assert e.value.kind == "length_error" and "exceeds" in str(e.value)
+    # an empty viewport renders nothing and, like re_render_raw, needs no output buffer
+    _noalloc(img, pipe, (0, 0, 0, 0), 1, None)
