@@ -197,6 +197,9 @@ public:
         std::uint64_t unbatchable_requests = 0;  // node requests whose chain is not a RAW point chain
         std::uint64_t batch_fallbacks = 0;  // waves whose batched render failed and were re-rendered per request
         std::string last_fallback;          // the error text of the last such failure
+        // host seconds spent by the lanes: lowering chains to batch items,
+        // planning the batches, waiting for the batched renders, delivering tiles
+        double lower_s = 0, plan_s = 0, device_s = 0, deliver_s = 0;
     };
     Stats stats() const;
 private:

@@ -387,15 +387,28 @@ RE_API re_status re_render_raster(const float* in, size_t in_row_stride, uint32_
  * `in` is a device image of width*height RGB pixels (row stride in floats),
  * `out` a device buffer of the same shape.  working_space selects the Y weights
  * (0 ProPhoto, 1 Rec2020, SpatialOps.cpp:191-192).  Radius 0..64, epsilon in
- * [2^-24, 65536].  Windows clip at the image edge with actual counts. */
+ * [2^-24, 65536].  Windows clip at the image edge with actual counts.  `out`
+ * must not overlap `in`.  Returns after the filter completed on `stream`. */
 RE_API re_status re_guided_filter(const float* in, size_t in_row_stride, float* out,
                                   size_t out_row_stride, uint32_t width, uint32_t height,
                                   uint32_t radius, double epsilon, uint32_t working_space,
                                   void* stream);
+/* The same filter, enqueued on `stream` without a host synchronization:
+ * non-finite input and float32 overflow are OR-ed into *device_status (a
+ * device word the caller zeroes and maps with re_status_from_device), and
+ * `scratch` is device memory of re_guided_filter_scratch_bytes(width, height,
+ * radius) bytes (the kernel's per-CTA rings of row sums).  `out` must not
+ * overlap `in`. */
+RE_API re_status re_guided_filter_async(const float* in, size_t in_row_stride, float* out,
+                                        size_t out_row_stride, uint32_t width, uint32_t height,
+                                        uint32_t radius, double epsilon, uint32_t working_space,
+                                        uint32_t* device_status, void* scratch, void* stream);
+RE_API size_t re_guided_filter_scratch_bytes(uint32_t width, uint32_t height, uint32_t radius);
 /* local_statistics_rgb (SpatialOps.cpp:79-121) over a whole image: per channel
  * box mean and population variance over the clipped (2r+1)^2 window, excluding
  * non-finite samples (count_out gets the finite count; mean/variance NaN when
- * it is 0).  Outputs are float32 interleaved RGB; count_out may be NULL. */
+ * it is 0).  Outputs are float32 interleaved RGB; count_out may be NULL.
+ * Enqueued on `stream`; returns without waiting for it. */
 RE_API re_status re_local_statistics(const float* in, size_t in_row_stride, uint32_t width,
                                      uint32_t height, uint32_t radius, float* mean_out,
                                      float* variance_out, uint32_t* count_out, void* stream);

@@ -160,7 +160,8 @@ re_status enqueue(re_batch* b, cudaStream_t stream) {
 
 // Requests of one image, description, level and output row stride whose
 // viewports tile a rectangle and whose outputs sit where one render of that
-// rectangle would write them merge into that one render (results do not depend
+// rectangle would write them (the merged rows fit in the row stride) merge
+// into that one render (results do not depend
 // on how a viewport is cut, so the pixels are the same): first along rows,
 // then along columns.
 std::vector<re_batch_item> merge_items(std::vector<re_batch_item> v) {
@@ -189,7 +190,8 @@ std::vector<re_batch_item> merge_items(std::vector<re_batch_item> v) {
                     same(a, it) &&
                     (rows ? (a.viewport.y == it.viewport.y && a.viewport.height == it.viewport.height &&
                              (uint64_t)a.viewport.x + a.viewport.width == it.viewport.x &&
-                             it.out == a.out + (size_t)a.viewport.width * 3)
+                             it.out == a.out + (size_t)a.viewport.width * 3 &&
+                             ((size_t)a.viewport.width + it.viewport.width) * 3 <= a.out_row_stride)
                           : (a.viewport.x == it.viewport.x && a.viewport.width == it.viewport.width &&
                              (uint64_t)a.viewport.y + a.viewport.height == it.viewport.y &&
                              it.out == a.out + (size_t)a.viewport.height * a.out_row_stride));

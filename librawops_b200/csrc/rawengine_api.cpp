@@ -18,6 +18,7 @@
 // renders a whole viewport in one pass while render_tiles keeps the
 // reference's per-tile loop and callback order.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
@@ -1242,6 +1243,8 @@ struct TileScheduler::Impl {
     struct Lane {
         cudaStream_t stream = nullptr;   // batched renders and their copies
         re_batch* batch = nullptr;
+        float* staging = nullptr;        // pinned host copy of a wave's host tiles
+        size_t staging_floats = 0;
         std::thread thread;
     };
 
@@ -1249,6 +1252,7 @@ struct TileScheduler::Impl {
         if (!lanes || lanes > 64 || !budget)
             throw std::invalid_argument("scheduler needs 1-64 workers and a pending budget");
         if (cudaGetDevice(&device_) != cudaSuccess) device_ = 0;   // lanes then report the error per request
+        copy_threads_ = std::max<size_t>(1, std::min<size_t>(8, std::thread::hardware_concurrency() / lanes));
         lanes_.resize(lanes);
         try {
             for (Lane& lane : lanes_) lane.thread = std::thread([this, &lane] { run_lane(lane); });
@@ -1354,6 +1358,7 @@ private:
             retire(wave);
         }
         if (lane.batch) re_batch_destroy(lane.batch);
+        if (lane.staging) cudaFreeHost(lane.staging);
         if (lane.stream) cudaStreamDestroy(lane.stream);
     }
 
@@ -1398,7 +1403,15 @@ private:
         }
     }
 
+    void add_time(double Stats::*field, std::chrono::steady_clock::time_point& since) {
+        const auto now = std::chrono::steady_clock::now();
+        std::lock_guard<std::mutex> lock(mu_);
+        stats_.*field += std::chrono::duration<double>(now - since).count();
+        since = now;
+    }
+
     void render_wave(Lane& lane, const std::vector<RequestPtr>& wave) {
+        auto mark = std::chrono::steady_clock::now();
         // 1. split: cancelled requests fail now; RAW point chains join the batch
         std::vector<Request*> batched, by_node;
         std::vector<RawLowering> lowered;
@@ -1420,6 +1433,7 @@ private:
                 by_node.push_back(r.get());
             }
         }
+        add_time(&Stats::lower_s, mark);
         // 2. one output block for the batch; requests with equal recipes share a program
         bool launched = false;
         std::shared_ptr<float> block;
@@ -1456,6 +1470,7 @@ private:
                 note_fallback(std::string("batch outputs: ") + e.what());
             }
         }
+        add_time(&Stats::plan_s, mark);
         // 3. the other requests render through their nodes while the batch runs
         //    (statistics are updated before any future of the wave resolves)
         count(0, by_node.size(), by_node.size());
@@ -1466,6 +1481,7 @@ private:
             launched = false;
             note_fallback(std::string("batch status: ") + re_last_error());
         }
+        add_time(&Stats::device_s, mark);
         if (!launched) {
             count(0, batched.size(), 0);
             for (Request* r : batched) render_one(*r);
@@ -1473,6 +1489,7 @@ private:
             count(batched.size(), 0, 0);
             deliver(lane, batched, block, offset);
         }
+        add_time(&Stats::deliver_s, mark);
     }
 
     void count(size_t batched, size_t node, size_t unbatchable) {
@@ -1490,19 +1507,51 @@ private:
 
     void deliver(Lane& lane, const std::vector<Request*>& batched, const std::shared_ptr<float>& block,
                  const std::vector<size_t>& offset) {
+        // Host tiles: one copy of the wave's output block into the lane's
+        // pinned staging buffer, then every tile's vector is constructed from
+        // its slice (no zero fill; each page is touched once), spread over a
+        // few host threads when the wave is large.
         std::vector<Tile> host(batched.size());
+        std::vector<size_t> wanted;
+        size_t end = 0;
+        for (size_t i = 0; i < batched.size(); ++i)
+            if (!batched[i]->device) {
+                wanted.push_back(i);
+                const Rect vp = batched[i]->request.viewport;
+                end = std::max(end, offset[i] + (size_t)vp.width * vp.height * 3);
+            }
         bool copied = true;
-        for (size_t i = 0; i < batched.size(); ++i) {
-            const Request& r = *batched[i];
-            if (r.device) continue;
-            host[i] = Tile{r.request.viewport,
-                           std::vector<float>((size_t)r.request.viewport.width * r.request.viewport.height * 3),
-                           r.node->output_descriptor()};
-            copied = copied && cudaMemcpyAsync(host[i].rgb.data(), block.get() + offset[i],
-                                               host[i].rgb.size() * sizeof(float), cudaMemcpyDeviceToHost,
-                                               lane.stream) == cudaSuccess;
+        if (!wanted.empty()) {
+            if (lane.staging_floats < end) {
+                if (lane.staging) cudaFreeHost(lane.staging);
+                lane.staging = nullptr;
+                lane.staging_floats = 0;
+                copied = cudaHostAlloc((void**)&lane.staging, end * sizeof(float), cudaHostAllocDefault) ==
+                         cudaSuccess;
+                if (copied) lane.staging_floats = end;
+            }
+            copied = copied && cudaMemcpyAsync(lane.staging, block.get(), end * sizeof(float),
+                                               cudaMemcpyDeviceToHost, lane.stream) == cudaSuccess &&
+                     cudaStreamSynchronize(lane.stream) == cudaSuccess;
         }
-        copied = copied && cudaStreamSynchronize(lane.stream) == cudaSuccess;
+        if (copied && !wanted.empty()) {
+            auto build = [&](size_t from, size_t to) {
+                for (size_t k = from; k < to; ++k) {
+                    const size_t i = wanted[k];
+                    const Request& r = *batched[i];
+                    const float* src = lane.staging + offset[i];
+                    const size_t n = (size_t)r.request.viewport.width * r.request.viewport.height * 3;
+                    host[i] = Tile{r.request.viewport, std::vector<float>(src, src + n), r.node->output_descriptor()};
+                }
+            };
+            const size_t parts = end * sizeof(float) < (size_t(32) << 20) ? 1 : copy_threads_;
+            std::vector<std::thread> helpers;
+            const size_t per = (wanted.size() + parts - 1) / parts;
+            for (size_t p = 1; p < parts && p * per < wanted.size(); ++p)
+                helpers.emplace_back(build, p * per, std::min(wanted.size(), (p + 1) * per));
+            build(0, std::min(wanted.size(), per));
+            for (auto& h : helpers) h.join();
+        }
         for (size_t i = 0; i < batched.size(); ++i) {
             Request& r = *batched[i];
             if (!copied) {
@@ -1521,6 +1570,7 @@ private:
     }
 
     const size_t budget_;
+    size_t copy_threads_ = 1;
     int device_ = 0;
     mutable std::mutex mu_;
     std::condition_variable wake_;

@@ -1,5 +1,5 @@
-// Spatial stages: the working-Y guided filter (SpatialOps.cpp:159-317) and
-// box local statistics (SpatialOps.cpp:52-157).
+// Spatial stages: the working-Y guided filter (SpatialOps.cpp:159-317) and box
+// local statistics (SpatialOps.cpp:52-157), each ONE streaming kernel.
 //
 // Guided filter.  The reference evaluates, per coefficient centre k, centred
 // moments over its clipped (2r+1)^2 window and then, per output pixel x,
@@ -7,21 +7,45 @@
 // in binary64 (O(r^2) per pixel).  Expanding the sum gives the classical form
 //     q(x) = mean_{k in W(x)} a(k) * Y(x) + mean_{k in W(x)} b(k),
 //     a(k) = cov(Y, p)/(var(Y) + eps),  b(k) = mean(p) - a(k) mean(Y),
-// with clipped windows and actual counts, which box filters evaluate in O(1)
-// per pixel independent of r.  The first box filter accumulates the eight
-// moments (Y, R, G, B, Y^2, YR, YG, YB) in binary64 (so E[Y^2]-E[Y]^2 keeps
-// ~1e-16 relative precision against eps >= 2^-24); a and b stay binary64 through
-// the second box filter, since a*Y and b can cancel when eps is small.  Output equals p(x) exactly when
-// the correction is zero (constants, signed zeros), as in SpatialOps.cpp:278.
+// with clipped windows and actual counts, which box sums evaluate in O(1) per
+// pixel independent of r.  Y is a fixed linear combination of R, G and B, so
+// the box sums of Y and Y^2 follow from those of R, G, B, YR, YG and YB: six
+// binary64 moments per pixel.  a and b stay binary64 through the second box
+// sum, since a*Y and b can cancel when eps is small.  Output equals p(x)
+// exactly when the correction is zero (constants, signed zeros), as in
+// SpatialOps.cpp:278.
 //
 // Local statistics.  Per channel, the finite count, mean and population
-// variance over the clipped window.  Each CTA shifts its samples by one of its
-// own values before summing (x - s, (x - s)^2 in binary64), so windows far
+// variance over the clipped window.  Each task shifts its samples by one of
+// its own values before summing (x - s, (x - s)^2 in binary64), so windows far
 // from zero (the reference's 1e20 offset test) keep their precision; the
 // reference's Welford/merge order is not reproduced, the result agrees within
 // float32 rounding of the outputs.
+//
+// Both kernels stream vertical STRIPS of the image from top to bottom.  A task
+// is one strip (the CTA's NT columns of input: TW output columns plus the
+// halo) over one band of output rows; tasks are taken band-major by a
+// persistent grid, so CTAs that run together share their strips' halo
+// columns in L2.  Per block of R rows:
+//   A  column owners (one thread per input column) keep the vertical window
+//      sums of the moments in registers, adding the entering row and
+//      subtracting the leaving one (re-read from the input, an L2 hit, instead
+//      of stored), and write the R rows of sums to shared memory;
+//   B  row segments (one thread per K consecutive centres of one row) slide
+//      the horizontal window over those sums -- two reads per centre and
+//      moment after the first window -- giving each centre's box sums;
+// and for the guided filter, additionally
+//   C  row segments slide the horizontal window over the centres' a and b;
+//   D  column owners keep the vertical window sums of C's rows in registers
+//      (the leaving row from a ring of 2r+1 rows per CTA in global memory,
+//      which stays in L2) and write the output rows.
+// Intermediates never reach HBM: DRAM traffic is the input (plus the strips'
+// halo columns where L2 misses them) and the output.  Shared-memory planes
+// are moment-major and skewed by one element every K, so the K-strided reads
+// of a warp's row segments are conflict-free.
 #include <cfloat>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include "re_device.cuh"
@@ -34,8 +58,6 @@ using namespace re;
 
 namespace {
 
-constexpr int GF_CHUNK = 32;  // pixels per thread along the sliding direction
-
 // Working-Y weights of SpatialOps.cpp:191-192.
 struct YWeights {
     double wr, wb;
@@ -45,259 +67,427 @@ __device__ __forceinline__ double working_y(double r, double g, double b, const 
     return __dadd_rn(__dadd_rn(g, __dmul_rn(w.wr, __dsub_rn(r, g))), __dmul_rn(w.wb, __dsub_rn(b, g)));
 }
 
-__device__ __forceinline__ void moments(const float* p, const YWeights& w, double m[8]) {
-    const double r = p[0], g = p[1], b = p[2];
-    const double y = working_y(r, g, b, w);
-    m[0] = y; m[1] = r; m[2] = g; m[3] = b;
-    m[4] = y * y; m[5] = y * r; m[6] = y * g; m[7] = y * b;
+// Skewed index of element j in a plane whose segments are K long.
+template <int K>
+__device__ __forceinline__ int sk(int j) {
+    return j + j / K;
 }
 
-// Horizontal box sums of the eight moments: one thread slides along GF_CHUNK
-// pixels of a row.  H: (height, width, 8) doubles.
-__global__ void gf_hbox_moments(const float* __restrict__ in, size_t in_stride, int width, int height, int r,
-                                YWeights w, double* __restrict__ H, uint32_t* status) {
-    const int row = blockIdx.y;
-    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * GF_CHUNK;
-    if (x0 >= width || row >= height) return;
-    const float* src = in + (size_t)row * in_stride;
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0}, m[8];
-    bool bad = false;
-    const int lo0 = max(0, x0 - r), hi0 = min(width - 1, x0 + r);
-    for (int j = lo0; j <= hi0; ++j) {
-        const float* p = src + (size_t)j * 3;
-        bad |= !(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]));
-        moments(p, w, m);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) s[q] += m[q];
-    }
-    const int x1 = min(width, x0 + GF_CHUNK);
-    for (int x = x0; x < x1; ++x) {
-        if (x > x0) {
-            const int enter = x + r, leave = x - r - 1;
-            if (enter < width) {
-                const float* p = src + (size_t)enter * 3;
-                bad |= !(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]));
-                moments(p, w, m);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s[q] += m[q];
-            }
-            if (leave >= 0) {
-                moments(src + (size_t)leave * 3, w, m);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s[q] -= m[q];
-            }
-        }
-        double* h = H + ((size_t)row * width + x) * 8;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) h[q] = s[q];
-    }
-    if (bad && status) atomicMax(status, (uint32_t)((401u << 8) | ST_INVALID));
+template <int K>
+__host__ __device__ constexpr int plane_len(int n) {
+    return n + n / K + 1;
 }
 
-// Vertical box sums of H, then the per-centre regression a, b (float AB: 6 per px).
-__global__ void gf_vbox_coefficients(const double* __restrict__ H, int width, int height, int r, double eps,
-                                     double* __restrict__ AB, uint32_t* status) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = blockIdx.y * GF_CHUNK;
-    if (x >= width || y0 >= height) return;
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int lo0 = max(0, y0 - r), hi0 = min(height - 1, y0 + r);
-    for (int j = lo0; j <= hi0; ++j) {
-        const double* h = H + ((size_t)j * width + x) * 8;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) s[q] += h[q];
-    }
-    const int wx = min(width - 1, x + r) - max(0, x - r) + 1;
-    const int y1 = min(height, y0 + GF_CHUNK);
-    bool overflow = false;
-    for (int y = y0; y < y1; ++y) {
-        if (y > y0) {
-            const int enter = y + r, leave = y - r - 1;
-            if (enter < height) {
-                const double* h = H + ((size_t)enter * width + x) * 8;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s[q] += h[q];
-            }
-            if (leave >= 0) {
-                const double* h = H + ((size_t)leave * width + x) * 8;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s[q] -= h[q];
-            }
-        }
-        const int wy = min(height - 1, y + r) - max(0, y - r) + 1;
-        const double n = (double)wx * (double)wy;
-        const double my = s[0] / n;
-        double var = s[4] / n - my * my;
-        if (var < 0) var = 0;
-        const double inv = 1.0 / (var + eps);
-        double* ab = AB + ((size_t)y * width + x) * 6;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const double mp = s[1 + c] / n;
-            const double cov = s[5 + c] / n - my * mp;
-            const double a = cov * inv;
-            const double b = mp - a * my;
-            overflow |= !(isfinite(a) && isfinite(b));
-            ab[c] = a;
-            ab[3 + c] = b;
-        }
-    }
-    if (overflow && status) atomicMax(status, (uint32_t)((400u << 8) | ST_OVERFLOW));
+// Clipped window extent along one axis of length len.
+__device__ __forceinline__ int extent(int c, int r, int len) {
+    return min(len - 1, c + r) - max(0, c - r) + 1;
 }
 
-// Horizontal box sums of AB.
-__global__ void gf_hbox_ab(const double* __restrict__ AB, int width, int height, int r, double* __restrict__ H2) {
-    const int row = blockIdx.y;
-    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * GF_CHUNK;
-    if (x0 >= width || row >= height) return;
-    const double* src = AB + (size_t)row * width * 6;
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int j = max(0, x0 - r); j <= min(width - 1, x0 + r); ++j)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) s[q] += src[(size_t)j * 6 + q];
-    const int x1 = min(width, x0 + GF_CHUNK);
-    for (int x = x0; x < x1; ++x) {
-        if (x > x0) {
-            const int enter = x + r, leave = x - r - 1;
-            if (enter < width)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) s[q] += src[(size_t)enter * 6 + q];
-            if (leave >= 0)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) s[q] -= src[(size_t)leave * 6 + q];
-        }
-        double* h = H2 + ((size_t)row * width + x) * 6;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) h[q] = s[q];
-    }
-}
-
-// Vertical box sums of H2 and the output q = mean(a) Y + mean(b).
-__global__ void gf_vbox_output(const double* __restrict__ H2, const float* __restrict__ in, size_t in_stride,
-                               int width, int height, int r, YWeights w, float* __restrict__ out,
-                               size_t out_stride, uint32_t* status) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = blockIdx.y * GF_CHUNK;
-    if (x >= width || y0 >= height) return;
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int j = max(0, y0 - r); j <= min(height - 1, y0 + r); ++j)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) s[q] += H2[((size_t)j * width + x) * 6 + q];
-    const int wx = min(width - 1, x + r) - max(0, x - r) + 1;
-    const int y1 = min(height, y0 + GF_CHUNK);
-    bool overflow = false;
-    for (int y = y0; y < y1; ++y) {
-        if (y > y0) {
-            const int enter = y + r, leave = y - r - 1;
-            if (enter < height)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) s[q] += H2[((size_t)enter * width + x) * 6 + q];
-            if (leave >= 0)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) s[q] -= H2[((size_t)leave * width + x) * 6 + q];
-        }
-        const int wy = min(height - 1, y + r) - max(0, y - r) + 1;
-        const double n = (double)wx * (double)wy;
-        const float* p = in + (size_t)y * in_stride + (size_t)x * 3;
-        const double Y = working_y(p[0], p[1], p[2], w);
-        float* o = out + (size_t)y * out_stride + (size_t)x * 3;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const double q = (s[c] / n) * Y + s[3 + c] / n;
-            const double delta = q - (double)p[c];
-            if (delta == 0) {
-                o[c] = p[c];
-                continue;
-            }
-            if (!isfinite(q) || fabs(q) > (double)FLT_MAX) overflow = true;
-            o[c] = (float)q;
-        }
-    }
-    if (overflow && status) atomicMax(status, (uint32_t)((400u << 8) | ST_OVERFLOW));
-}
-
-// ----------------------------------------------------------- local statistics
-
-constexpr int LS_TW = 32, LS_TH = 16, LS_THREADS = 256, LS_MAX_R = 32;
-
-struct LsSmem {
-    double s1[LS_TH + 2 * LS_MAX_R][LS_TW];
-    double s2[LS_TH + 2 * LS_MAX_R][LS_TW];
-    int n[LS_TH + 2 * LS_MAX_R][LS_TW];
+struct StripTask {
+    int x0, y0, y1;   // first output column; output rows [y0, y1)
 };
 
-// T = float (re_local_statistics) or double (re_local_statistics_f64, the
-// reference's LocalStatisticsTile precision).
-template <typename T>
-__global__ void __launch_bounds__(LS_THREADS)
-local_stats_kernel(const float* __restrict__ in, size_t in_stride, int width, int height, int r,
-                   T* __restrict__ mean_out, T* __restrict__ var_out, uint32_t* __restrict__ count_out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    LsSmem& S = *reinterpret_cast<LsSmem*>(smem_raw);
-    const int x0 = blockIdx.x * LS_TW, y0 = blockIdx.y * LS_TH;
-    const int rows_lo = max(0, y0 - r), rows_hi = min(height - 1, y0 + LS_TH - 1 + r);
-    const int nrows = rows_hi - rows_lo + 1;
-    for (int c = 0; c < 3; ++c) {
-        // the CTA's shift: its first in-image sample of this channel (0 if not finite)
-        float sh = in[(size_t)y0 * in_stride + (size_t)x0 * 3 + c];
-        const double shift = isfinite(sh) ? (double)sh : 0.0;
-        // horizontal window moments for every needed row and output column
-        for (int i = threadIdx.x; i < nrows * LS_TW; i += LS_THREADS) {
-            const int tx = i % LS_TW, ty = i / LS_TW;
-            const int x = x0 + tx, y = rows_lo + ty;
-            double a = 0, b = 0;
-            int n = 0;
-            if (x < width) {
-                const float* row = in + (size_t)y * in_stride;
-                for (int j = max(0, x - r); j <= min(width - 1, x + r); ++j) {
-                    const float v = row[(size_t)j * 3 + c];
-                    if (!isfinite(v)) continue;
-                    const double d = (double)v - shift;
-                    a += d;
-                    b += d * d;
-                    ++n;
+__device__ __forceinline__ StripTask strip_task(int task, int strips, int tw, int th, int height) {
+    const int band = task / strips, strip = task % strips;
+    StripTask t;
+    t.x0 = strip * tw;
+    t.y0 = band * th;
+    t.y1 = min(height, t.y0 + th);
+    return t;
+}
+
+// --------------------------------------------------------------- guided filter
+
+constexpr int GF_MOMENTS = 6;   // R, G, B, YR, YG, YB
+
+struct GfParams {
+    const float* in;
+    size_t in_stride;
+    float* out;
+    size_t out_stride;
+    int width, height, r;
+    int tw, th, strips, tasks;
+    double eps;
+    YWeights w;
+    double* ring;          // per CTA: (2r+1) rows x 6 moments x tw outputs
+    uint32_t* status;
+};
+
+// One input pixel; zero outside the image or when `use` is false.
+__device__ __forceinline__ float3 gf_pixel(const GfParams& P, int x, int y, bool use) {
+    if (!use || x < 0 || x >= P.width) return make_float3(0.f, 0.f, 0.f);
+    const float* p = P.in + (size_t)y * P.in_stride + (size_t)x * 3;
+    return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+
+// The six moments of one pixel; flags non-finite input.
+__device__ __forceinline__ void gf_moments(const GfParams& P, float3 v, double m[GF_MOMENTS], bool& bad) {
+    bad |= !(isfinite(v.x) && isfinite(v.y) && isfinite(v.z));
+    const double r = v.x, g = v.y, b = v.z;
+    const double y_ = fma(P.w.wb, b - g, fma(P.w.wr, r - g, g));
+    m[0] = r; m[1] = g; m[2] = b;
+    m[3] = y_ * r; m[4] = y_ * g; m[5] = y_ * b;
+}
+
+// 1/n for a window count 1 <= n <= 2^24: the correctly rounded binary32
+// reciprocal refined by two Newton steps in binary64 (relative error below
+// 2^-50).
+__device__ __forceinline__ double rcp_count(int n) {
+    const double x = (double)n;
+    double q = (double)__frcp_rn((float)n);
+    q = fma(q, fma(-x, q, 1.0), q);
+    q = fma(q, fma(-x, q, 1.0), q);
+    return q;
+}
+
+template <int NT, int R, int K, int MINB>
+__global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
+    constexpr int C1 = NT;                  // input columns of a strip
+    constexpr int C1P = plane_len<K>(C1);
+    extern __shared__ __align__(16) double smem_gf[];
+    const int r = P.r, tw = P.tw, c2 = tw + 2 * r, c2p = c2 + c2 / K + 1;
+    double* Vb = smem_gf;                                   // [R][6][C1P]  phase A sums
+    double* ABb = Vb + (size_t)R * GF_MOMENTS * C1P;        // [R][6][c2p]  a (3), b (3) per centre
+    double* H2b = Vb;                                       // [R][6][C1P]  phase C sums (aliases Vb)
+    const int period = 2 * r + 1;
+    double* ring = P.ring + (size_t)blockIdx.x * period * GF_MOMENTS * tw;
+    const int tid = threadIdx.x;
+    bool bad = false, overflow = false;
+    for (int task = blockIdx.x; task < P.tasks; task += gridDim.x) {
+        const StripTask T = strip_task(task, P.strips, tw, P.th, P.height);
+        const int xa = T.x0 - 2 * r;                        // image column of input column 0
+        const int tc0 = max(0, T.y0 - r);                   // first centre row
+        const int t_end = T.y1 - 1 + r;                     // last step (emits output row T.y1 - 1)
+        const int last_centre = min(P.height - 1, t_end);
+        // phase A state: window sums of the column's moments for centre row t
+        double V[GF_MOMENTS];
+        {
+            const int x = xa + tid;
+#pragma unroll
+            for (int k = 0; k < GF_MOMENTS; ++k) V[k] = 0.0;
+            for (int y = max(0, tc0 - r); y <= min(P.height - 1, tc0 + r - 1); ++y) {
+                if (x < 0 || x >= P.width) break;
+                double m[GF_MOMENTS];
+                gf_moments(P, gf_pixel(P, x, y, true), m, bad);
+#pragma unroll
+                for (int k = 0; k < GF_MOMENTS; ++k) V[k] += m[k];
+            }
+        }
+        // phase D state: window sums of the centres' horizontal a/b sums
+        double Q[GF_MOMENTS];
+#pragma unroll
+        for (int k = 0; k < GF_MOMENTS; ++k) Q[k] = 0.0;
+        for (int tb = tc0; tb <= t_end; tb += R) {
+            const int rows = min(R, last_centre - tb + 1);   // centre rows in this block (may be <= 0)
+            // A: vertical window sums, one column per thread
+            if (rows > 0) {
+                const int x = xa + tid;
+                // every pixel of the block's rows is requested before any is used
+                float3 pin[R], pout[R];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int t = tb + i;
+                    pin[i] = gf_pixel(P, x, t + r, i < rows && t + r <= P.height - 1);
+                    pout[i] = gf_pixel(P, x, t - r - 1, i < rows && t - r - 1 >= max(0, tc0 - r));
+                }
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    if (i >= rows) break;
+                    double m[GF_MOMENTS], l[GF_MOMENTS];
+                    gf_moments(P, pin[i], m, bad);
+                    gf_moments(P, pout[i], l, bad);
+                    double* vrow = Vb + (size_t)i * GF_MOMENTS * C1P + sk<K>(tid);
+#pragma unroll
+                    for (int k = 0; k < GF_MOMENTS; ++k) {
+                        V[k] += m[k] - l[k];
+                        vrow[k * C1P] = V[k];
+                    }
                 }
             }
-            S.s1[ty][tx] = a;
-            S.s2[ty][tx] = b;
-            S.n[ty][tx] = n;
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < LS_TW * LS_TH; i += LS_THREADS) {
-            const int tx = i % LS_TW, ty = i / LS_TW;
-            const int x = x0 + tx, y = y0 + ty;
-            if (x >= width || y >= height) continue;
-            double a = 0, b = 0;
-            int n = 0;
-            for (int j = max(0, y - r); j <= min(height - 1, y + r); ++j) {
-                a += S.s1[j - rows_lo][tx];
-                b += S.s2[j - rows_lo][tx];
-                n += S.n[j - rows_lo][tx];
+            __syncthreads();
+            // B: horizontal window sums per centre, then a and b
+            const int segs_b = (c2 + K - 1) / K;
+            for (int item = tid; item < max(rows, 0) * segs_b; item += NT) {
+                const int i = item / segs_b, c0 = (item % segs_b) * K, c1 = min(c0 + K, c2);
+                const int t = tb + i;
+                const double* vrow = Vb + (size_t)i * GF_MOMENTS * C1P;
+                double* abrow = ABb + (size_t)i * GF_MOMENTS * c2p;
+                double S[GF_MOMENTS];
+#pragma unroll
+                for (int k = 0; k < GF_MOMENTS; ++k) S[k] = 0.0;
+                for (int j = c0; j <= c0 + 2 * r; ++j)
+#pragma unroll
+                    for (int k = 0; k < GF_MOMENTS; ++k) S[k] += vrow[k * C1P + sk<K>(j)];
+                const int wy = extent(t, r, P.height);
+                for (int c = c0; c < c1; ++c) {
+                    if (c > c0)
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k)
+                            S[k] += vrow[k * C1P + sk<K>(c + 2 * r)] - vrow[k * C1P + sk<K>(c - 1)];
+                    const int xc = T.x0 - r + c;
+                    if (xc < 0 || xc >= P.width) {
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k) abrow[k * c2p + sk<K>(c)] = 0.0;
+                        continue;
+                    }
+                    const double inv_n = rcp_count(extent(xc, r, P.width) * wy);
+                    const double sy = fma(P.w.wb, S[2] - S[1], fma(P.w.wr, S[0] - S[1], S[1]));
+                    const double syy = fma(P.w.wb, S[5] - S[4], fma(P.w.wr, S[3] - S[4], S[4]));
+                    const double my = sy * inv_n;
+                    double var = syy * inv_n - my * my;
+                    if (var < 0) var = 0;
+                    const double inv = 1.0 / (var + P.eps);
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) {
+                        const double mp = S[ch] * inv_n;
+                        const double cov = S[3 + ch] * inv_n - my * mp;
+                        const double a = cov * inv;
+                        const double b = mp - a * my;
+                        overflow |= !(isfinite(a) && isfinite(b));
+                        abrow[ch * c2p + sk<K>(c)] = a;
+                        abrow[(3 + ch) * c2p + sk<K>(c)] = b;
+                    }
+                }
             }
-            const size_t o = (size_t)y * width * 3 + (size_t)x * 3 + c;
-            if (count_out) count_out[o] = (uint32_t)n;
-            if (n == 0) {
-                mean_out[o] = NAN;
-                var_out[o] = NAN;
-                continue;
+            __syncthreads();
+            // C: horizontal window sums of a and b per output column
+            const int segs_c = (tw + K - 1) / K;
+            for (int item = tid; item < max(rows, 0) * segs_c; item += NT) {
+                const int i = item / segs_c, o0 = (item % segs_c) * K, o1 = min(o0 + K, tw);
+                const double* abrow = ABb + (size_t)i * GF_MOMENTS * c2p;
+                double* hrow = H2b + (size_t)i * GF_MOMENTS * C1P;
+                double S[GF_MOMENTS];
+#pragma unroll
+                for (int k = 0; k < GF_MOMENTS; ++k) S[k] = 0.0;
+                for (int c = o0; c <= o0 + 2 * r; ++c)
+#pragma unroll
+                    for (int k = 0; k < GF_MOMENTS; ++k) S[k] += abrow[k * c2p + sk<K>(c)];
+                for (int o = o0; o < o1; ++o) {
+                    if (o > o0)
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k)
+                            S[k] += abrow[k * c2p + sk<K>(o + 2 * r)] - abrow[k * c2p + sk<K>(o - 1)];
+#pragma unroll
+                    for (int k = 0; k < GF_MOMENTS; ++k) hrow[k * C1P + sk<K>(o)] = S[k];
+                }
             }
-            const double mean = a / n;
-            double var = (b - a * mean) / n;
-            if (var < 0) var = 0;
-            mean_out[o] = (T)(shift + mean);
-            var_out[o] = (T)var;
+            __syncthreads();
+            // D: vertical window sums of C's rows, one output column per thread
+            if (tid < tw) {
+                const int x = T.x0 + tid;
+                const int steps = min(R, t_end - tb + 1);
+                for (int i = 0; i < steps; ++i) {
+                    const int t = tb + i;
+                    double* slot = ring + (size_t)(t % period) * GF_MOMENTS * tw + tid;
+                    double h[GF_MOMENTS];
+                    if (t <= last_centre) {
+                        const double* hrow = H2b + (size_t)i * GF_MOMENTS * C1P;
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k) {
+                            h[k] = hrow[k * C1P + sk<K>(tid)];
+                            Q[k] += h[k];
+                        }
+                    }
+                    if (t - period >= tc0)
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k) Q[k] -= slot[(size_t)k * tw];
+                    if (t <= last_centre)
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k) slot[(size_t)k * tw] = h[k];
+                    const int yo = t - r;
+                    if (yo < T.y0 || yo >= T.y1 || x >= P.width) continue;
+                    const float* p = P.in + (size_t)yo * P.in_stride + (size_t)x * 3;
+                    const float pv[3] = {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+                    const double Y = working_y(pv[0], pv[1], pv[2], P.w);
+                    const double inv_n = rcp_count(extent(x, r, P.width) * extent(yo, r, P.height));
+                    float* o = P.out + (size_t)yo * P.out_stride + (size_t)x * 3;
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) {
+                        const double q = (Q[ch] * inv_n) * Y + Q[3 + ch] * inv_n;
+                        const double delta = q - (double)pv[ch];
+                        if (delta == 0) {
+                            o[ch] = pv[ch];
+                            continue;
+                        }
+                        if (!isfinite(q) || fabs(q) > (double)FLT_MAX) overflow = true;
+                        o[ch] = (float)q;
+                    }
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
+    }
+    if (P.status) {
+        if (bad) atomicMax(P.status, (uint32_t)((401u << 8) | ST_INVALID));
+        if (overflow) atomicMax(P.status, (uint32_t)((400u << 8) | ST_OVERFLOW));
     }
 }
 
-struct Scratch {
-    void* p = nullptr;
-    cudaStream_t s = nullptr;
-    ~Scratch() {
-        if (p) cudaFreeAsync(p, s);
-    }
+// ---------------------------------------------------------- local statistics
+
+constexpr int LS_NT = 256, LS_R = 4, LS_K = 8, LS_MAX_R = 32;
+
+struct LsParams {
+    const float* in;
+    size_t in_stride;
+    int width, height, r;
+    int tw, th, strips, tasks;
+    void* mean_out;
+    void* var_out;
+    uint32_t* count_out;
 };
+
+// Byte offsets of the local-statistics planes in shared memory (16-byte
+// aligned).  The output staging planes are channel-major and skewed like the
+// sum planes, so that the row segments' K-strided writes do not conflict.
+struct LsSmem {
+    size_t v, n, o, c, total;
+    int twp;
+};
+__host__ __device__ inline LsSmem ls_smem_layout(int tw, size_t out_bytes) {
+    const size_t c1p = plane_len<LS_K>(LS_NT);
+    auto up = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    LsSmem L;
+    L.twp = plane_len<LS_K>(tw);
+    L.v = 0;
+    L.n = up(L.v + (size_t)LS_R * 6 * c1p * sizeof(double));
+    L.o = up(L.n + (size_t)LS_R * 3 * c1p * sizeof(int));
+    L.c = up(L.o + (size_t)LS_R * 6 * L.twp * out_bytes);
+    L.total = up(L.c + (size_t)LS_R * 3 * L.twp * sizeof(uint32_t));
+    return L;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
+    constexpr int C1P = plane_len<LS_K>(LS_NT);
+    extern __shared__ __align__(16) double smem_ls[];
+    const LsSmem L = ls_smem_layout(P.tw, sizeof(T));
+    char* base = reinterpret_cast<char*>(smem_ls);
+    double* Vb = reinterpret_cast<double*>(base + L.v);       // [R][6][C1P]: s1 x3, s2 x3
+    int* Nb = reinterpret_cast<int*>(base + L.n);             // [R][3][C1P]
+    T* Ob = reinterpret_cast<T*>(base + L.o);                 // [6][R][twp]: mean x3, var x3
+    uint32_t* Cb = reinterpret_cast<uint32_t*>(base + L.c);   // [3][R][twp]
+    const int r = P.r, tw = P.tw, twp = L.twp, tid = threadIdx.x;
+    T* mean_out = static_cast<T*>(P.mean_out);
+    T* var_out = static_cast<T*>(P.var_out);
+    for (int task = blockIdx.x; task < P.tasks; task += gridDim.x) {
+        const StripTask Tk = strip_task(task, P.strips, tw, P.th, P.height);
+        const int xa = Tk.x0 - r;
+        // the task's shift: its first output pixel, per channel (0 if not finite)
+        double shift[3];
+        {
+            const float* p = P.in + (size_t)Tk.y0 * P.in_stride + (size_t)Tk.x0 * 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float v = __ldg(p + c);
+                shift[c] = isfinite(v) ? (double)v : 0.0;
+            }
+        }
+        const int x = xa + tid;
+        const bool in_image = x >= 0 && x < P.width;
+        double s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
+        int n[3] = {0, 0, 0};
+        auto load = [&](int y, bool use) -> float3 {
+            if (!use || !in_image) return make_float3(NAN, NAN, NAN);
+            const float* p = P.in + (size_t)y * P.in_stride + (size_t)x * 3;
+            return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+        };
+        // adds (sign +1) or removes (sign -1) one pixel's finite channels
+        auto add = [&](float3 v, int sign) {
+            const float c3[3] = {v.x, v.y, v.z};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                if (!isfinite(c3[c])) continue;
+                const double d = (double)c3[c] - shift[c];
+                s1[c] += sign > 0 ? d : -d;
+                s2[c] += sign > 0 ? d * d : -(d * d);
+                n[c] += sign;
+            }
+        };
+        for (int y = max(0, Tk.y0 - r); y <= min(P.height - 1, Tk.y0 + r - 1); ++y) add(load(y, true), 1);
+        for (int tb = Tk.y0; tb < Tk.y1; tb += LS_R) {
+            const int rows = min(LS_R, Tk.y1 - tb);
+            // A: vertical window sums of the column; every pixel of the block's
+            //    rows is requested before any is used
+            float3 pin[LS_R], pout[LS_R];
+#pragma unroll
+            for (int i = 0; i < LS_R; ++i) {
+                const int t = tb + i;
+                pin[i] = load(t + r, i < rows && t + r <= P.height - 1);
+                pout[i] = load(t - r - 1, i < rows && t - r - 1 >= max(0, Tk.y0 - r));
+            }
+#pragma unroll
+            for (int i = 0; i < LS_R; ++i) {
+                if (i >= rows) break;
+                add(pin[i], 1);
+                add(pout[i], -1);
+                double* vrow = Vb + (size_t)i * 6 * C1P + sk<LS_K>(tid);
+                int* nrow = Nb + (size_t)i * 3 * C1P + sk<LS_K>(tid);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    vrow[c * C1P] = s1[c];
+                    vrow[(3 + c) * C1P] = s2[c];
+                    nrow[c * C1P] = n[c];
+                }
+            }
+            __syncthreads();
+            // B: horizontal window sums per output column, mean and variance
+            const int segs = (tw + LS_K - 1) / LS_K;
+            for (int item = tid; item < rows * segs; item += LS_NT) {
+                const int i = item / segs, o0 = (item % segs) * LS_K, o1 = min(o0 + LS_K, tw);
+                const double* vrow = Vb + (size_t)i * 6 * C1P;
+                const int* nrow = Nb + (size_t)i * 3 * C1P;
+                double S[6] = {0, 0, 0, 0, 0, 0};
+                int N[3] = {0, 0, 0};
+                for (int j = o0; j <= o0 + 2 * r; ++j) {
+                    const int sj = sk<LS_K>(j);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) S[k] += vrow[k * C1P + sj];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) N[c] += nrow[c * C1P + sj];
+                }
+                for (int o = o0; o < o1; ++o) {
+                    if (o > o0) {
+                        const int in_j = sk<LS_K>(o + 2 * r), out_j = sk<LS_K>(o - 1);
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) S[k] += vrow[k * C1P + in_j] - vrow[k * C1P + out_j];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) N[c] += nrow[c * C1P + in_j] - nrow[c * C1P + out_j];
+                    }
+                    const int so = sk<LS_K>(o);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        Cb[((size_t)c * LS_R + i) * twp + so] = (uint32_t)N[c];
+                        T mean = (T)NAN, var = (T)NAN;
+                        if (N[c]) {
+                            const double inv = rcp_count(N[c]);
+                            const double m = S[c] * inv;
+                            double v = (S[3 + c] - S[c] * m) * inv;
+                            if (v < 0) v = 0;
+                            mean = (T)(shift[c] + m);
+                            var = (T)v;
+                        }
+                        Ob[((size_t)c * LS_R + i) * twp + so] = mean;
+                        Ob[((size_t)(3 + c) * LS_R + i) * twp + so] = var;
+                    }
+                }
+            }
+            __syncthreads();
+            // coalesced stores of the block's rows
+            const int width_out = min(tw, P.width - Tk.x0);
+            for (int e = tid; e < rows * width_out * 3; e += LS_NT) {
+                const int i = e / (width_out * 3), rem = e % (width_out * 3);
+                const int o = rem / 3, c = rem % 3;
+                const size_t at = ((size_t)(tb + i) * P.width + Tk.x0 + o) * 3 + c;
+                const int so = sk<LS_K>(o);
+                mean_out[at] = Ob[((size_t)c * LS_R + i) * twp + so];
+                var_out[at] = Ob[((size_t)(3 + c) * LS_R + i) * twp + so];
+                if (P.count_out) P.count_out[at] = Cb[((size_t)c * LS_R + i) * twp + so];
+            }
+            __syncthreads();
+        }
+    }
+}
 
 #define SP_CUDA(call)                                                         \
     do {                                                                      \
@@ -307,6 +497,111 @@ struct Scratch {
             return RE_CUDA_ERROR;                                             \
         }                                                                     \
     } while (0)
+
+// Bands of output rows: when the strips leave room, as many equal bands as
+// there are resident CTAs per strip, so that each CTA streams one long band
+// and pays the vertical halo (`halo` rows above and below) once; bands stay at
+// least 2 halo (and 16) rows tall.
+int band_height(int height, int strips, int ctas, int halo) {
+    const int bands = std::max(1, ctas / strips);
+    int th = (height + bands - 1) / bands;
+    th = std::max(th, std::max(16, 2 * halo));
+    return std::min(th, height);
+}
+
+int sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+struct GfLaunch {
+    GfParams P;
+    dim3 grid;
+    int threads;
+    size_t smem;
+    void (*kernel)(GfParams);
+};
+
+// MINB CTAs per SM: two for r <= 16, where each CTA's ring of a/b row sums
+// is at most 183 KB; one above, so that the rings of all resident CTAs
+// (up to 400 KB each at r = 32) stay well inside the 126 MB L2.
+template <int NT, int R, int K, int MINB>
+GfLaunch gf_plan(GfParams P, int sms) {
+    GfLaunch L;
+    P.tw = NT - 4 * P.r;
+    P.strips = (P.width + P.tw - 1) / P.tw;
+    const int ctas = MINB * sms;
+    P.th = band_height(P.height, P.strips, ctas, 2 * P.r);
+    P.tasks = P.strips * ((P.height + P.th - 1) / P.th);
+    const int c2 = P.tw + 2 * P.r;
+    L.smem = ((size_t)R * GF_MOMENTS * plane_len<K>(NT) + (size_t)R * GF_MOMENTS * (c2 + c2 / K + 1)) * sizeof(double);
+    L.grid = dim3(std::min(P.tasks, ctas));
+    L.threads = NT;
+    L.kernel = gf_strip_kernel<NT, R, K, MINB>;
+    L.P = P;
+    return L;
+}
+
+GfLaunch gf_choose(const GfParams& P, int sms) {
+    if (P.r <= 16) return gf_plan<256, 4, 8, 2>(P, sms);
+    if (P.r <= 32) return gf_plan<256, 8, 16, 1>(P, sms);
+    return gf_plan<512, 4, 16, 1>(P, sms);
+}
+
+size_t gf_ring_bytes(const GfLaunch& L) {
+    return (size_t)L.grid.x * (2 * L.P.r + 1) * GF_MOMENTS * L.P.tw * sizeof(double);
+}
+
+re_status gf_validate(const float* in, size_t in_stride, const float* out, size_t out_stride, uint32_t width,
+                      uint32_t height, uint32_t radius, double epsilon, uint32_t space) {
+    if (radius > 64 || !std::isfinite(epsilon) || epsilon < 0x1p-24 || epsilon > 65536.0) {
+        set_last_error("guided filter requires radius 0..64 and finite epsilon [2^-24,65536]");
+        return RE_INVALID_ARGUMENT;
+    }
+    if (space > 1) {
+        set_last_error("guided filter requires scene-linear working RGB");
+        return RE_INVALID_ARGUMENT;
+    }
+    if (!width || !height || !in || !out || in_stride < (size_t)width * 3 || out_stride < (size_t)width * 3) {
+        set_last_error("guided filter requires nonempty addressable bounds");
+        return RE_INVALID_ARGUMENT;
+    }
+    const char* ib = reinterpret_cast<const char*>(in);
+    const char* ie = reinterpret_cast<const char*>(in + ((size_t)height - 1) * in_stride + (size_t)width * 3);
+    const char* ob = reinterpret_cast<const char*>(out);
+    const char* oe = reinterpret_cast<const char*>(out + ((size_t)height - 1) * out_stride + (size_t)width * 3);
+    if (ob < ie && ib < oe) {
+        set_last_error("guided filter output must not overlap its input");
+        return RE_INVALID_ARGUMENT;
+    }
+    return RE_OK;
+}
+
+GfParams gf_params(const float* in, size_t in_stride, float* out, size_t out_stride, uint32_t width,
+                   uint32_t height, uint32_t radius, double epsilon, uint32_t space) {
+    GfParams P{};
+    P.in = in;
+    P.in_stride = in_stride;
+    P.out = out;
+    P.out_stride = out_stride;
+    P.width = (int)width;
+    P.height = (int)height;
+    P.r = (int)radius;
+    P.eps = epsilon;
+    P.w = space == 0 ? YWeights{0.28807112822929337, 0.00008565396060525903}
+                     : YWeights{0.26270021201126703, 0.059301716469861945};
+    return P;
+}
+
+re_status gf_enqueue(GfLaunch L, void* scratch, uint32_t* status, cudaStream_t stream) {
+    L.P.ring = static_cast<double*>(scratch);
+    L.P.status = status;
+    SP_CUDA(cudaFuncSetAttribute(L.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    L.kernel<<<L.grid, L.threads, L.smem, stream>>>(L.P);
+    SP_CUDA(cudaGetLastError());
+    return RE_OK;
+}
 
 template <typename T>
 re_status local_statistics(const float* in, size_t in_stride, uint32_t width, uint32_t height, uint32_t radius,
@@ -320,57 +615,74 @@ re_status local_statistics(const float* in, size_t in_stride, uint32_t width, ui
         return RE_INVALID_ARGUMENT;
     }
     cudaStream_t stream = (cudaStream_t)stream_;
-    SP_CUDA(cudaFuncSetAttribute(local_stats_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(LsSmem)));
-    dim3 grid((width + LS_TW - 1) / LS_TW, (height + LS_TH - 1) / LS_TH);
-    local_stats_kernel<T><<<grid, LS_THREADS, sizeof(LsSmem), stream>>>(in, in_stride, (int)width, (int)height,
-                                                                         (int)radius, mean_out, var_out, count_out);
+    LsParams P{};
+    P.in = in;
+    P.in_stride = in_stride;
+    P.width = (int)width;
+    P.height = (int)height;
+    P.r = (int)radius;
+    P.tw = LS_NT - 2 * P.r;
+    P.strips = (P.width + P.tw - 1) / P.tw;
+    const int ctas = 2 * sm_count();
+    P.th = band_height(P.height, P.strips, ctas, P.r);
+    P.tasks = P.strips * ((P.height + P.th - 1) / P.th);
+    P.mean_out = mean_out;
+    P.var_out = var_out;
+    P.count_out = count_out;
+    const size_t smem = ls_smem_layout(P.tw, sizeof(T)).total;
+    SP_CUDA(cudaFuncSetAttribute(ls_strip_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ls_strip_kernel<T><<<std::min(P.tasks, ctas), LS_NT, smem, stream>>>(P);
     SP_CUDA(cudaGetLastError());
-    SP_CUDA(cudaStreamSynchronize(stream));
     return RE_OK;
 }
+
+struct Scratch {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~Scratch() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
 
 }  // namespace
 
 extern "C" {
 
+size_t re_guided_filter_scratch_bytes(uint32_t width, uint32_t height, uint32_t radius) {
+    if (!width || !height || radius > 64) return 0;
+    GfParams P = gf_params(nullptr, 0, nullptr, 0, width, height, radius, 1.0, 0);
+    return 256 + gf_ring_bytes(gf_choose(P, sm_count()));
+}
+
 // SpatialOps.cpp:159-163 settings (radius extended to 64), 168-287 output.
+re_status re_guided_filter_async(const float* in, size_t in_stride, float* out, size_t out_stride, uint32_t width,
+                                 uint32_t height, uint32_t radius, double epsilon, uint32_t space,
+                                 uint32_t* device_status, void* scratch, void* stream) {
+    re_status s = gf_validate(in, in_stride, out, out_stride, width, height, radius, epsilon, space);
+    if (s) return s;
+    if (!scratch) {
+        set_last_error("guided filter needs scratch of re_guided_filter_scratch_bytes()");
+        return RE_INVALID_ARGUMENT;
+    }
+    const GfLaunch L = gf_choose(gf_params(in, in_stride, out, out_stride, width, height, radius, epsilon, space),
+                                 sm_count());
+    return gf_enqueue(L, static_cast<char*>(scratch) + 256, device_status, (cudaStream_t)stream);
+}
+
 re_status re_guided_filter(const float* in, size_t in_stride, float* out, size_t out_stride, uint32_t width,
                            uint32_t height, uint32_t radius, double epsilon, uint32_t space, void* stream_) {
-    if (radius > 64 || !std::isfinite(epsilon) || epsilon < 0x1p-24 || epsilon > 65536.0) {
-        set_last_error("guided filter requires radius 0..64 and finite epsilon [2^-24,65536]");
-        return RE_INVALID_ARGUMENT;
-    }
-    if (space > 1) {
-        set_last_error("guided filter requires scene-linear working RGB");
-        return RE_INVALID_ARGUMENT;
-    }
-    if (!width || !height || !in || !out || in_stride < (size_t)width * 3 || out_stride < (size_t)width * 3) {
-        set_last_error("guided filter requires nonempty addressable bounds");
-        return RE_INVALID_ARGUMENT;
-    }
+    re_status s = gf_validate(in, in_stride, out, out_stride, width, height, radius, epsilon, space);
+    if (s) return s;
     cudaStream_t stream = (cudaStream_t)stream_;
-    const YWeights w = space == 0 ? YWeights{0.28807112822929337, 0.00008565396060525903}
-                                  : YWeights{0.26270021201126703, 0.059301716469861945};
-    const size_t px = (size_t)width * height;
+    const GfLaunch L = gf_choose(gf_params(in, in_stride, out, out_stride, width, height, radius, epsilon, space),
+                                 sm_count());
     Scratch sc;
     sc.s = stream;
-    SP_CUDA(cudaMallocAsync(&sc.p, 256 + px * 8 * sizeof(double) + 2 * px * 6 * sizeof(double), stream));
+    SP_CUDA(cudaMallocAsync(&sc.p, 256 + gf_ring_bytes(L), stream));
     uint32_t* status = (uint32_t*)sc.p;
-    double* H = (double*)((char*)sc.p + 256);
-    double* AB = H + px * 8;
-    double* H2 = AB + px * 6;
     SP_CUDA(cudaMemsetAsync(status, 0, 4, stream));
-    const int r = (int)radius;
-    const int chunks = ((int)width + GF_CHUNK - 1) / GF_CHUNK;
-    gf_hbox_moments<<<dim3((chunks + 63) / 64, height), 64, 0, stream>>>(in, in_stride, width, height, r, w, H,
-                                                                         status);
-    gf_vbox_coefficients<<<dim3((width + 127) / 128, (height + GF_CHUNK - 1) / GF_CHUNK), 128, 0, stream>>>(
-        H, width, height, r, epsilon, AB, status);
-    gf_hbox_ab<<<dim3((chunks + 63) / 64, height), 64, 0, stream>>>(AB, width, height, r, H2);
-    gf_vbox_output<<<dim3((width + 127) / 128, (height + GF_CHUNK - 1) / GF_CHUNK), 128, 0, stream>>>(
-        H2, in, in_stride, width, height, r, w, out, out_stride, status);
-    SP_CUDA(cudaGetLastError());
+    s = gf_enqueue(L, static_cast<char*>(sc.p) + 256, status, stream);
+    if (s) return s;
     uint32_t key = 0;
     SP_CUDA(cudaMemcpyAsync(&key, status, 4, cudaMemcpyDeviceToHost, stream));
     SP_CUDA(cudaStreamSynchronize(stream));

@@ -238,12 +238,14 @@ int main(int argc, char** argv) {
     std::printf("{\"requests\": %zu, \"images\": %zu, \"lanes\": %zu, \"output_mpix\": %.3f, \"mismatches\": %zu, "
                 "\"per_request_s\": %.5f, \"scheduler_host_s\": %.5f, \"scheduler_device_s\": %.5f, "
                 "\"waves\": %llu, \"batched_requests\": %llu, \"node_requests\": %llu, \"unbatchable_requests\": %llu, \"batch_fallbacks\": %llu, "
-                "\"last_fallback\": \"%s\"}\n",
+                "\"last_fallback\": \"%s\", \"lane_lower_s\": %.4f, \"lane_plan_s\": %.4f, "
+                "\"lane_device_s\": %.4f, \"lane_deliver_s\": %.4f}\n",
                 tiles.size(), images.size(), lanes, out_px / 1e6, mismatches, direct_s, host_s, device_s,
                 (unsigned long long)(after.waves - before.waves),
                 (unsigned long long)(after.batched_requests - before.batched_requests),
                 (unsigned long long)(after.node_requests - before.node_requests),
                 (unsigned long long)(after.unbatchable_requests - before.unbatchable_requests),
-                (unsigned long long)after.batch_fallbacks, after.last_fallback.c_str());
+                (unsigned long long)after.batch_fallbacks, after.last_fallback.c_str(), after.lower_s - before.lower_s,
+                after.plan_s - before.plan_s, after.device_s - before.device_s, after.deliver_s - before.deliver_s);
     return mismatches ? 1 : 0;
 }

@@ -247,3 +247,24 @@ def test_batch_merges_tiles_of_one_render():
     for f, w in zip(frames, wants):
         assert bits_equal(f.cpu().numpy(), w)
     batch.close()
+
+
+def test_batch_keeps_row_tiles_apart_when_the_stride_is_too_small():
+    """One-row tiles whose outputs lie back to back in one buffer, each with
+    its own narrow row stride (a scheduler's packed output block): the
+    planner must not merge them into a render wider than that stride."""
+    images, recipes, _ = _small_batch(seed=17)
+    imgs = _device_images(images)
+    pipes = [workloads.mixed_pipeline(im, r) for im, r in zip(images, recipes)]
+    img, pipe = imgs[0], pipes[0]
+    ax, ay, aw, ah = images[0].active
+    width = 8
+    vps = [(ax + 16 + k * width, ay + 9, width, 1) for k in range(6)]
+    arena = torch.full((len(vps) * width * 3,), float("nan"), device="cuda")
+    outs = [arena[k * width * 3:(k + 1) * width * 3].view(1, width, 3) for k in range(len(vps))]
+    batch = render.Batch().plan([(img, pipe, vp, 0, 1, o) for vp, o in zip(vps, outs)])
+    batch.launch()
+    batch.status()
+    for vp, o in zip(vps, outs):
+        assert bits_equal(o.cpu().numpy(), render.render(img, pipe, vp))
+    batch.close()
