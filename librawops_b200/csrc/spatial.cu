@@ -78,6 +78,42 @@ __host__ __device__ constexpr int plane_len(int n) {
     return n + n / K + 1;
 }
 
+// Sums of the K-element blocks of `rows` rows of M skewed planes of length
+// plen: bs[(i * M + k) * nb + b] = plane (i, k) summed over columns
+// [b K, b K + K), which sit contiguously from b (K + 1).
+template <int NT, int K, int M, typename V>
+__device__ __forceinline__ void block_sums(const V* planes, int plen, int rows, int nb, V* bs) {
+    for (int item = threadIdx.x; item < rows * nb; item += NT) {
+        const int i = item / nb, b = item % nb;
+        const V* row = planes + (size_t)i * M * plen + b * (K + 1);
+        V acc[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) acc[k] = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+#pragma unroll
+            for (int k = 0; k < M; ++k) acc[k] += row[k * plen + j];
+#pragma unroll
+        for (int k = 0; k < M; ++k) bs[((size_t)i * M + k) * nb + b] = acc[k];
+    }
+}
+
+// The window sum over columns [c0, c0 + 2r] (c0 a multiple of K) of one row
+// of M skewed planes: the whole blocks from their block sums, the rest
+// element by element.
+template <int K, int M, typename V>
+__device__ __forceinline__ void window_start(const V* row, int plen, const V* bsrow, int nb, int c0, int r, V S[M]) {
+    const int b0 = c0 / K, q = (2 * r + 1) / K;
+#pragma unroll
+    for (int k = 0; k < M; ++k) S[k] = 0;
+    for (int b = b0; b < b0 + q; ++b)
+#pragma unroll
+        for (int k = 0; k < M; ++k) S[k] += bsrow[k * nb + b];
+    for (int j = (b0 + q) * K; j <= c0 + 2 * r; ++j)
+#pragma unroll
+        for (int k = 0; k < M; ++k) S[k] += row[k * plen + j + j / K];
+}
+
 // Clipped window extent along one axis of length len.
 __device__ __forceinline__ int extent(int c, int r, int len) {
     return min(len - 1, c + r) - max(0, c - r) + 1;
@@ -113,10 +149,13 @@ struct GfParams {
     uint32_t* status;
 };
 
-// One input pixel; zero outside the image or when `use` is false.
-__device__ __forceinline__ float3 gf_pixel(const GfParams& P, int x, int y, bool use) {
+// One input pixel; zero outside the image or when `use` is false.  `last`
+// marks the pixel's last read by the CTA (the row leaving the vertical
+// window), loaded evict-first so that it leaves L2 before the rings do.
+__device__ __forceinline__ float3 gf_pixel(const GfParams& P, int x, int y, bool use, bool last = false) {
     if (!use || x < 0 || x >= P.width) return make_float3(0.f, 0.f, 0.f);
     const float* p = P.in + (size_t)y * P.in_stride + (size_t)x * 3;
+    if (last) return make_float3(__ldcs(p), __ldcs(p + 1), __ldcs(p + 2));
     return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
@@ -149,6 +188,9 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
     double* Vb = smem_gf;                                   // [R][6][C1P]  phase A sums
     double* ABb = Vb + (size_t)R * GF_MOMENTS * C1P;        // [R][6][c2p]  a (3), b (3) per centre
     double* H2b = Vb;                                       // [R][6][C1P]  phase C sums (aliases Vb)
+    double* Bs = ABb + (size_t)R * GF_MOMENTS * c2p;        // [R][6][C1 / K] block sums (V, then a/b)
+    constexpr int NBV = C1 / K;
+    const int nba = c2 / K;
     const int period = 2 * r + 1;
     double* ring = P.ring + (size_t)blockIdx.x * period * GF_MOMENTS * tw;
     const int tid = threadIdx.x;
@@ -188,7 +230,7 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 for (int i = 0; i < R; ++i) {
                     const int t = tb + i;
                     pin[i] = gf_pixel(P, x, t + r, i < rows && t + r <= P.height - 1);
-                    pout[i] = gf_pixel(P, x, t - r - 1, i < rows && t - r - 1 >= max(0, tc0 - r));
+                    pout[i] = gf_pixel(P, x, t - r - 1, i < rows && t - r - 1 >= max(0, tc0 - r), true);
                 }
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
@@ -205,6 +247,8 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 }
             }
             __syncthreads();
+            block_sums<NT, K, GF_MOMENTS>(Vb, C1P, max(rows, 0), NBV, Bs);
+            __syncthreads();
             // B: horizontal window sums per centre, then a and b
             const int segs_b = (c2 + K - 1) / K;
             for (int item = tid; item < max(rows, 0) * segs_b; item += NT) {
@@ -213,11 +257,7 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 const double* vrow = Vb + (size_t)i * GF_MOMENTS * C1P;
                 double* abrow = ABb + (size_t)i * GF_MOMENTS * c2p;
                 double S[GF_MOMENTS];
-#pragma unroll
-                for (int k = 0; k < GF_MOMENTS; ++k) S[k] = 0.0;
-                for (int j = c0; j <= c0 + 2 * r; ++j)
-#pragma unroll
-                    for (int k = 0; k < GF_MOMENTS; ++k) S[k] += vrow[k * C1P + sk<K>(j)];
+                window_start<K, GF_MOMENTS>(vrow, C1P, Bs + (size_t)i * GF_MOMENTS * NBV, NBV, c0, r, S);
                 const int wy = extent(t, r, P.height);
                 for (int c = c0; c < c1; ++c) {
                     if (c > c0)
@@ -250,6 +290,8 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 }
             }
             __syncthreads();
+            block_sums<NT, K, GF_MOMENTS>(ABb, c2p, max(rows, 0), nba, Bs);
+            __syncthreads();
             // C: horizontal window sums of a and b per output column
             const int segs_c = (tw + K - 1) / K;
             for (int item = tid; item < max(rows, 0) * segs_c; item += NT) {
@@ -257,11 +299,7 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 const double* abrow = ABb + (size_t)i * GF_MOMENTS * c2p;
                 double* hrow = H2b + (size_t)i * GF_MOMENTS * C1P;
                 double S[GF_MOMENTS];
-#pragma unroll
-                for (int k = 0; k < GF_MOMENTS; ++k) S[k] = 0.0;
-                for (int c = o0; c <= o0 + 2 * r; ++c)
-#pragma unroll
-                    for (int k = 0; k < GF_MOMENTS; ++k) S[k] += abrow[k * c2p + sk<K>(c)];
+                window_start<K, GF_MOMENTS>(abrow, c2p, Bs + (size_t)i * GF_MOMENTS * nba, nba, o0, r, S);
                 for (int o = o0; o < o1; ++o) {
                     if (o > o0)
 #pragma unroll
@@ -272,45 +310,62 @@ __global__ void __launch_bounds__(NT, MINB) gf_strip_kernel(const GfParams P) {
                 }
             }
             __syncthreads();
-            // D: vertical window sums of C's rows, one output column per thread
+            // D: vertical window sums of C's rows, one output column per thread.
+            //    The leaving ring rows and the input pixels of up to four steps
+            //    are requested before any is used (a step's ring slot is the one
+            //    it overwrites, so no more steps than the ring has rows).
             if (tid < tw) {
                 const int x = T.x0 + tid;
                 const int steps = min(R, t_end - tb + 1);
-                for (int i = 0; i < steps; ++i) {
-                    const int t = tb + i;
-                    double* slot = ring + (size_t)(t % period) * GF_MOMENTS * tw + tid;
-                    double h[GF_MOMENTS];
-                    if (t <= last_centre) {
-                        const double* hrow = H2b + (size_t)i * GF_MOMENTS * C1P;
+                const int chunk = period >= 4 ? 4 : 1;
+                for (int i0 = 0; i0 < steps; i0 += chunk) {
+                    double lv[4][GF_MOMENTS];
+                    float3 pv[4];
 #pragma unroll
-                        for (int k = 0; k < GF_MOMENTS; ++k) {
-                            h[k] = hrow[k * C1P + sk<K>(tid)];
-                            Q[k] += h[k];
-                        }
+                    for (int u = 0; u < 4; ++u) {
+                        const int i = i0 + u, t = tb + i;
+                        const bool live = u < chunk && i < steps;
+                        const bool leave = live && t - period >= tc0;
+                        const double* slot = ring + (size_t)(t % period) * GF_MOMENTS * tw + tid;
+#pragma unroll
+                        for (int k = 0; k < GF_MOMENTS; ++k) lv[u][k] = leave ? slot[(size_t)k * tw] : 0.0;
+                        const int yo = t - r;
+                        pv[u] = gf_pixel(P, x, yo, live && yo >= T.y0 && yo < T.y1);
                     }
-                    if (t - period >= tc0)
 #pragma unroll
-                        for (int k = 0; k < GF_MOMENTS; ++k) Q[k] -= slot[(size_t)k * tw];
-                    if (t <= last_centre)
+                    for (int u = 0; u < 4; ++u) {
+                        const int i = i0 + u, t = tb + i;
+                        if (u >= chunk || i >= steps) break;
+                        double* slot = ring + (size_t)(t % period) * GF_MOMENTS * tw + tid;
+                        if (t <= last_centre) {
+                            const double* hrow = H2b + (size_t)i * GF_MOMENTS * C1P + sk<K>(tid);
 #pragma unroll
-                        for (int k = 0; k < GF_MOMENTS; ++k) slot[(size_t)k * tw] = h[k];
-                    const int yo = t - r;
-                    if (yo < T.y0 || yo >= T.y1 || x >= P.width) continue;
-                    const float* p = P.in + (size_t)yo * P.in_stride + (size_t)x * 3;
-                    const float pv[3] = {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
-                    const double Y = working_y(pv[0], pv[1], pv[2], P.w);
-                    const double inv_n = rcp_count(extent(x, r, P.width) * extent(yo, r, P.height));
-                    float* o = P.out + (size_t)yo * P.out_stride + (size_t)x * 3;
+                            for (int k = 0; k < GF_MOMENTS; ++k) {
+                                const double h = hrow[k * C1P];
+                                Q[k] += h - lv[u][k];
+                                slot[(size_t)k * tw] = h;
+                            }
+                        } else {
 #pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) {
-                        const double q = (Q[ch] * inv_n) * Y + Q[3 + ch] * inv_n;
-                        const double delta = q - (double)pv[ch];
-                        if (delta == 0) {
-                            o[ch] = pv[ch];
-                            continue;
+                            for (int k = 0; k < GF_MOMENTS; ++k) Q[k] -= lv[u][k];
                         }
-                        if (!isfinite(q) || fabs(q) > (double)FLT_MAX) overflow = true;
-                        o[ch] = (float)q;
+                        const int yo = t - r;
+                        if (yo < T.y0 || yo >= T.y1 || x >= P.width) continue;
+                        const float pc[3] = {pv[u].x, pv[u].y, pv[u].z};
+                        const double Y = working_y(pc[0], pc[1], pc[2], P.w);
+                        const double inv_n = rcp_count(extent(x, r, P.width) * extent(yo, r, P.height));
+                        float* o = P.out + (size_t)yo * P.out_stride + (size_t)x * 3;
+#pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) {
+                            const double q = (Q[ch] * inv_n) * Y + Q[3 + ch] * inv_n;
+                            const double delta = q - (double)pc[ch];
+                            if (delta == 0) {
+                                __stcs(o + ch, pc[ch]);   // written once, never re-read: evict first
+                                continue;
+                            }
+                            if (!isfinite(q) || fabs(q) > (double)FLT_MAX) overflow = true;
+                            __stcs(o + ch, (float)q);
+                        }
                     }
                 }
             }
@@ -341,7 +396,7 @@ struct LsParams {
 // aligned).  The output staging planes are channel-major and skewed like the
 // sum planes, so that the row segments' K-strided writes do not conflict.
 struct LsSmem {
-    size_t v, n, o, c, total;
+    size_t v, n, o, c, bv, bn, total;
     int twp;
 };
 __host__ __device__ inline LsSmem ls_smem_layout(int tw, size_t out_bytes) {
@@ -353,7 +408,9 @@ __host__ __device__ inline LsSmem ls_smem_layout(int tw, size_t out_bytes) {
     L.n = up(L.v + (size_t)LS_R * 6 * c1p * sizeof(double));
     L.o = up(L.n + (size_t)LS_R * 3 * c1p * sizeof(int));
     L.c = up(L.o + (size_t)LS_R * 6 * L.twp * out_bytes);
-    L.total = up(L.c + (size_t)LS_R * 3 * L.twp * sizeof(uint32_t));
+    L.bv = up(L.c + (size_t)LS_R * 3 * L.twp * sizeof(uint32_t));
+    L.bn = up(L.bv + (size_t)LS_R * 6 * (LS_NT / LS_K) * sizeof(double));
+    L.total = up(L.bn + (size_t)LS_R * 3 * (LS_NT / LS_K) * sizeof(int));
     return L;
 }
 
@@ -367,6 +424,9 @@ __global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
     int* Nb = reinterpret_cast<int*>(base + L.n);             // [R][3][C1P]
     T* Ob = reinterpret_cast<T*>(base + L.o);                 // [6][R][twp]: mean x3, var x3
     uint32_t* Cb = reinterpret_cast<uint32_t*>(base + L.c);   // [3][R][twp]
+    double* BsV = reinterpret_cast<double*>(base + L.bv);     // [R][6][NB] block sums
+    int* BsN = reinterpret_cast<int*>(base + L.bn);           // [R][3][NB]
+    constexpr int NB = LS_NT / LS_K;
     const int r = P.r, tw = P.tw, twp = L.twp, tid = threadIdx.x;
     T* mean_out = static_cast<T*>(P.mean_out);
     T* var_out = static_cast<T*>(P.var_out);
@@ -387,9 +447,10 @@ __global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
         const bool in_image = x >= 0 && x < P.width;
         double s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
         int n[3] = {0, 0, 0};
-        auto load = [&](int y, bool use) -> float3 {
+        auto load = [&](int y, bool use, bool last = false) -> float3 {
             if (!use || !in_image) return make_float3(NAN, NAN, NAN);
             const float* p = P.in + (size_t)y * P.in_stride + (size_t)x * 3;
+            if (last) return make_float3(__ldcs(p), __ldcs(p + 1), __ldcs(p + 2));
             return make_float3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
         };
         // adds (sign +1) or removes (sign -1) one pixel's finite channels
@@ -414,7 +475,7 @@ __global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
             for (int i = 0; i < LS_R; ++i) {
                 const int t = tb + i;
                 pin[i] = load(t + r, i < rows && t + r <= P.height - 1);
-                pout[i] = load(t - r - 1, i < rows && t - r - 1 >= max(0, Tk.y0 - r));
+                pout[i] = load(t - r - 1, i < rows && t - r - 1 >= max(0, Tk.y0 - r), true);
             }
 #pragma unroll
             for (int i = 0; i < LS_R; ++i) {
@@ -431,21 +492,19 @@ __global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
                 }
             }
             __syncthreads();
+            block_sums<LS_NT, LS_K, 6>(Vb, C1P, rows, NB, BsV);
+            block_sums<LS_NT, LS_K, 3>(Nb, C1P, rows, NB, BsN);
+            __syncthreads();
             // B: horizontal window sums per output column, mean and variance
             const int segs = (tw + LS_K - 1) / LS_K;
             for (int item = tid; item < rows * segs; item += LS_NT) {
                 const int i = item / segs, o0 = (item % segs) * LS_K, o1 = min(o0 + LS_K, tw);
                 const double* vrow = Vb + (size_t)i * 6 * C1P;
                 const int* nrow = Nb + (size_t)i * 3 * C1P;
-                double S[6] = {0, 0, 0, 0, 0, 0};
-                int N[3] = {0, 0, 0};
-                for (int j = o0; j <= o0 + 2 * r; ++j) {
-                    const int sj = sk<LS_K>(j);
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) S[k] += vrow[k * C1P + sj];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) N[c] += nrow[c * C1P + sj];
-                }
+                double S[6];
+                int N[3];
+                window_start<LS_K, 6>(vrow, C1P, BsV + (size_t)i * 6 * NB, NB, o0, r, S);
+                window_start<LS_K, 3>(nrow, C1P, BsN + (size_t)i * 3 * NB, NB, o0, r, N);
                 for (int o = o0; o < o1; ++o) {
                     if (o > o0) {
                         const int in_j = sk<LS_K>(o + 2 * r), out_j = sk<LS_K>(o - 1);
@@ -480,9 +539,9 @@ __global__ void __launch_bounds__(LS_NT, 2) ls_strip_kernel(const LsParams P) {
                 const int o = rem / 3, c = rem % 3;
                 const size_t at = ((size_t)(tb + i) * P.width + Tk.x0 + o) * 3 + c;
                 const int so = sk<LS_K>(o);
-                mean_out[at] = Ob[((size_t)c * LS_R + i) * twp + so];
-                var_out[at] = Ob[((size_t)(3 + c) * LS_R + i) * twp + so];
-                if (P.count_out) P.count_out[at] = Cb[((size_t)c * LS_R + i) * twp + so];
+                __stcs(mean_out + at, Ob[((size_t)c * LS_R + i) * twp + so]);
+                __stcs(var_out + at, Ob[((size_t)(3 + c) * LS_R + i) * twp + so]);
+                if (P.count_out) __stcs(P.count_out + at, Cb[((size_t)c * LS_R + i) * twp + so]);
             }
             __syncthreads();
         }
@@ -535,7 +594,8 @@ GfLaunch gf_plan(GfParams P, int sms) {
     P.th = band_height(P.height, P.strips, ctas, 2 * P.r);
     P.tasks = P.strips * ((P.height + P.th - 1) / P.th);
     const int c2 = P.tw + 2 * P.r;
-    L.smem = ((size_t)R * GF_MOMENTS * plane_len<K>(NT) + (size_t)R * GF_MOMENTS * (c2 + c2 / K + 1)) * sizeof(double);
+    L.smem = ((size_t)R * GF_MOMENTS * plane_len<K>(NT) + (size_t)R * GF_MOMENTS * (c2 + c2 / K + 1) +
+              (size_t)R * GF_MOMENTS * (NT / K)) * sizeof(double);
     L.grid = dim3(std::min(P.tasks, ctas));
     L.threads = NT;
     L.kernel = gf_strip_kernel<NT, R, K, MINB>;

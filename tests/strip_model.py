@@ -72,6 +72,28 @@ def band_height(height, strips, ctas, halo):
     return min(th, height)
 
 
+def block_sums(plane, plen, rows, nb, m, K, bs):
+    """block_sums<NT, K, M>: bs[(i*M + k)*nb + b] = plane (i, k) over [bK, bK + K)."""
+    for i in range(rows):
+        for b in range(nb):
+            base = i * m * plen + b * (K + 1)
+            for k in range(m):
+                bs.set((i * m + k) * nb + b, plane.get(base + k * plen + np.arange(K)).sum())
+
+
+def window_start(plane, row_base, plen, bs, bs_base, nb, c0, r, m, K):
+    """window_start<K, M> for an array of segment starts c0 (multiples of K)."""
+    b0, q = c0 // K, (2 * r + 1) // K
+    S = np.zeros((c0.size, m))
+    for b in range(q):
+        for k in range(m):
+            S[:, k] += bs.get(bs_base + k * nb + b0 + b)
+    for j in range(q * K, 2 * r + 1):
+        for k in range(m):
+            S[:, k] += plane.get(row_base + k * plen + sk(c0 + j, K))
+    return S
+
+
 def _load(img, x, y, mask):
     """Input pixels of columns x (where mask) at row y; zero elsewhere."""
     h, w = img.shape[:2]
@@ -112,9 +134,11 @@ def guided_filter(img, r, eps, space=0, NT=256, R=4, K=8, ctas=8):
         m[~mask] = 0
         return m
 
+    nbv, nba = NT // K, c2 // K
     for cta in range(grid):
         vb = Flat(R * 6 * c1p)       # also H2b
         ab = Flat(R * 6 * c2p)
+        bs = Flat(R * 6 * nbv)
         ring = Flat(period * 6 * tw)
         for task in range(cta, tasks, grid):
             band, strip = task // strips, task % strips
@@ -140,14 +164,13 @@ def guided_filter(img, r, eps, space=0, NT=256, R=4, K=8, ctas=8):
                     for k in range(6):
                         vb.set(i * 6 * c1p + k * c1p + sk(tid, K), V[:, k])
                 ab.poison()
+                bs.poison()
+                block_sums(vb, c1p, max(rows, 0), nbv, 6, K, bs)
                 segs = (c2 + K - 1) // K
                 for i in range(max(rows, 0)):           # phase B (lanes = segments)
                     t = tb + i
                     c0 = np.arange(segs) * K
-                    S = np.zeros((segs, 6))
-                    for j in range(2 * r + 1):
-                        for k in range(6):
-                            S[:, k] += vb.get(i * 6 * c1p + k * c1p + sk(c0 + j, K))
+                    S = window_start(vb, i * 6 * c1p, c1p, bs, i * 6 * nbv, nbv, c0, r, 6, K)
                     wy = float(extent(t, r, H))
                     for d in range(K):
                         c = c0 + d
@@ -177,13 +200,12 @@ def guided_filter(img, r, eps, space=0, NT=256, R=4, K=8, ctas=8):
                             ab.set(i * 6 * c2p + ch * c2p + sk(c[inside], K), a)
                             ab.set(i * 6 * c2p + (3 + ch) * c2p + sk(c[inside], K), b)
                 vb.poison()                              # Vb is dead; H2b aliases it
+                bs.poison()
+                block_sums(ab, c2p, max(rows, 0), nba, 6, K, bs)
                 segs_c = (tw + K - 1) // K
                 for i in range(max(rows, 0)):           # phase C
                     o0 = np.arange(segs_c) * K
-                    S = np.zeros((segs_c, 6))
-                    for j in range(2 * r + 1):
-                        for k in range(6):
-                            S[:, k] += ab.get(i * 6 * c2p + k * c2p + sk(o0 + j, K))
+                    S = window_start(ab, i * 6 * c2p, c2p, bs, i * 6 * nba, nba, o0, r, 6, K)
                     for d in range(K):
                         o = o0 + d
                         live = o < tw
@@ -240,9 +262,12 @@ def local_statistics(img, r, NT=256, R=4, K=8, ctas=8):
     cnt = np.full((H, W, 3), -1, np.int64)
     written = np.zeros((H, W), np.int32)
     tid = np.arange(NT)
+    nblk = NT // K
     for cta in range(grid):
         vb = Flat(R * 6 * c1p)
         nb = Flat(R * 3 * c1p, np.int64)
+        bsv = Flat(R * 6 * nblk)
+        bsn = Flat(R * 3 * nblk, np.int64)
         for task in range(cta, tasks, grid):
             band, strip = task // strips, task % strips
             x0, y0 = strip * tw, band * th
@@ -279,17 +304,16 @@ def local_statistics(img, r, NT=256, R=4, K=8, ctas=8):
                         vb.set(i * 6 * c1p + c * c1p + sk(tid, K), s1[:, c])
                         vb.set(i * 6 * c1p + (3 + c) * c1p + sk(tid, K), s2[:, c])
                         nb.set(i * 3 * c1p + c * c1p + sk(tid, K), n[:, c])
+                bsv.poison()
+                bsn.poison()
+                block_sums(vb, c1p, rows, nblk, 6, K, bsv)
+                block_sums(nb, c1p, rows, nblk, 3, K, bsn)
                 segs = (tw + K - 1) // K
                 for i in range(rows):
                     t = tb + i
                     o0 = np.arange(segs) * K
-                    S = np.zeros((segs, 6))
-                    N = np.zeros((segs, 3), np.int64)
-                    for j in range(2 * r + 1):
-                        for k in range(6):
-                            S[:, k] += vb.get(i * 6 * c1p + k * c1p + sk(o0 + j, K))
-                        for c in range(3):
-                            N[:, c] += nb.get(i * 3 * c1p + c * c1p + sk(o0 + j, K))
+                    S = window_start(vb, i * 6 * c1p, c1p, bsv, i * 6 * nblk, nblk, o0, r, 6, K)
+                    N = window_start(nb, i * 3 * c1p, c1p, bsn, i * 3 * nblk, nblk, o0, r, 3, K).astype(np.int64)
                     for d in range(K):
                         o = o0 + d
                         live = o < tw
