@@ -19,7 +19,6 @@ namespace re {
 
 constexpr int BL_TW = 64, BL_TH = 16, BL_THREADS = 256;
 constexpr int BL_SW = BL_TW + 2, BL_SH = BL_TH + 2;
-constexpr int BL_OTILE_OFFSET = (BL_SW * BL_SH * 4 + 15) / 16 * 16;   // staged output in the batch's smem
 
 // Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
 __host__ __device__ constexpr int pat(int l, int k) {
@@ -29,86 +28,91 @@ __host__ __device__ constexpr int pat(int l, int k) {
                     : (k == 1 ? 2 : k == 2 ? 0 : 1);
 }
 
-// Writes a tile's float RGB, staged in shared memory (rows of TW pixels, 3
-// floats each), to the output rows it covers: one warp per row, aligned 16-byte
-// stores in the row's middle and single floats at its two ends, so the 12-byte
-// pixels of a row leave as full, contiguous lines instead of strided scalars.
-template <int TW, int TH, int THREADS>
-__device__ __forceinline__ void store_tile(const float* __restrict__ otile, int x0, int y0, int ox, int oy, int ow,
-                                           int oh, float* __restrict__ out, size_t out_stride) {
-    const int xa = max(x0, ox), xb = min(x0 + TW, ox + ow);
-    if (xa >= xb) return;
-    const int n = 3 * (xb - xa);
-    const int lane = threadIdx.x & 31;
-    for (int row = threadIdx.x >> 5; row < TH; row += THREADS / 32) {
-        const int y = y0 + row;
-        if (y < oy || y >= oy + oh) continue;
-        const float* src = otile + row * (TW * 3) + (xa - x0) * 3;
-        float* dst = out + (size_t)(y - oy) * out_stride + (size_t)(xa - ox) * 3;
-        const int lead = min(n, (int)(((16u - ((unsigned)(uintptr_t)dst & 15u)) & 15u) >> 2));
-        if (lane < lead) dst[lane] = src[lane];
-        const int nv = (n - lead) >> 2;
-        float4* d4 = reinterpret_cast<float4*>(dst + lead);
-        for (int v = lane; v < nv; v += 32) {
-            const float* s4 = src + lead + 4 * v;
-            d4[v] = make_float4(s4[0], s4[1], s4[2], s4[3]);
-        }
-        for (int i = lead + 4 * nv + lane; i < n; i += 32) dst[i] = src[i];
-    }
-}
-
 // Interior tiles of RawEngine.cpp:299-344: every 3x3 neighbourhood is present,
 // so each colour's neighbours and their row-major order are fixed by the
 // quad position -- four edge neighbours (N, W, E, S) or four diagonals at R/B
 // sites, a horizontal or vertical pair at G sites -- and the division by the
-// count (4 or 2, a power of two) is an exact multiply.
+// count (4 or 2, a power of two) is an exact multiply.  A thread renders one
+// 2x2 quad from its 4x4 neighbourhood, read as eight 8-byte shared-memory
+// loads; a warp covers one quad row of the tile.
 template <int L>
-__device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], float* otile, int x0, int y0, int ox,
-                                              int oy, int ow, int oh, int stage_end, const DevProgram& P,
-                                              float* __restrict__ out, size_t out_stride, uint32_t& err) {
+__device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0, int y0, int ox, int oy, int ow,
+                                              int oh, int stage_end, const DevProgram& P, float* __restrict__ out,
+                                              size_t out_stride, uint32_t& err) {
+    // The tile's row span inside the viewport and 16-byte aligned (the same
+    // for the whole block): adjacent lanes pair up per row and the pair's four
+    // pixels (48 bytes) leave as three aligned 16-byte stores.
+    const bool wide = x0 >= ox && x0 + BL_TW <= ox + ow && ((x0 - ox) & 3) == 0 && (out_stride & 3) == 0 &&
+                      (reinterpret_cast<uintptr_t>(out) & 15) == 0;
     for (int q = threadIdx.x; q < (BL_TW / 2) * (BL_TH / 2); q += BL_THREADS) {
         const int qx = q % (BL_TW / 2), qy = q / (BL_TW / 2);
+        float n[4][4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float2 a = *reinterpret_cast<const float2*>(&tile[2 * qy + j][2 * qx]);
+            const float2 b = *reinterpret_cast<const float2*>(&tile[2 * qy + j][2 * qx + 2]);
+            n[j][0] = a.x;
+            n[j][1] = a.y;
+            n[j][2] = b.x;
+            n[j][3] = b.y;
+        }
         float R[4], G[4], B[4];
         bool keep[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int i = k & 1, j = k >> 1;
-            const int tx = 2 * qx + i + 1, ty = 2 * qy + j + 1;
-            const int x = x0 + tx - 1, y = y0 + ty - 1;
+            const int x = x0 + 2 * qx + i, y = y0 + 2 * qy + j;
             const int own = pat(L, k);
+            const float c = n[1 + j][1 + i];
+            const float nn = n[j][1 + i], ss = n[2 + j][1 + i], ww = n[1 + j][i], ee = n[1 + j][2 + i];
             float rgb[3];
-            rgb[own] = tile[ty][tx];
+            rgb[own] = c;
             if (own == 1) {
                 const int row_colour = pat(L, (j << 1) | (i ^ 1));       // colour of the W/E neighbours
-                const float hsum = __fadd_rn(tile[ty][tx - 1], tile[ty][tx + 1]);
-                const float vsum = __fadd_rn(tile[ty - 1][tx], tile[ty + 1][tx]);
-                rgb[row_colour] = __fmul_rn(hsum, 0.5f);
-                rgb[2 - row_colour] = __fmul_rn(vsum, 0.5f);
+                rgb[row_colour] = __fmul_rn(__fadd_rn(ww, ee), 0.5f);
+                rgb[2 - row_colour] = __fmul_rn(__fadd_rn(nn, ss), 0.5f);
             } else {
-                const float edge = __fadd_rn(__fadd_rn(__fadd_rn(tile[ty - 1][tx], tile[ty][tx - 1]), tile[ty][tx + 1]),
-                                             tile[ty + 1][tx]);
-                const float diag = __fadd_rn(__fadd_rn(__fadd_rn(tile[ty - 1][tx - 1], tile[ty - 1][tx + 1]),
-                                                       tile[ty + 1][tx - 1]),
-                                             tile[ty + 1][tx + 1]);
+                const float edge = __fadd_rn(__fadd_rn(__fadd_rn(nn, ww), ee), ss);
+                const float diag =
+                    __fadd_rn(__fadd_rn(__fadd_rn(n[j][i], n[j][2 + i]), n[2 + j][i]), n[2 + j][2 + i]);
                 rgb[1] = __fmul_rn(edge, 0.25f);
                 rgb[2 - own] = __fmul_rn(diag, 0.25f);
             }
             keep[k] = x >= ox && y >= oy && x < ox + ow && y < oy + oh;
+            // pixels outside the viewport enter the stages as zeros (never written)
             R[k] = keep[k] ? rgb[0] : 0.0f;
             G[k] = keep[k] ? rgb[1] : 0.0f;
             B[k] = keep[k] ? rgb[2] : 0.0f;
         }
         apply_stages_n<4, 6>(P, 0, stage_end, R, G, B, err);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            float* o = otile + (2 * qy + (k >> 1)) * (BL_TW * 3) + (2 * qx + (k & 1)) * 3;
-            o[0] = R[k];
-            o[1] = G[k];
-            o[2] = B[k];
+        for (int j = 0; j < 2; ++j) {
+            const int y = y0 + 2 * qy + j;
+            const int a = 2 * j, b = 2 * j + 1;   // the row's two pixels
+            if (wide) {
+                const float p0 = __shfl_down_sync(0xffffffffu, R[a], 1);
+                const float p1 = __shfl_down_sync(0xffffffffu, G[a], 1);
+                if (y < oy || y >= oy + oh) continue;
+                float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x0 - ox) * 3 + 6 * qx;
+                if ((qx & 1) == 0) {
+                    reinterpret_cast<float4*>(o)[0] = make_float4(R[a], G[a], B[a], R[b]);
+                    reinterpret_cast<float4*>(o)[1] = make_float4(G[b], B[b], p0, p1);
+                } else {
+                    *reinterpret_cast<float4*>(o + 2) = make_float4(B[a], R[b], G[b], B[b]);
+                }
+                continue;
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int k = 2 * j + i;
+                if (!keep[k]) continue;
+                float* o = out + (size_t)(y - oy) * out_stride + (size_t)(x0 + 2 * qx + i - ox) * 3;
+                o[0] = R[k];
+                o[1] = G[k];
+                o[2] = B[k];
+            }
         }
     }
-    __syncthreads();
-    store_tile<BL_TW, BL_TH, BL_THREADS>(otile, x0, y0, ox, oy, ow, oh, out, out_stride);
 }
 
 // RawEngine.cpp:299-344.  The normalized samples of the tile and its one-pixel
@@ -116,7 +120,7 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], float*
 // are never read: the reference skips them and counts only present neighbours).
 // Tiles are anchored at even sensor coordinates; interior tiles take the quad
 // path, tiles meeting the active-area edge the general neighbour scan.
-__device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], float* otile, const DevRaw& raw, int x0, int y0,
+__device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw& raw, int x0, int y0,
                                              int ox, int oy, int ow, int oh, int layout, int stage_end,
                                              const DevProgram& P, float* __restrict__ out, size_t out_stride,
                                              uint32_t& err) {
@@ -139,10 +143,10 @@ __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], float* otile,
     __syncthreads();
     if (interior) {
         switch (layout) {
-        case 0: bilinear_fast<0>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 1: bilinear_fast<1>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 2: bilinear_fast<2>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        default: bilinear_fast<3>(tile, otile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
         }
         return;
     }
@@ -187,11 +191,10 @@ __global__ void __launch_bounds__(BL_THREADS, 4)
 bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
-    __shared__ float tile[BL_SH][BL_SW];
-    __shared__ __align__(16) float otile[BL_TH * BL_TW * 3];
+    __shared__ __align__(16) float tile[BL_SH][BL_SW];
     const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
     uint32_t err = 0;
-    bilinear_cta(tile, otile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
+    bilinear_cta(tile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
     report(status, err);
 }
 
@@ -997,9 +1000,8 @@ __device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchP
         menon_cta(smem_raw, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, nullptr, err,
                   POLICY == 1, nullptr);
     else
-        bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw),
-                     reinterpret_cast<float*>(smem_raw + BL_OTILE_OFFSET), raw, x0, y0, ox, oy, ow, oh, layout,
-                     stage_end, P, out, out_stride, err);
+        bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw), raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P,
+                     out, out_stride, err);
 }
 
 __device__ __forceinline__ void prefetch_unit(BatchUnit* dst, const BatchUnit* src) {
@@ -1065,8 +1067,7 @@ static_assert(BL_THREADS == MN_THREADS, "batched tiles share one block size");
 static_assert(BATCH_MENON_TW == MN_TW && BATCH_MENON_TH == MN_TH && BATCH_BILINEAR_TW == BL_TW &&
                   BATCH_BILINEAR_TH == BL_TH,
               "batch planner tile sizes");
-static_assert(sizeof(MenonShared) >= BL_OTILE_OFFSET + sizeof(float) * BL_TH * BL_TW * 3,
-              "bilinear tiles fit the batch's shared memory");
+static_assert(sizeof(MenonShared) >= sizeof(float) * BL_SH * BL_SW, "bilinear tiles fit the batch's shared memory");
 
 static_assert(sizeof(BatchParams) <= 32000, "batch launch parameters exceed the 32 KB kernel parameter limit");
 
