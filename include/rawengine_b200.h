@@ -221,6 +221,15 @@ RE_API size_t re_render_scratch_bytes(const re_image* image, const re_render_des
                                       re_rect viewport, uint32_t mip);
 RE_API re_status re_status_from_device(uint32_t device_status_word);
 
+/* Per-call device scratch of the synchronous entry points (the native
+ * footprint of a reduced render, geometry and filter intermediates, the
+ * differentiable planes) comes from a stream-ordered memory pool that the
+ * library creates on each device and that keeps freed blocks mapped, so
+ * repeated calls of the same size do not map and unmap device memory.  No
+ * counterpart in the reference (its scratch is host memory).  This returns
+ * the pool's idle blocks to the driver; blocks in use are unaffected. */
+RE_API re_status re_release_scratch(void);
+
 /* Reduced-level (mip 1 or 2, Preview) RAW render that allocates no memory.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory while rendering -- a plug-in inside a host application whose
@@ -362,13 +371,14 @@ RE_API size_t re_diff_point_grad_count(uint32_t knots);
  * guided filter (radius 0..64, epsilon [2^-24, 65536], clipped windows with
  * actual counts; at most 65535 rows).  `strength` is one device float.  The
  * backward recomputes every box mean from p and adds d loss / d strength to
- * *dstrength (double, device). */
+ * *dstrength and d loss / d epsilon to *depsilon (doubles, device). */
 RE_API re_status re_diff_detail_forward(const float* p, uint32_t width, uint32_t height, uint32_t radius,
                                         double epsilon, const float* strength, uint32_t working_space, float* out,
                                         void* stream);
 RE_API re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t width, uint32_t height,
                                          uint32_t radius, double epsilon, const float* strength,
-                                         uint32_t working_space, float* dp, double* dstrength, void* stream);
+                                         uint32_t working_space, float* dp, double* dstrength, double* depsilon,
+                                         void* stream);
 
 /* ------------------------------------------------------------- raster I/O */
 

@@ -27,6 +27,7 @@ EXPORTS = [
     "re_camera_to_working_matrix", "re_working_to_srgb_matrix", "re_working_to_working_matrix",
     "re_exposure_multiplier", "re_curve_set_create", "re_curve_set_destroy",
     "re_render_raw", "re_render_raw_async", "re_menon_directions", "re_render_scratch_bytes", "re_status_from_device",
+    "re_release_scratch",
     "re_render_tiles", "re_render_raster", "re_guided_filter", "re_guided_filter_async", "re_guided_filter_scratch_bytes", "re_local_statistics", "re_local_statistics_f64", "re_cubic_resize", "re_rotate",
     "re_cubic_axis", "re_rotation_coefficients", "re_cubic_resize_window", "re_rotate_window",
     "re_rotation_support",
@@ -139,6 +140,7 @@ def lib() -> C.CDLL:
         L.re_render_scratch_bytes.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32]
         L.re_render_scratch_bytes.restype = sz
         L.re_status_from_device.argtypes = [u32]
+        L.re_release_scratch.argtypes = []
         L.re_render_tiles.argtypes = [vp, C.POINTER(RenderDesc), Rect, u32, u32, u32, TILE_CALLBACK, vp, vp]
         L.re_render_raster.argtypes = [vp, sz, u32, u32, C.POINTER(RenderDesc), Rect, u32, u32, vp, sz, vp]
         L.re_guided_filter.argtypes = [vp, sz, vp, sz, u32, u32, u32, C.c_double, u32, vp]
@@ -172,7 +174,7 @@ def lib() -> C.CDLL:
         L.re_diff_point_grad_count.argtypes = [u32]
         L.re_diff_point_grad_count.restype = sz
         L.re_diff_detail_forward.argtypes = [vp, u32, u32, u32, C.c_double, vp, u32, vp, vp]
-        L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, vp, u32, vp, vp, vp]
+        L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, vp, u32, vp, vp, vp, vp]
         _lib = L
     return _lib
 

@@ -52,7 +52,56 @@ re_status cuda_fail(cudaError_t e, const char* where) {
 
 namespace re {
 void set_last_error(const std::string& msg) { g_error = msg; }
+
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
+cudaError_t pool_for_current_device(cudaMemPool_t* out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = ~0ull;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream) {
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = pool_for_current_device(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, bytes, pool, stream);
+}
 }  // namespace re
+
+extern "C" re_status re_release_scratch(void) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    for (cudaMemPool_t pool : g_pools)
+        if (pool) {
+            const cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+            if (e != cudaSuccess) return cuda_fail(e, "release scratch");
+        }
+    return RE_OK;
+}
 
 namespace {
 
@@ -694,7 +743,7 @@ re_status re_render_raw(const re_image* img, const re_render_desc* desc, re_rect
     const size_t head = 256;
     DeviceScratch scratch;
     scratch.s = stream;
-    RE_CUDA(cudaMallocAsync(&scratch.p, head + out_bytes + native_bytes, stream));
+    RE_CUDA(scratch_alloc(&scratch.p, head + out_bytes + native_bytes, stream));
     char* base = static_cast<char*>(scratch.p);
     uint32_t* status = reinterpret_cast<uint32_t*>(base);
     unsigned long long* ties = reinterpret_cast<unsigned long long*>(base + 8);
@@ -749,7 +798,7 @@ re_status re_menon_directions(const re_image* img, uint32_t demosaic, re_rect vi
     const size_t rgb = (size_t)viewport.width * viewport.height * 3 * sizeof(float);
     DeviceScratch scratch;
     scratch.s = stream;
-    RE_CUDA(cudaMallocAsync(&scratch.p, 256 + rgb, stream));
+    RE_CUDA(scratch_alloc(&scratch.p, 256 + rgb, stream));
     char* base = static_cast<char*>(scratch.p);
     RE_CUDA(cudaMemsetAsync(base, 0, 256, stream));
     RE_CUDA(launch_demosaic(demosaic, img->raw, (int)viewport.x, (int)viewport.y, (int)viewport.width,
@@ -781,7 +830,7 @@ re_status re_render_raster(const float* in, size_t in_stride, uint32_t width, ui
     cudaStream_t stream = (cudaStream_t)stream_;
     DeviceScratch scratch;
     scratch.s = stream;
-    RE_CUDA(cudaMallocAsync(&scratch.p, 256, stream));
+    RE_CUDA(scratch_alloc(&scratch.p, 256, stream));
     uint32_t* status = static_cast<uint32_t*>(scratch.p);
     RE_CUDA(cudaMemsetAsync(status, 0, 4, stream));
     RE_CUDA(launch_raster(in, in_stride, (int)width, (int)height, (int)viewport.x, (int)viewport.y,

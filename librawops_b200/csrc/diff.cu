@@ -475,11 +475,11 @@ __global__ void gf_bwd1_kernel(const float* __restrict__ p, const float* __restr
 }
 
 // Backward step 2: from the box sums of step 1 (da, db) to the adjoints of
-// the eight moment means, divided by N for the next box adjoint.
-__global__ void gf_bwd2_kernel(const double* __restrict__ S8, const double* __restrict__ DAB, GfGeom g, double eps,
-                               double* __restrict__ H8) {
-    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (i >= g.plane) return;
+// the eight moment means, divided by N for the next box adjoint.  epsilon
+// enters every centre only through var + eps, so its adjoint is the sum over
+// centres of the variance adjoint; each CTA adds its part to *deps.
+__device__ __forceinline__ double gf_bwd2_centre(const double* __restrict__ S8, const double* __restrict__ DAB,
+                                                 const GfGeom& g, double eps, size_t i, double* __restrict__ H8) {
     const int x = (int)(i % g.w), y = (int)(i / g.w);
     const double n = count_at(g, x, y);
     const Moments M = moments_at(S8, g, i, n, eps);
@@ -500,6 +500,22 @@ __global__ void gf_bwd2_kernel(const double* __restrict__ S8, const double* __re
     dmI -= 2.0 * M.mI * dvar;
     H8[i] = dmI / n;
     H8[g.plane + i] = dvar / n;
+    return dvar;
+}
+
+__global__ void gf_bwd2_kernel(const double* __restrict__ S8, const double* __restrict__ DAB, GfGeom g, double eps,
+                               double* __restrict__ H8, double* __restrict__ deps) {
+    __shared__ double red[8];
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    double part = i < g.plane ? gf_bwd2_centre(S8, DAB, g, eps, i, H8) : 0.0;
+    part = warp_sum(part);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int j = 0; j < (int)(blockDim.x >> 5); ++j) s += red[j];
+        atomicAdd(deps, s);
+    }
 }
 
 __global__ void gf_bwd3_kernel(const float* __restrict__ p, const float* __restrict__ dout,
@@ -644,7 +660,7 @@ re_status re_diff_detail_forward(const float* p, uint32_t w, uint32_t h, uint32_
     const GfGeom g{(int)w, (int)h, (int)radius, (size_t)w * h};
     DScratch sc;
     sc.s = s;
-    DF_CUDA(cudaMallocAsync(&sc.p, (8 + 8 + 8 + 6) * g.plane * sizeof(double), s));
+    DF_CUDA(scratch_alloc(&sc.p, (8 + 8 + 8 + 6) * g.plane * sizeof(double), s));
     double* S8 = (double*)sc.p;
     double* T8 = S8 + 8 * g.plane;
     double* AB = T8 + 8 * g.plane;
@@ -658,16 +674,16 @@ re_status re_diff_detail_forward(const float* p, uint32_t w, uint32_t h, uint32_
 
 re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t w, uint32_t h, uint32_t radius,
                                   double eps, const float* strength, uint32_t space, float* dp, double* dstrength,
-                                  void* stream_) {
+                                  double* depsilon, void* stream_) {
     re_status st = gf_check(w, h, radius, eps, space);
     if (st) return st;
-    if (!p || !dout || !dp || !dstrength || !strength)
+    if (!p || !dout || !dp || !dstrength || !depsilon || !strength)
         return df_fail(RE_INVALID_ARGUMENT, "null image, strength or gradient");
     cudaStream_t s = (cudaStream_t)stream_;
     const GfGeom g{(int)w, (int)h, (int)radius, (size_t)w * h};
     DScratch sc;
     sc.s = s;
-    DF_CUDA(cudaMallocAsync(&sc.p, (8 + 8 + 8 + 6 + 8) * g.plane * sizeof(double), s));
+    DF_CUDA(scratch_alloc(&sc.p, (8 + 8 + 8 + 6 + 8) * g.plane * sizeof(double), s));
     double* S8 = (double*)sc.p;
     double* T8 = S8 + 8 * g.plane;
     double* W8 = T8 + 8 * g.plane;      // prepared planes, then a/b, then step-1 and step-2 planes
@@ -678,7 +694,7 @@ re_status re_diff_detail_backward(const float* p, const float* dout, uint32_t w,
     gf_forward_planes(p, g, yw, eps, S8, T8, W8, SAB, s);       // the means, recomputed
     gf_bwd1_kernel<<<blocks, 256, 0, s>>>(p, dout, SAB, g, yw, strength, W8, dstrength);
     box(W8, T8, B8, g, 6, s);                                   // da, db
-    gf_bwd2_kernel<<<blocks, 256, 0, s>>>(S8, B8, g, eps, W8);
+    gf_bwd2_kernel<<<blocks, 256, 0, s>>>(S8, B8, g, eps, W8, depsilon);
     box(W8, T8, B8, g, 8, s);
     gf_bwd3_kernel<<<blocks, 256, 0, s>>>(p, dout, SAB, B8, g, yw, strength, dp);
     DF_CUDA(cudaGetLastError());

@@ -367,7 +367,7 @@ re_status re_cubic_resize_window(const float* in, size_t in_stride, re_rect wind
     const size_t nat_bytes = mip ? (size_t)native.width * native.height * 3 * sizeof(float) : 0;
     Scratch sc;
     sc.s = stream;
-    GEO_CUDA(cudaMallocAsync(&sc.p, 256 + axes_bytes + h_bytes + nat_bytes, stream));
+    GEO_CUDA(scratch_alloc(&sc.p, 256 + axes_bytes + h_bytes + nat_bytes, stream));
     char* base = (char*)sc.p;
     uint32_t* status = (uint32_t*)base;
     Axis* dax = (Axis*)(base + 256);
@@ -466,7 +466,7 @@ re_status re_rotate_window(const float* in, size_t in_stride, re_rect window, ui
     const size_t nat_bytes = mip ? (size_t)native.width * native.height * 3 * sizeof(float) : 0;
     Scratch sc;
     sc.s = stream;
-    GEO_CUDA(cudaMallocAsync(&sc.p, 256 + nat_bytes, stream));
+    GEO_CUDA(scratch_alloc(&sc.p, 256 + nat_bytes, stream));
     uint32_t* status = (uint32_t*)sc.p;
     float* nat = (float*)((char*)sc.p + 256);
     GEO_CUDA(cudaMemsetAsync(status, 0, 4, stream));

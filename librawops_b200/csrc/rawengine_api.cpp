@@ -33,6 +33,11 @@
 #include "rawengine/Operators.hpp"
 #include "rawengine_b200.h"
 
+namespace re {
+// The library's stream-ordered scratch pool (capi.cu).
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
+}  // namespace re
+
 namespace rawengine {
 
 // ------------------------------------------------------------- errors
@@ -645,7 +650,7 @@ struct DevImage {
     cudaStream_t stream = nullptr;
     DevImage(Rect r, cudaStream_t s) : stride((size_t)r.width * 3), bounds(r), stream(s) {
         if (r.width && r.height)
-            check_cuda(cudaMallocAsync((void**)&data, (size_t)r.width * r.height * 3 * sizeof(float), s),
+            check_cuda(re::scratch_alloc((void**)&data, (size_t)r.width * r.height * 3 * sizeof(float), s),
                        "device tile");
     }
     ~DevImage() {
@@ -1062,7 +1067,7 @@ LocalStatisticsTile local_statistics_rgb(const Tile& input, Rect output, Rect im
     const size_t n_needed = (size_t)needed.width * needed.height * 3;
     DevImage in(needed, s);
     void* scratch = nullptr;
-    check_cuda(cudaMallocAsync(&scratch, n_needed * (2 * sizeof(double) + sizeof(uint32_t)), s), "statistics");
+    check_cuda(re::scratch_alloc(&scratch, n_needed * (2 * sizeof(double) + sizeof(uint32_t)), s), "statistics");
     double* mean = (double*)scratch;
     double* var = mean + n_needed;
     uint32_t* count = (uint32_t*)(var + n_needed);
@@ -1195,7 +1200,7 @@ std::string desc_key(const re_render_desc& d) {
 // default stream once the last tile that points into it is released.
 std::shared_ptr<float> device_block(size_t bytes, cudaStream_t s) {
     float* p = nullptr;
-    if (bytes) check_cuda(cudaMallocAsync((void**)&p, bytes, s), "scheduler output");
+    if (bytes) check_cuda(re::scratch_alloc((void**)&p, bytes, s), "scheduler output");
     return std::shared_ptr<float>(p, [](float* q) {
         if (q) cudaFreeAsync(q, nullptr);
     });

@@ -234,4 +234,11 @@ struct DevProgram {
 constexpr uint32_t KEY_GUARD = (511u << 8) | ST_GUARD;
 constexpr uint32_t KEY_TIMEOUT = (511u << 8) | ST_TIMEOUT;
 
+// Per-call device scratch, stream-ordered, from a memory pool the library
+// owns on each device (capi.cu).  The pool keeps freed blocks mapped (its
+// release threshold is unlimited), so steady-state calls neither map nor
+// unmap device memory; re_release_scratch() returns the idle blocks.  Free
+// with cudaFreeAsync on a stream ordered after the last use.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
+
 }  // namespace re

@@ -738,7 +738,7 @@ re_status re_guided_filter(const float* in, size_t in_stride, float* out, size_t
                                  sm_count());
     Scratch sc;
     sc.s = stream;
-    SP_CUDA(cudaMallocAsync(&sc.p, 256 + gf_ring_bytes(L), stream));
+    SP_CUDA(scratch_alloc(&sc.p, 256 + gf_ring_bytes(L), stream));
     uint32_t* status = (uint32_t*)sc.p;
     SP_CUDA(cudaMemsetAsync(status, 0, 4, stream));
     s = gf_enqueue(L, static_cast<char*>(sc.p) + 256, status, stream);

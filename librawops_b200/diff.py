@@ -1,7 +1,7 @@
 """Differentiable render: torch.autograd Functions over the CUDA adjoints.
 
     plane (h, w)  --BilinearDemosaic-->  camera RGB  --PointStages(wb, stops,
-    matrix, curve knots)-->  working RGB  --DetailBoost(strength)-->  out
+    matrix, curve knots)-->  working RGB  --DetailBoost(strength, eps)-->  out
 
 Each Function's forward and backward are the hand-written kernels of
 csrc/diff.cu (include/rawengine_b200.h, re_diff_*), launched on torch's current
@@ -14,6 +14,7 @@ parameters; `fit_recipe` fits them to a target render with Adam.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import torch
 
@@ -126,30 +127,34 @@ def point_stages(x, wb, stops, matrix, kx, ky):
 # -------------------------------------------------------------- detail boost
 
 class DetailBoost(torch.autograd.Function):
-    """out = v + strength (v - GF(v)), GF the self-guided working-Y guided filter."""
+    """out = v + strength (v - GF(v)), GF the self-guided working-Y guided filter.
+
+    `eps` is a one-element float64 tensor: the kernels take its value by value
+    (read on the host once per call) and the backward returns its gradient."""
 
     @staticmethod
-    def forward(ctx, v, strength, radius: int, eps: float, space: int):
+    def forward(ctx, v, strength, eps, radius: int, space: int):
         v = v.contiguous()
         h, w = v.shape[:2]
         k = strength.detach().float().reshape(1).contiguous()
+        e = float(eps.detach())
         out = torch.empty_like(v)
-        check(lib().re_diff_detail_forward(_ptr(v), w, h, radius, eps, _ptr(k), space, _ptr(out), _stream()))
+        check(lib().re_diff_detail_forward(_ptr(v), w, h, radius, e, _ptr(k), space, _ptr(out), _stream()))
         ctx.save_for_backward(v, k)
-        ctx.args = (radius, eps, space)
+        ctx.args = (radius, e, space, eps.dtype)
         return out
 
     @staticmethod
     def backward(ctx, grad):
         v, k = ctx.saved_tensors
-        radius, eps, space = ctx.args
+        radius, e, space, eps_dtype = ctx.args
         h, w = v.shape[:2]
         grad = grad.contiguous()
         dv = torch.empty_like(v)
-        dk = torch.zeros(1, dtype=torch.float64, device=v.device)
-        check(lib().re_diff_detail_backward(_ptr(v), _ptr(grad), w, h, radius, eps, _ptr(k), space, _ptr(dv),
-                                            _ptr(dk), _stream()))
-        return dv, dk.float()[0], None, None, None
+        dk = torch.zeros(2, dtype=torch.float64, device=v.device)     # d strength, d eps
+        check(lib().re_diff_detail_backward(_ptr(v), _ptr(grad), w, h, radius, e, _ptr(k), space, _ptr(dv),
+                                            _ptr(dk), C.c_void_p(dk.data_ptr() + 8), _stream()))
+        return dv, dk[0].float(), dk[1].to(eps_dtype), None, None
 
 
 # --------------------------------------------------------------------- model
@@ -157,14 +162,16 @@ class DetailBoost(torch.autograd.Function):
 class RecipeModel(torch.nn.Module):
     """The differentiable render with learnable recipe parameters: WB gains,
     exposure stops, the 3x3 camera->working matrix, the master-curve knot values
-    (knot positions fixed) and the detail-boost strength."""
+    (knot positions fixed), the detail-boost strength and the guided filter's
+    epsilon (learned as its natural logarithm, float64, so that it stays
+    positive)."""
 
     def __init__(self, quad, kx, ky, wb=(1.0, 1.0, 1.0), stops=0.0, matrix=None, strength=0.0, radius=16,
                  eps=1e-3, space=PROPHOTO, device="cuda"):
         super().__init__()
         f = dict(dtype=torch.float32, device=device)
         self.quad = quad_code(quad)
-        self.radius, self.eps, self.space = radius, eps, space
+        self.radius, self.space = radius, space
         self.register_buffer("kx", torch.tensor(kx, **f))
         self.wb = torch.nn.Parameter(torch.tensor(wb, **f))
         self.stops = torch.nn.Parameter(torch.tensor(float(stops), **f))
@@ -172,11 +179,16 @@ class RecipeModel(torch.nn.Module):
         self.matrix = torch.nn.Parameter(m.to(**f).clone())
         self.ky = torch.nn.Parameter(torch.tensor(ky, **f))
         self.strength = torch.nn.Parameter(torch.tensor(float(strength), **f))
+        self.log_eps = torch.nn.Parameter(torch.tensor(math.log(eps), dtype=torch.float64, device=device))
+
+    @property
+    def eps(self) -> float:
+        return math.exp(float(self.log_eps.detach()))
 
     def forward(self, plane):
         x = BilinearDemosaic.apply(plane, self.quad)
         v = point_stages(x, self.wb, self.stops, self.matrix, self.kx, self.ky)
-        return DetailBoost.apply(v, self.strength, self.radius, self.eps, self.space)
+        return DetailBoost.apply(v, self.strength, torch.exp(self.log_eps), self.radius, self.space)
 
 
 def fit_recipe(model: RecipeModel, planes, targets, steps: int = 200, lr: float = 0.01, params=None):

@@ -238,7 +238,8 @@ def detail_forward(p: np.ndarray, r: int, eps: float, k: float, space: int = 0) 
 
 
 def detail_backward(p: np.ndarray, dout: np.ndarray, r: int, eps: float, k: float, space: int = 0):
-    """Returns (dp, dk)."""
+    """Returns (dp, dk, deps).  epsilon enters each centre only through
+    var + eps, so d/d eps is the sum over centres of the variance adjoint."""
     q, (n, I, mI, mII, mp, mIp, var, cov, a, b, ma, mb) = guided_forward(p, r, eps, space)
     dk = float(((p - q) * dout).sum())
     dq = -k * dout
@@ -252,6 +253,7 @@ def detail_backward(p: np.ndarray, dout: np.ndarray, r: int, eps: float, k: floa
     dmI = -(db * a).sum(-1)
     dcov = dA * inv[..., None]
     dvar = -(dA * cov).sum(-1) * inv * inv
+    deps = float(dvar.sum())
     dmIp = dcov
     dmI += -(dcov * mp).sum(-1)
     dmp += -dcov * mI[..., None]
@@ -265,7 +267,7 @@ def detail_backward(p: np.ndarray, dout: np.ndarray, r: int, eps: float, k: floa
     dI += BI + 2 * I * BII + (p * BIp).sum(-1)
     wr, wb = Y_WEIGHTS[space]
     dp += dI[..., None] * np.array([wr, 1 - wr - wb, wb])[None, None, :]
-    return dp, dk
+    return dp, dk, deps
 
 
 # ----------------------------------------------------------------- full model
@@ -277,10 +279,10 @@ def render_forward(s, quad, wb, stops, M, kx, ky, r, eps, k, space=0):
 
 
 def render_backward(s, dout, quad, wb, stops, M, kx, ky, r, eps, k, space=0):
-    """Gradients of sum(dout * render) w.r.t. (s, wb, stops, M, ky, k)."""
+    """Gradients of sum(dout * render) w.r.t. (s, wb, stops, M, ky, k, eps)."""
     x = bilinear_forward(s, quad)
     v = point_forward(x, wb, stops, M, kx, ky)
-    dv, dk = detail_backward(v, dout, r, eps, k, space)
+    dv, dk, deps = detail_backward(v, dout, r, eps, k, space)
     dx, dwb, dstops, dM, dky = point_backward(x, dv, wb, stops, M, kx, ky)
     ds = bilinear_backward(dx, quad)
-    return ds, dwb, dstops, dM, dky, dk
+    return ds, dwb, dstops, dM, dky, dk, deps

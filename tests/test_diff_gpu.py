@@ -1,11 +1,13 @@
 """The CUDA adjoints of the differentiable render (librawops_b200.diff) on a B200.
 
 Gradients of sum(dout * render) with respect to the sensor plane, WB, exposure
-stops, the 3x3 matrix, the curve knot values and the detail-boost strength are
-checked against the float64 CPU adjoint (oracle/diff_oracle.py, itself pinned
-to central differences) and directly against FP64 central finite differences
-(step 1e-3), both within 1e-3 relative; a 200-step Adam fit recovers a hidden
-recipe from its target render.
+stops, the 3x3 matrix, the curve knot values, the detail-boost strength and
+the guided filter's epsilon are checked against the float64 CPU adjoint
+(oracle/diff_oracle.py, itself pinned to central differences) and directly
+against FP64 central finite differences (step 1e-3; 1e-3 of epsilon for
+epsilon), both within 1e-3 relative.  Adam fits recover a hidden recipe from
+its target renders, at radius 4 and at radius 16 on 192x256 frames, where the
+recovered parameters themselves are checked.
 """
 import numpy as np
 import pytest
@@ -52,8 +54,9 @@ def test_gradients_match_cpu_adjoint_and_central_differences():
     want_out = D.render_forward(plane.astype(np.float64), **args)
     assert _rel(out.detach().cpu().numpy(), want_out) < 1e-5
     ref = D.render_backward(plane.astype(np.float64), dout, **args)
-    got = [p.grad, m.wb.grad, m.stops.grad, m.matrix.grad, m.ky.grad, m.strength.grad]
-    names = ["plane", "wb", "stops", "matrix", "ky", "strength"]
+    # the model learns log(eps): d/d log(eps) = eps d/d eps
+    got = [p.grad, m.wb.grad, m.stops.grad, m.matrix.grad, m.ky.grad, m.strength.grad, m.log_eps.grad / m.eps]
+    names = ["plane", "wb", "stops", "matrix", "ky", "strength", "eps"]
     for name, g, r in zip(names, got, ref):
         assert _rel(g.detach().cpu().numpy(), r) < 1e-3, name
 
@@ -71,6 +74,9 @@ def test_gradients_match_cpu_adjoint_and_central_differences():
     assert _rel(float(m.stops.grad), fd_stops) < 1e-3
     fd_k = (f(k=args["k"] + step) - f(k=args["k"] - step)) / (2 * step)
     assert _rel(float(m.strength.grad), fd_k) < 1e-3
+    e_step = 1e-3 * args["eps"]
+    fd_eps = (f(eps=args["eps"] + e_step) - f(eps=args["eps"] - e_step)) / (2 * e_step)
+    assert _rel(float(m.log_eps.grad) / args["eps"], fd_eps) < 1e-3
     fd_m = np.zeros((3, 3))
     for i in range(3):
         for j in range(3):
@@ -123,3 +129,30 @@ def test_fit_recipe_recovers_hidden_parameters():
     params = [model.wb, model.stops, model.ky, model.strength]
     history = diff.fit_recipe(model, frames, targets, steps=200, lr=0.02, params=params)
     assert history[-1] < 1e-3 * history[0], (history[0], history[-1])
+
+
+def test_fit_recipe_recovers_hidden_parameters_at_radius_16():
+    """Radius 16 on three 192x256 frames: the red and blue gains, every knot
+    value, the strength and epsilon come back from the target renders.  The
+    green gain and the exposure are held at the hidden values: a common scale
+    of the curve's input is otherwise interchangeable with moved knots, so the
+    fit could match the renders without recovering either."""
+    from librawops_b200 import diff
+    torch.manual_seed(0)
+    frames = [torch.tensor(_case(192, 256, seed=s)[0], device="cuda") for s in range(3)]
+    hidden = _model(radius=16, strength=0.6, wb=(2.1, 1.0, 1.35), stops=0.25)
+    with torch.no_grad():
+        targets = [hidden(f) for f in frames]
+    model = diff.RecipeModel(QUAD, KX, KY, wb=(1.6, 1.0, 1.7), stops=0.25, matrix=MATRIX, strength=0.2, radius=16,
+                             eps=3e-3)
+    with torch.no_grad():
+        model.ky.copy_(torch.tensor(KY, device="cuda") * 0.9)
+    model.wb.register_hook(lambda g: g * torch.tensor([1.0, 0.0, 1.0], device=g.device))
+    params = [model.wb, model.ky, model.strength, model.log_eps]
+    history = diff.fit_recipe(model, frames, targets, steps=250, lr=0.02, params=params)
+    assert history[-1] < 1e-4 * history[0], (history[0], history[-1])
+    wb = model.wb.detach().cpu().numpy()
+    assert np.all(np.abs(wb / np.array([2.1, 1.0, 1.35]) - 1) < 0.01), wb
+    assert abs(float(model.strength) - 0.6) < 0.02, float(model.strength)
+    assert np.max(np.abs(model.ky.detach().cpu().numpy() - np.array(KY))) < 0.01
+    assert abs(np.log(model.eps / 1e-3)) < 0.25, model.eps

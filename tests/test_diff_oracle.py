@@ -51,3 +51,16 @@ def test_bilinear_adjoint_is_transpose():
         lhs = float((D.bilinear_forward(s, quad) * d).sum())
         rhs = float((s * D.bilinear_backward(d, quad)).sum())
         assert abs(lhs - rhs) < 1e-10 * max(1.0, abs(lhs))
+
+
+def test_eps_adjoint_matches_central_differences():
+    c = _case(seed=2)
+    quad, kx, r, dout = c["quad"], c["kx"], c["r"], c["dout"]
+    for eps in (1e-4, 1e-3, 1e-2):
+        def f(e):
+            return float((D.render_forward(c["s"], quad, c["wb"], c["stops"], c["M"], kx, c["ky"], r, e, c["k"])
+                          * dout).sum())
+        g = D.render_backward(c["s"], dout, quad, c["wb"], c["stops"], c["M"], kx, c["ky"], r, eps, c["k"])[6]
+        step = 1e-4 * eps
+        fd = (f(eps + step) - f(eps - step)) / (2 * step)
+        assert abs(g - fd) <= 1e-6 * abs(fd), (eps, g, fd)
