@@ -460,6 +460,29 @@ RE_API re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, 
 /* GeometryOps.cpp:46-67 rotation constants (host). */
 RE_API re_status re_rotation_coefficients(double angle_degrees, double* cosine, double* sine);
 
+/* ------------------------------------------------------------------ analysis */
+
+/* histogram_rgb (ImageAnalysis.cpp:9-69) over a DEVICE float32 RGB image:
+ * per channel `bins` equal bins over [lower, upper] (the last includes upper;
+ * bin = min(bins-1, uint32((double(s) - lower) / (upper - lower) * bins))),
+ * under/overflow and non-finite tallies, and the extrema of all finite
+ * samples.  Accumulates into DEVICE counters, so an image may be passed in
+ * pieces: counts (3 * bins, R then G then B), tallies (underflow[3],
+ * overflow[3], nonfinite[3]) and extrema (min key[3], max key[3]), all
+ * uint64.  re_histogram_reset clears them.  The pieces' pixels are numbered
+ * in the reference's tile traversal (tiles of tile_size, row-major, pixels
+ * row-major in a tile; tile_size 0 = one tile) starting at first_index, and
+ * among equal extrema (+0 and -0) the earliest in that order wins, as in the
+ * reference.  re_histogram_extremum decodes a key (host): returns 0 when the
+ * channel had no finite sample.  Enqueued on `stream`; no host sync. */
+RE_API re_status re_histogram_reset(uint32_t bins, uint64_t* counts, uint64_t* tallies, uint64_t* extrema,
+                                    void* stream);
+RE_API re_status re_histogram_rgb(const float* rgb, size_t row_stride, uint32_t width, uint32_t height,
+                                  uint32_t tile_size, uint64_t first_index, uint32_t bins, double lower,
+                                  double upper, uint64_t* counts, uint64_t* tallies, uint64_t* extrema,
+                                  void* stream);
+RE_API int re_histogram_extremum(uint64_t key, int is_max, float* value);
+
 #ifdef __cplusplus
 }
 #endif

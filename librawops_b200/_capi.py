@@ -37,6 +37,7 @@ EXPORTS = [
     "re_batch_info_get", "re_batch_autotune",
     "re_diff_bilinear_forward", "re_diff_bilinear_backward", "re_diff_point_forward", "re_diff_point_backward",
     "re_diff_point_grad_count", "re_diff_detail_forward", "re_diff_detail_backward",
+    "re_histogram_reset", "re_histogram_rgb", "re_histogram_extremum",
 ]
 
 
@@ -175,6 +176,11 @@ def lib() -> C.CDLL:
         L.re_diff_point_grad_count.restype = sz
         L.re_diff_detail_forward.argtypes = [vp, u32, u32, u32, C.c_double, vp, u32, vp, vp]
         L.re_diff_detail_backward.argtypes = [vp, vp, u32, u32, u32, C.c_double, vp, u32, vp, vp, vp, vp]
+        L.re_histogram_reset.argtypes = [u32, vp, vp, vp, vp]
+        L.re_histogram_rgb.argtypes = [vp, sz, u32, u32, u32, C.c_uint64, u32, C.c_double, C.c_double, vp, vp, vp,
+                                       vp]
+        L.re_histogram_extremum.argtypes = [C.c_uint64, C.c_int, C.POINTER(C.c_float)]
+        L.re_histogram_extremum.restype = C.c_int
         _lib = L
     return _lib
 

@@ -30,6 +30,7 @@
 
 #include <cuda_runtime.h>
 
+#include "rawengine/ImageAnalysis.hpp"
 #include "rawengine/Operators.hpp"
 #include "rawengine_b200.h"
 
@@ -1131,6 +1132,125 @@ void analyze_local_rgb(const Node& output, Rect native_bounds, const RenderReque
 void analyze_local_rgb(const ImageGraph& graph, const RenderRequest& request, const LocalStatisticsCallback& callback,
                        std::uint32_t radius, const CancellationToken* cancellation) {
     analyze_local_rgb(graph.output(), graph.source_bounds(), request, callback, radius, cancellation);
+}
+
+// ---------------------------------------------------------- ImageAnalysis
+
+namespace {
+
+// Device counters of one histogram: counts[3 * bins], tallies[9], extrema[6].
+struct HistogramCounters {
+    uint64_t* base = nullptr;
+    uint32_t bins;
+    cudaStream_t s;
+    HistogramCounters(uint32_t b, cudaStream_t stream) : bins(b), s(stream) {
+        check_cuda(re::scratch_alloc((void**)&base, ((size_t)3 * bins + 15) * sizeof(uint64_t), s), "histogram");
+        check(re_histogram_reset(bins, counts(), tallies(), extrema(), s));
+    }
+    ~HistogramCounters() {
+        if (base) cudaFreeAsync(base, s);
+    }
+    uint64_t* counts() const { return base; }
+    uint64_t* tallies() const { return base + (size_t)3 * bins; }
+    uint64_t* extrema() const { return base + (size_t)3 * bins + 9; }
+};
+
+// Rows of device scratch per band: whole tile rows, about 24 MiB, so that a
+// band written by the render is still in L2 when the histogram reads it.
+constexpr uint64_t kHistogramBandBytes = 24ull << 20;
+
+}  // namespace
+
+// ImageAnalysis.cpp:9-69
+RgbHistogram histogram_rgb(const Node& output, Rect source_bounds, const RenderRequest& request,
+                           const HistogramOptions& options, const CancellationToken* cancellation) {
+    const double span = options.upper - options.lower;
+    if (options.bins == 0 || options.bins > 65536 || !std::isfinite(options.lower) || !std::isfinite(options.upper) ||
+        !(span > 0.0) || !std::isfinite(span))
+        throw std::invalid_argument("histogram requires 1..65536 bins and a finite positive range");
+    auto check_cancelled = [&] {
+        if (cancellation && cancellation->is_cancelled()) throw RenderCancelled();
+    };
+    check_cancelled();
+    RgbHistogram result;
+    result.request = request;
+    result.options = options;
+    result.descriptor = output.output_descriptor();
+    if (result.descriptor.format != PixelFormat::RGBFloat32)
+        throw std::invalid_argument("histogram requires RGBFloat32 output");
+    const Rect vp = request.viewport;
+    const uint64_t right = (uint64_t)vp.x + vp.width, bottom = (uint64_t)vp.y + vp.height;
+    if (!vp.width || !vp.height || right > (1ull << 32) || bottom > (1ull << 32))
+        throw std::invalid_argument("histogram requires a nonempty addressable viewport");
+    validate_request(output, source_bounds, request, nullptr);
+    if (!request.tile_size) throw std::invalid_argument("callback and tile size are required");
+    const uint32_t T = request.tile_size;
+    cudaStream_t s = thread_stream();
+    HistogramCounters hc(options.bins, s);
+    auto count = [&](const float* rgb, size_t stride, uint32_t w, uint32_t h, uint32_t tile, uint64_t first) {
+        check(re_histogram_rgb(rgb, stride, w, h, tile, first, options.bins, options.lower, options.upper,
+                               hc.counts(), hc.tallies(), hc.extrema(), s));
+    };
+    if (dynamic_cast<const DeviceNode*>(&output)) {
+        const uint64_t row_bytes = (uint64_t)vp.width * 3 * sizeof(float);
+        const uint64_t band = std::max<uint64_t>(T, kHistogramBandBytes / row_bytes / T * T);
+        Executor ex{s, cancellation};
+        for (uint64_t y = vp.y; y < bottom; y += band) {
+            check_cancelled();
+            const Rect r{vp.x, (uint32_t)y, vp.width, (uint32_t)std::min<uint64_t>(band, bottom - y)};
+            DevPtr img = ex.eval(output, r, request.level);
+            count(img->data, img->stride, r.width, r.height, T, (y - vp.y) * vp.width);
+        }
+    } else {
+        // The reference's tile stream with its checks on each delivered tile.
+        uint64_t next_x = vp.x, next_y = vp.y, first = 0;
+        Renderer{}.render_tiles(output, source_bounds, request, [&](const Tile& tile) {
+            check_cancelled();
+            const Rect expected{(uint32_t)next_x, (uint32_t)next_y,
+                                (uint32_t)std::min<uint64_t>(T, right - next_x),
+                                (uint32_t)std::min<uint64_t>(T, bottom - next_y)};
+            const uint64_t pixels = (uint64_t)expected.width * expected.height;
+            if (!same(tile.bounds, expected) || tile.rgb.size() % 3 != 0 || tile.rgb.size() / 3 != pixels ||
+                tile.descriptor != result.descriptor)
+                throw std::invalid_argument("histogram received inconsistent tile bounds, storage or descriptor");
+            DevImage dev(expected, s);
+            check_cuda(cudaMemcpyAsync(dev.data, tile.rgb.data(), tile.rgb.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, s),
+                       "histogram tile");
+            count(dev.data, dev.stride, expected.width, expected.height, 0, first);
+            first += pixels;
+            next_x += expected.width;
+            if (next_x == right) {
+                next_x = vp.x;
+                next_y += expected.height;
+            }
+            check_cancelled();
+        }, cancellation);
+    }
+    std::vector<uint64_t> host((size_t)3 * options.bins + 15);
+    check_cuda(cudaMemcpyAsync(host.data(), hc.base, host.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost, s),
+               "histogram");
+    check_cuda(cudaStreamSynchronize(s), "histogram");
+    check_cancelled();
+    const uint64_t* tallies = host.data() + (size_t)3 * options.bins;
+    const uint64_t* keys = tallies + 9;
+    for (int c = 0; c < 3; ++c) {
+        ChannelHistogram& ch = result.channels[c];
+        ch.counts.assign(host.begin() + (size_t)c * options.bins, host.begin() + (size_t)(c + 1) * options.bins);
+        ch.underflow = tallies[c];
+        ch.overflow = tallies[3 + c];
+        ch.nonfinite = tallies[6 + c];
+        float v = 0;
+        if (re_histogram_extremum(keys[c], 0, &v)) ch.minimum = v;
+        if (re_histogram_extremum(keys[3 + c], 1, &v)) ch.maximum = v;
+    }
+    result.pixel_count = (uint64_t)vp.width * vp.height;
+    return result;
+}
+
+RgbHistogram histogram_rgb(const ImageGraph& graph, const RenderRequest& request, const HistogramOptions& options,
+                           const CancellationToken* cancellation) {
+    return histogram_rgb(graph.output(), graph.source_bounds(), request, options, cancellation);
 }
 
 // ----------------------------------------------------------- TileScheduler

@@ -458,6 +458,35 @@ def local_statistics(rgb, radius: int, with_count: bool = False, stream=None):
     return (mean, var, cnt) if with_count else (mean, var)
 
 
+def histogram_rgb(rgb, bins: int = 256, lower: float = 0.0, upper: float = 1.0, tile_size: int = 0, stream=None):
+    """histogram_rgb of a CUDA float tensor (h, w, 3) rendered as one viewport
+    whose tiles are tile_size (0: one tile), the order that decides between
+    equal extrema.  Returns per channel a dict with counts (numpy uint64),
+    underflow, overflow, nonfinite, minimum and maximum (None when absent)."""
+    import torch
+    h, w = int(rgb.shape[0]), int(rgb.shape[1])
+    dev = rgb.device
+    counts = torch.empty(3 * bins, dtype=torch.int64, device=dev)
+    tallies = torch.empty(9, dtype=torch.int64, device=dev)
+    extrema = torch.empty(6, dtype=torch.int64, device=dev)
+    s = C.c_void_p(_stream_ptr(stream))
+    check(lib().re_histogram_reset(bins, _dev(counts), _dev(tallies), _dev(extrema), s))
+    check(lib().re_histogram_rgb(_dev(rgb), rgb.stride(0), w, h, tile_size, 0, bins, float(lower), float(upper),
+                                 _dev(counts), _dev(tallies), _dev(extrema), s))
+    counts = counts.cpu().numpy().view(np.uint64).reshape(3, bins)
+    tallies = tallies.cpu().numpy().view(np.uint64)
+    keys = extrema.cpu().numpy().view(np.uint64)
+    out = []
+    for c in range(3):
+        ext = []
+        for k, is_max in ((keys[c], 0), (keys[3 + c], 1)):
+            v = C.c_float()
+            ext.append(v.value if lib().re_histogram_extremum(int(k), is_max, C.byref(v)) else None)
+        out.append(dict(counts=counts[c], underflow=int(tallies[c]), overflow=int(tallies[3 + c]),
+                        nonfinite=int(tallies[6 + c]), minimum=ext[0], maximum=ext[1]))
+    return out
+
+
 def cubic_resize(rgb, out_w: int, out_h: int, output=None, mip: int = 0, stream=None):
     h, w = int(rgb.shape[0]), int(rgb.shape[1])
     output = output or (0, 0, *request_bounds((0, 0, out_w, out_h), mip, PREVIEW if mip else FINAL)[2:])

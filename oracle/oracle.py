@@ -434,6 +434,40 @@ class Oracle:
 
 # ------------------------------------------------------------------------ reference
 
+def histogram_rgb(rgb, bins=256, lower=0.0, upper=1.0, tile=0):
+    """NumPy restatement of histogram_rgb (ImageAnalysis.cpp:9-69) over an
+    (h, w, 3) float32 image rendered as one viewport in tiles of `tile` (0: one
+    tile).  Bins: min(bins - 1, uint32((double(s) - lower) / span * bins)) in
+    binary64; extrema over finite samples, the first in tile traversal order
+    among equal values (which decides between +0 and -0)."""
+    rgb = np.asarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    t = tile or max(h, w)
+    order = []
+    for y0 in range(0, h, t):
+        for x0 in range(0, w, t):
+            order.append(rgb[y0:y0 + t, x0:x0 + t].reshape(-1, 3))
+    flat = np.concatenate(order) if order else np.zeros((0, 3), np.float32)
+    span = upper - lower
+    out = []
+    for c in range(3):
+        v = flat[:, c]
+        fin = np.isfinite(v)
+        d = v[fin].astype(np.float64)
+        under, over = d < lower, d > upper
+        mid = d[~under & ~over]
+        idx = np.minimum(bins - 1, ((mid - lower) / span * bins).astype(np.uint64))
+        counts = np.bincount(idx.astype(np.int64), minlength=bins).astype(np.uint64)
+        fv = v[fin]
+        mn = mx = None
+        if fv.size:
+            mn = float(fv[int(np.argmax(fv == fv.min()))])
+            mx = float(fv[int(np.argmax(fv == fv.max()))])
+        out.append(dict(counts=counts, underflow=int(under.sum()), overflow=int(over.sum()),
+                        nonfinite=int((~fin).sum()), minimum=mn, maximum=mx))
+    return out
+
+
 class Reference:
     """The unmodified reference library (oracle/_ref), through ref_shim.cpp."""
 
@@ -466,6 +500,10 @@ class Reference:
                                                u32p]
         L.refshim_guided_filter.argtypes = [f32p, u32p, u32p, u32p, C.c_uint32, C.c_double, C.c_int,
                                             f32p]
+        L.refshim_histogram_raster.argtypes = [C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t, i32p, C.c_int,
+                                               f64p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                               C.c_double, C.c_double, C.POINTER(C.c_uint64),
+                                               C.POINTER(C.c_uint64), f32p, C.POINTER(C.c_uint8)]
 
     def _check(self, st):
         if st:
@@ -561,6 +599,29 @@ class Reference:
             _ptr(tile, C.c_float), _ptr(self._u32(needed), C.c_uint32), _ptr(o, C.c_uint32),
             _ptr(self._u32(image), C.c_uint32), radius, eps, space, _ptr(out, C.c_float)))
         return out
+
+
+    def histogram(self, pixels, viewport, bins=256, lower=0.0, upper=1.0, ops=(), tile=256, mip=0, quality=1,
+                  space=0):
+        """histogram_rgb of a raster-source chain (finite pixels only: the
+        reference's raster source rejects non-finite input).  Returns per
+        channel the same dict layout as librawops_b200.render.histogram_rgb."""
+        pixels = _f32(pixels)
+        h, w = pixels.shape[:2]
+        codes, params = flatten_ops(ops)
+        counts = np.zeros(3 * bins, np.uint64)
+        tallies = np.zeros(9, np.uint64)
+        extrema = np.zeros(6, np.float32)
+        present = np.zeros(6, np.uint8)
+        self._check(self.lib.refshim_histogram_raster(
+            w, h, space, _ptr(pixels, C.c_float), pixels.size, _ptr(codes, C.c_int32), len(ops),
+            _ptr(params, C.c_double), _ptr(self._u32(viewport), C.c_uint32), tile, mip, quality, bins, lower, upper,
+            _ptr(counts, C.c_uint64), _ptr(tallies, C.c_uint64), _ptr(extrema, C.c_float),
+            _ptr(present, C.c_uint8)))
+        counts = counts.reshape(3, bins)
+        return [dict(counts=counts[c], underflow=int(tallies[c]), overflow=int(tallies[3 + c]),
+                     nonfinite=int(tallies[6 + c]), minimum=float(extrema[c]) if present[c] else None,
+                     maximum=float(extrema[3 + c]) if present[3 + c] else None) for c in range(3)]
 
 
 class RefSession:

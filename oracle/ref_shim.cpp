@@ -15,6 +15,7 @@
 #include "ToneOps.hpp"
 #include "GeometryOps.hpp"
 #include "TileScheduler.hpp"
+#include "ImageAnalysis.hpp"
 
 #include <cstdint>
 #include <cstring>
@@ -260,6 +261,37 @@ int refshim_render_raster(std::uint32_t width, std::uint32_t height, std::uint32
         RenderRequest req{{viewport[0], viewport[1], viewport[2], viewport[3]}, tile_size,
                           {mip, static_cast<RenderQuality>(quality)}};
         copy_out(Renderer{}.render_image(*node, bounds, req), out);
+    });
+}
+
+// histogram_rgb (ImageAnalysis.cpp:9-69) of a raster-source chain: counts
+// (3 * bins), tallies (underflow[3], overflow[3], nonfinite[3]), extrema
+// (min[3], max[3]) with present[6] flags.
+int refshim_histogram_raster(std::uint32_t width, std::uint32_t height, int space, const float* pixels,
+                             std::size_t count, const std::int32_t* ops, int nops, const double* params,
+                             const std::uint32_t* viewport, std::uint32_t tile_size, std::uint32_t mip,
+                             std::uint32_t quality, std::uint32_t bins, double lower, double upper,
+                             std::uint64_t* counts, std::uint64_t* tallies, float* extrema,
+                             std::uint8_t* present) {
+    return guarded([&] {
+        RasterMetadata m{width, height, 0, static_cast<WorkingSpace>(space)};
+        RasterImage image(m, std::vector<float>(pixels, pixels + count));
+        Rect bounds{0, 0, width, height};
+        auto node = build_chain(std::make_shared<RasterSourceNode>(image), bounds, ops, nops, params);
+        RenderRequest req{{viewport[0], viewport[1], viewport[2], viewport[3]}, tile_size,
+                          {mip, static_cast<RenderQuality>(quality)}};
+        const auto h = histogram_rgb(*node, bounds, req, HistogramOptions{bins, lower, upper});
+        for (int c = 0; c < 3; ++c) {
+            const auto& ch = h.channels[c];
+            std::memcpy(counts + std::size_t(c) * bins, ch.counts.data(), bins * sizeof(std::uint64_t));
+            tallies[c] = ch.underflow;
+            tallies[3 + c] = ch.overflow;
+            tallies[6 + c] = ch.nonfinite;
+            present[c] = ch.minimum.has_value();
+            present[3 + c] = ch.maximum.has_value();
+            extrema[c] = ch.minimum.value_or(0.0f);
+            extrema[3 + c] = ch.maximum.value_or(0.0f);
+        }
     });
 }
 

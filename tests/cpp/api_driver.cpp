@@ -12,12 +12,15 @@
 // tests (tests/core_tests.cpp, spatial_ops_tests.cpp, rotate_tests.cpp,
 // cubic_resize_tests.cpp of tylermcm/librawops) on this path.
 #include <rawengine/GeometryOps.hpp>
+#include <rawengine/ImageAnalysis.hpp>
 #include <rawengine/RawEngine.hpp>
 #include <rawengine/SpatialOps.hpp>
 #include <rawengine/TileScheduler.hpp>
 #include <rawengine/ToneOps.hpp>
 
 #include <chrono>
+#include <limits>
+#include <numeric>
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
@@ -179,6 +182,193 @@ CameraColorTransform camera(const std::map<std::string, std::vector<double>>& P,
 }
 
 // ------------------------------------------------------------------ render
+
+// ------------------------------------------------------------- histogram
+
+// The reference's analysis probe (image_analysis_tests.cpp:20-41): a caller
+// Node whose tiles are R = (x % 9) / 4 - 0.5, G = (y % 9) / 4 - 0.5, B = NaN,
+// with optional faults in the delivered tile.
+class HistogramProbe final : public Node {
+public:
+    enum class Fault { None, Bounds, Storage, Descriptor };
+    Fault fault = Fault::None;
+    CancellationToken* cancellation = nullptr;
+    mutable unsigned calls = 0;
+    mutable std::uint64_t largest_tile = 0;
+    ImageDescriptor output_descriptor() const noexcept override { return ImageDescriptor::camera_linear(); }
+    Tile render(Rect r) const override {
+        ++calls;
+        largest_tile = std::max<std::uint64_t>(largest_tile, std::uint64_t(r.width) * r.height);
+        Tile tile{r, {}, output_descriptor()};
+        for (std::uint32_t y = r.y; y < r.y + r.height; ++y)
+            for (std::uint32_t x = r.x; x < r.x + r.width; ++x) {
+                tile.rgb.push_back(float(x % 9) * 0.25f - 0.5f);
+                tile.rgb.push_back(float(y % 9) * 0.25f - 0.5f);
+                tile.rgb.push_back(std::numeric_limits<float>::quiet_NaN());
+            }
+        if (fault == Fault::Bounds) ++tile.bounds.x;
+        if (fault == Fault::Storage) tile.rgb.pop_back();
+        if (fault == Fault::Descriptor) tile.descriptor = ImageDescriptor::srgb_output();
+        if (cancellation) cancellation->cancel();
+        return tile;
+    }
+};
+
+bool same_histogram(const RgbHistogram& a, const RgbHistogram& b) {
+    for (int c = 0; c < 3; ++c) {
+        const auto &x = a.channels[c], &y = b.channels[c];
+        if (x.counts != y.counts || x.underflow != y.underflow || x.overflow != y.overflow ||
+            x.nonfinite != y.nonfinite || x.minimum != y.minimum || x.maximum != y.maximum)
+            return false;
+    }
+    return a.pixel_count == b.pixel_count;
+}
+
+// Histogram of a rendered device image counted sample by sample on the host,
+// for comparing the device path of a DeviceNode chain.
+RgbHistogram host_histogram(const Tile& t, const HistogramOptions& o) {
+    RgbHistogram h;
+    for (auto& c : h.channels) c.counts.assign(o.bins, 0);
+    const double span = o.upper - o.lower;
+    for (size_t i = 0; i < t.rgb.size(); ++i) {
+        const float s = t.rgb[i];
+        auto& c = h.channels[i % 3];
+        if (!std::isfinite(s)) {
+            ++c.nonfinite;
+            continue;
+        }
+        if (!c.minimum || s < *c.minimum) c.minimum = s;
+        if (!c.maximum || s > *c.maximum) c.maximum = s;
+        if (s < o.lower) {
+            ++c.underflow;
+            continue;
+        }
+        if (s > o.upper) {
+            ++c.overflow;
+            continue;
+        }
+        ++c.counts[std::min<std::uint32_t>(o.bins - 1, (std::uint32_t)((double(s) - o.lower) / span * o.bins))];
+    }
+    h.pixel_count = t.rgb.size() / 3;
+    return h;
+}
+
+void histogram_checks(const std::shared_ptr<const Node>& graph_node, Rect area) {
+    {   // edge bins, clipped tiles over a nonzero viewport, tile partitions
+        HistogramProbe node;
+        const Rect bounds{7, 5, 31, 23};
+        const RenderRequest request{{9, 7, 19, 13}, 4};
+        const auto result = histogram_rgb(node, bounds, request, {4, 0, 1});
+        check(result.pixel_count == 247 && node.largest_tile <= 16 && node.calls == 20, "histogram_streams_tiles");
+        check(result.descriptor == node.output_descriptor(), "histogram_descriptor");
+        bool bins_ok = true;
+        for (unsigned c = 0; c < 2; ++c) {
+            std::array<std::uint64_t, 4> expected{};
+            std::uint64_t below = 0, above = 0;
+            for (unsigned y = 7; y < 20; ++y)
+                for (unsigned x = 9; x < 28; ++x) {
+                    const auto site = (c == 0 ? x : y) % 9;
+                    if (site < 2) ++below;
+                    else if (site > 6) ++above;
+                    else ++expected[site == 6 ? 3 : site - 2];
+                }
+            const auto& ch = result.channels[c];
+            bins_ok &= std::equal(expected.begin(), expected.end(), ch.counts.begin()) && ch.underflow == below &&
+                       ch.overflow == above && ch.nonfinite == 0 && ch.minimum == -0.5f && ch.maximum == 1.5f;
+        }
+        check(bins_ok, "histogram_bin_edges_and_outliers");
+        check(result.channels[2].nonfinite == 247 && !result.channels[2].minimum && !result.channels[2].maximum,
+              "histogram_all_nonfinite_channel");
+        bool partitions = true;
+        for (unsigned size : {1u, 3u, 7u, 256u})
+            partitions &= same_histogram(histogram_rgb(node, bounds, RenderRequest{request.viewport, size}, {4, 0, 1}),
+                                         result);
+        check(partitions, "histogram_tile_partitions");
+    }
+    {   // non-finite samples and extreme ranges
+        class Values final : public Node {
+        public:
+            ImageDescriptor output_descriptor() const noexcept override { return ImageDescriptor::linear_srgb(); }
+            Tile render(Rect r) const override {
+                const float inf = std::numeric_limits<float>::infinity();
+                return {r, {-inf, 0, -2, inf, 1, 2, std::numeric_limits<float>::quiet_NaN(), 0.5f, 0},
+                        output_descriptor()};
+            }
+        } node;
+        auto result = histogram_rgb(node, {0, 0, 3, 1}, RenderRequest{{0, 0, 3, 1}}, {1, 0, 1});
+        check(result.channels[0].nonfinite == 3 && !result.channels[0].minimum, "histogram_infinities_nonfinite");
+        check(result.channels[1].counts[0] == 3 && result.channels[2].underflow == 1 &&
+                  result.channels[2].overflow == 1,
+              "histogram_single_bin_endpoints");
+        result = histogram_rgb(node, {0, 0, 3, 1}, RenderRequest{{0, 0, 3, 1}}, {65536, -1e300, 1e300});
+        check(result.channels[1].counts[32768] == 3, "histogram_wide_range");
+        result = histogram_rgb(node, {0, 0, 3, 1}, RenderRequest{{0, 0, 3, 1}},
+                               {2, 0, std::numeric_limits<double>::denorm_min()});
+        check(result.channels[1].counts[0] == 1 && result.channels[1].overflow == 2, "histogram_tiny_range");
+    }
+    {   // invalid arguments and cancellation
+        HistogramProbe node;
+        const Rect bounds{0, 0, 9, 9};
+        const RenderRequest request{bounds, 3};
+        const double nan = std::numeric_limits<double>::quiet_NaN(), inf = std::numeric_limits<double>::infinity();
+        int i = 0;
+        for (const auto options : {HistogramOptions{0, 0, 1}, {65537, 0, 1}, {4, 1, 1}, {4, 2, 1}, {4, nan, 1},
+                                   {4, 0, inf}, {4, -1e308, 1e308}})
+            expect_throw<std::invalid_argument>([&] { histogram_rgb(node, bounds, request, options); },
+                                                "histogram_rejects_options_" + std::to_string(i++));
+        check(node.calls == 0, "histogram_invalid_options_render_nothing");
+        expect_throw<std::invalid_argument>([&] { histogram_rgb(node, bounds, RenderRequest{{0, 0, 0, 1}}); },
+                                            "histogram_rejects_empty");
+        expect_throw<std::invalid_argument>([&] { histogram_rgb(node, bounds, RenderRequest{bounds, 0}); },
+                                            "histogram_rejects_zero_tile");
+        expect_throw<std::invalid_argument>(
+            [&] { histogram_rgb(node, bounds, RenderRequest{{0, 0, 4, 4}, 3, {1, RenderQuality::Preview}}); },
+            "histogram_rejects_level");
+        expect_throw<std::out_of_range>([&] { histogram_rgb(node, bounds, RenderRequest{{8, 8, 2, 2}}); },
+                                        "histogram_rejects_outside");
+        expect_throw<std::invalid_argument>(
+            [&] { histogram_rgb(node, {0xffffffffu, 0, 2, 1}, RenderRequest{{0xffffffffu, 0, 2, 1}}); },
+            "histogram_rejects_unaddressable");
+        for (auto fault : {HistogramProbe::Fault::Bounds, HistogramProbe::Fault::Storage,
+                           HistogramProbe::Fault::Descriptor}) {
+            node.fault = fault;
+            expect_throw<std::invalid_argument>([&] { histogram_rgb(node, bounds, request); },
+                                                "histogram_rejects_fault_" + std::to_string((int)fault));
+        }
+        node.fault = HistogramProbe::Fault::None;
+        CancellationToken token;
+        token.cancel();
+        const auto before = node.calls;
+        expect_throw<RenderCancelled>([&] { histogram_rgb(node, bounds, request, {}, &token); },
+                                      "histogram_precancelled");
+        check(node.calls == before, "histogram_precancelled_renders_nothing");
+        CancellationToken last_tile;
+        node.cancellation = &last_tile;
+        expect_throw<RenderCancelled>([&] { histogram_rgb(node, bounds, RenderRequest{bounds}, {}, &last_tile); },
+                                      "histogram_cancelled_in_tile");
+        check(node.calls == before + 1, "histogram_cancelled_after_one_tile");
+    }
+    {   // ImageGraph overload
+        RawImage image(5, 3, std::vector<std::uint16_t>(15, 32768));
+        ImageGraph graph(image, GraphRecipe{});
+        const auto h = histogram_rgb(graph, RenderRequest{{0, 0, 5, 3}, 2});
+        bool covered = h.pixel_count == 15 && h.descriptor == graph.output().output_descriptor();
+        for (const auto& c : h.channels)
+            covered &= std::accumulate(c.counts.begin(), c.counts.end(), std::uint64_t{}) + c.underflow + c.overflow +
+                           c.nonfinite == 15;
+        check(covered, "histogram_image_graph_overload");
+    }
+    {   // a device chain: counted on the device in bands, equal to counting its rendered image
+        const HistogramOptions o{1024, -0.1, 1.1};
+        bool ok = true;
+        for (std::uint32_t tile : {5u, 64u, 4096u}) {
+            const RenderRequest req{area, tile};
+            const Tile img = Renderer{}.render_image(*graph_node, area, req);
+            ok &= same_histogram(histogram_rgb(*graph_node, area, req, o), host_histogram(img, o));
+        }
+        check(ok, "histogram_device_chain_equals_rendered_image");
+    }
+}
 
 int run_render(const std::string& dir) {
     const auto P = read_params(dir + "/params.txt");
@@ -467,6 +657,7 @@ int run_render(const std::string& dir) {
                 "scheduler_rejects_zero_tile");
         }
     }
+    histogram_checks(graph.output_node(), area);
     return failures ? 1 : 0;
 }
 

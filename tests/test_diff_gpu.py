@@ -153,6 +153,6 @@ def test_fit_recipe_recovers_hidden_parameters_at_radius_16():
     assert history[-1] < 1e-4 * history[0], (history[0], history[-1])
     wb = model.wb.detach().cpu().numpy()
     assert np.all(np.abs(wb / np.array([2.1, 1.0, 1.35]) - 1) < 0.01), wb
-    assert abs(float(model.strength) - 0.6) < 0.02, float(model.strength)
+    assert abs(float(model.strength.detach()) - 0.6) < 0.02, float(model.strength.detach())
     assert np.max(np.abs(model.ky.detach().cpu().numpy() - np.array(KY))) < 0.01
     assert abs(np.log(model.eps / 1e-3)) < 0.25, model.eps

@@ -231,3 +231,65 @@ def test_plan_and_halo_match_reference(oracle, reference):
     tiles = oracle.plan_tiles(vp, 128)
     assert tiles[0] == (3, 5, 128, 128) and tiles[-1] == (3 + 512, 5 + 256, 5, 45)
     assert len(tiles) == 5 * 3
+
+
+def _probe_pattern(bounds, viewport):
+    """The reference's analysis probe (image_analysis_tests.cpp:20-41):
+    R = (x % 9) / 4 - 0.5, G = (y % 9) / 4 - 0.5, B = NaN over the viewport."""
+    x0, y0, w, h = viewport
+    y, x = np.mgrid[y0:y0 + h, x0:x0 + w]
+    return np.stack([(x % 9) * 0.25 - 0.5, (y % 9) * 0.25 - 0.5, np.full(x.shape, np.nan)], -1).astype(np.float32)
+
+
+def test_histogram_restatement_known_answers():
+    """The discrete truths of image_analysis_tests.cpp:44-103, restated."""
+    from oracle.oracle import histogram_rgb
+    vp = (9, 7, 19, 13)
+    img = _probe_pattern(None, vp)
+    for tile in (1, 3, 4, 7, 256):
+        h = histogram_rgb(img, 4, 0.0, 1.0, tile)
+        for c in range(2):
+            expected, below, above = np.zeros(4, np.uint64), 0, 0
+            for y in range(7, 20):
+                for x in range(9, 28):
+                    site = (x if c == 0 else y) % 9
+                    if site < 2:
+                        below += 1
+                    elif site > 6:
+                        above += 1
+                    else:
+                        expected[3 if site == 6 else site - 2] += 1
+            assert np.array_equal(h[c]["counts"], expected)
+            assert (h[c]["underflow"], h[c]["overflow"], h[c]["nonfinite"]) == (below, above, 0)
+            assert (h[c]["minimum"], h[c]["maximum"]) == (-0.5, 1.5)
+        assert h[2]["nonfinite"] == 247 and h[2]["minimum"] is None and h[2]["maximum"] is None
+    inf = np.float32(np.inf)
+    vals = np.array([[[-inf, 0, -2], [inf, 1, 2], [np.nan, 0.5, 0]]], np.float32)
+    h = histogram_rgb(vals, 1, 0.0, 1.0)
+    assert h[0]["nonfinite"] == 3 and h[0]["minimum"] is None
+    assert h[1]["counts"][0] == 3 and h[2]["underflow"] == 1 and h[2]["overflow"] == 1
+    assert histogram_rgb(vals, 65536, -1e300, 1e300)[1]["counts"][32768] == 3
+    h = histogram_rgb(vals, 2, 0.0, 5e-324)
+    assert h[1]["counts"][0] == 1 and h[1]["overflow"] == 2
+
+
+@pytest.mark.parametrize("bins,lower,upper,tile", [(4, 0.0, 1.0, 7), (256, -0.5, 1.5, 16), (5000, 0.2, 0.3, 8),
+                                                   (65536, -1e300, 1e300, 256), (1, 0.0, 1.0, 5)])
+def test_histogram_restatement_matches_reference(reference, bins, lower, upper, tile):
+    """Finite images (the reference's raster source rejects others), including
+    +0 / -0 ties at the minimum of a channel."""
+    from oracle.oracle import histogram_rgb
+    rng = np.random.default_rng(bins)
+    img = rng.normal(0.5, 0.6, (37, 53, 3)).astype(np.float32)
+    img[..., 2] = np.abs(img[..., 2])
+    img[1, 40, 2] = -0.0          # first in row order, in a later tile ...
+    img[3, 2, 2] = 0.0            # ... than this +0 when tiles are narrower than 40
+    img[20, 50, 2] = -0.0
+    want = reference.histogram(img, (0, 0, 53, 37), bins, lower, upper, tile=tile)
+    got = histogram_rgb(img, bins, lower, upper, tile)
+    for c in range(3):
+        for k in ("underflow", "overflow", "nonfinite"):
+            assert got[c][k] == want[c][k], (c, k)
+        assert np.array_equal(got[c]["counts"], want[c]["counts"]), c
+        for k in ("minimum", "maximum"):
+            assert np.float32(got[c][k]).tobytes() == np.float32(want[c][k]).tobytes(), (c, k)
