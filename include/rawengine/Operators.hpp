@@ -82,6 +82,98 @@ private:
     ImageDescriptor descriptor_;
 };
 
+// Local-contrast stencils (SpatialOps.hpp:36-170): settings and validators
+// with the reference's names and ranges, and nodes rendered on the device.
+struct ConvolutionKernel {
+    std::uint32_t width = 1, height = 1;       // odd, each 1..17
+    std::vector<double> coefficients{1.0};     // row-major, finite, |c| <= 65536
+};
+RAWENGINE_API void validate_convolution_kernel(const ConvolutionKernel& kernel);
+
+struct ClaritySettings {
+    double amount = 0.0;          // finite [-1, 1]
+    std::uint32_t radius = 3;     // 1..8, requested-level pixels
+};
+RAWENGINE_API void validate_clarity_settings(const ClaritySettings& settings);
+
+struct TextureSettings {
+    double amount = 0.0;          // finite [-1, 1]
+    std::uint32_t scale = 2;      // 1..4 unit blur passes; support is 2 * scale pixels
+};
+RAWENGINE_API void validate_texture_settings(const TextureSettings& settings);
+
+struct SharpenSettings {
+    double amount = 0.0;          // finite 0..2; exact zero passes the input through
+    std::uint32_t radius = 1;     // 1..3, requested-level pixels
+};
+RAWENGINE_API void validate_sharpen_settings(const SharpenSettings& settings);
+
+// Base of the four stencil nodes: a scene-linear working-RGB input rendered
+// over the output grown by halo_x() x halo_y() (clipped to the level's image
+// bounds), then one stencil launch.  Levels: mip 0 Final or Preview, mip 1/2
+// Preview, when the input supports them.
+class RAWENGINE_API StencilNode : public DeviceNode {
+public:
+    bool supports_level(RenderLevel level) const noexcept override;
+    Rect input_region(Rect output, Rect source_bounds) const override;
+    Rect input_region_level(Rect output, Rect source_bounds, RenderLevel level) const override;
+    const Node* input_node() const noexcept override { return input_.get(); }
+    ImageDescriptor output_descriptor() const noexcept override { return input_->output_descriptor(); }
+    Rect native_bounds() const noexcept { return native_bounds_; }
+    virtual std::uint32_t halo_x() const noexcept = 0;
+    virtual std::uint32_t halo_y() const noexcept = 0;
+    std::uint32_t working_space() const noexcept { return space_; }
+protected:
+    StencilNode(std::shared_ptr<const Node> input, Rect native_bounds, const char* name);
+    std::shared_ptr<const Node> input_;
+    Rect native_bounds_;
+    std::uint32_t space_ = 0;
+    const char* name_;
+};
+
+class RAWENGINE_API ClarityNode final : public StencilNode {
+public:
+    ClarityNode(std::shared_ptr<const Node> input, Rect native_bounds, ClaritySettings settings = {});
+    std::uint32_t halo_x() const noexcept override { return settings_.amount == 0 ? 0 : settings_.radius; }
+    std::uint32_t halo_y() const noexcept override { return halo_x(); }
+    const ClaritySettings& settings() const noexcept { return settings_; }
+private:
+    ClaritySettings settings_;
+};
+
+class RAWENGINE_API TextureNode final : public StencilNode {
+public:
+    TextureNode(std::shared_ptr<const Node> input, Rect native_bounds, TextureSettings settings = {});
+    std::uint32_t halo_x() const noexcept override { return settings_.amount == 0 ? 0 : 2 * settings_.scale; }
+    std::uint32_t halo_y() const noexcept override { return halo_x(); }
+    const TextureSettings& settings() const noexcept { return settings_; }
+private:
+    TextureSettings settings_;
+};
+
+class RAWENGINE_API SharpenNode final : public StencilNode {
+public:
+    SharpenNode(std::shared_ptr<const Node> input, Rect native_bounds, SharpenSettings settings = {});
+    std::uint32_t halo_x() const noexcept override { return settings_.amount == 0 ? 0 : settings_.radius; }
+    std::uint32_t halo_y() const noexcept override { return halo_x(); }
+    const SharpenSettings& settings() const noexcept { return settings_; }
+private:
+    SharpenSettings settings_;
+};
+
+// Flipped on both axes (a convolution), binary64 accumulation, replicate
+// boundary, no normalisation or clipping.
+class RAWENGINE_API ConvolutionNode final : public StencilNode {
+public:
+    ConvolutionNode(std::shared_ptr<const Node> input, Rect native_bounds, ConvolutionKernel kernel);
+    std::uint32_t halo_x() const noexcept override { return identity_ ? 0 : kernel_.width / 2; }
+    std::uint32_t halo_y() const noexcept override { return identity_ ? 0 : kernel_.height / 2; }
+    const ConvolutionKernel& kernel() const noexcept { return kernel_; }
+private:
+    ConvolutionKernel kernel_;
+    bool identity_ = false;
+};
+
 // ------------------------------------------------------------- GeometryOps
 
 struct RAWENGINE_API RotateSettings {

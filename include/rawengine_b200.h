@@ -460,6 +460,35 @@ RE_API re_status re_cubic_axis(uint32_t input, uint32_t output, uint32_t index, 
 /* GeometryOps.cpp:46-67 rotation constants (host). */
 RE_API re_status re_rotation_coefficients(double angle_degrees, double* cosine, double* sine);
 
+/* ----------------------------------------------------- local-contrast stencils */
+
+/* SharpenNode, ClarityNode, TextureNode and ConvolutionNode::render_level
+ * (SpatialOps.cpp:319-701) on device float32 RGB, bit-exact: `in` holds the
+ * image rectangle `window` (row stride in floats), which must cover `output`
+ * grown by the stencil's halo and clipped to `image` (the level's image
+ * bounds; the reference's `needed` region): radius for Sharpen and Clarity,
+ * 2 * scale for Texture, kernel_width/2 x kernel_height/2 for Convolution,
+ * none for a zero amount or an identity kernel.  `out` receives the output
+ * rectangle.  A non-finite sample of the needed region or a result beyond
+ * float32 returns RE_INVALID_ARGUMENT with the reference's message.  Working
+ * space 0 = linear ProPhoto D50, 1 = linear Rec.2020 D65.  Returns after
+ * completion on `stream`. */
+RE_API re_status re_sharpen_window(const float* in, size_t in_row_stride, re_rect window, re_rect image,
+                                   re_rect output, double amount, uint32_t radius, float* out,
+                                   size_t out_row_stride, void* stream);
+RE_API re_status re_clarity_window(const float* in, size_t in_row_stride, re_rect window, re_rect image,
+                                   re_rect output, double amount, uint32_t radius, uint32_t working_space,
+                                   float* out, size_t out_row_stride, void* stream);
+RE_API re_status re_texture_window(const float* in, size_t in_row_stride, re_rect window, re_rect image,
+                                   re_rect output, double amount, uint32_t scale, uint32_t working_space,
+                                   float* out, size_t out_row_stride, void* stream);
+/* coefficients: host, row-major kernel_height x kernel_width (flipped on both
+ * axes when applied, as a convolution). */
+RE_API re_status re_convolution_window(const float* in, size_t in_row_stride, re_rect window, re_rect image,
+                                       re_rect output, uint32_t kernel_width, uint32_t kernel_height,
+                                       const double* coefficients, float* out, size_t out_row_stride,
+                                       void* stream);
+
 /* ------------------------------------------------------------------ analysis */
 
 /* histogram_rgb (ImageAnalysis.cpp:9-69) over a DEVICE float32 RGB image:

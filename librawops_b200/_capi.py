@@ -38,6 +38,7 @@ EXPORTS = [
     "re_diff_bilinear_forward", "re_diff_bilinear_backward", "re_diff_point_forward", "re_diff_point_backward",
     "re_diff_point_grad_count", "re_diff_detail_forward", "re_diff_detail_backward",
     "re_histogram_reset", "re_histogram_rgb", "re_histogram_extremum",
+    "re_sharpen_window", "re_clarity_window", "re_texture_window", "re_convolution_window",
 ]
 
 
@@ -181,6 +182,10 @@ def lib() -> C.CDLL:
                                        vp]
         L.re_histogram_extremum.argtypes = [C.c_uint64, C.c_int, C.POINTER(C.c_float)]
         L.re_histogram_extremum.restype = C.c_int
+        L.re_sharpen_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, vp, sz, vp]
+        L.re_clarity_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, u32, vp, sz, vp]
+        L.re_texture_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, u32, vp, sz, vp]
+        L.re_convolution_window.argtypes = [vp, sz, Rect, Rect, Rect, u32, u32, f64p, vp, sz, vp]
         _lib = L
     return _lib
 

@@ -522,6 +522,74 @@ Rect WorkingYGuidedFilterNode::input_region_level(Rect output, Rect source_bound
     return working_y_guided_filter_region(output, image, settings_.radius);
 }
 
+// ------------------------------------------------------------- stencils
+
+// SpatialOps.cpp:319-327, 386-390, 496-500, 621-624
+void validate_convolution_kernel(const ConvolutionKernel& k) {
+    if (!k.width || !k.height || k.width > 17 || k.height > 17 || k.width % 2 != 1 || k.height % 2 != 1 ||
+        k.coefficients.size() != (size_t)k.width * k.height)
+        throw std::invalid_argument("convolution kernel needs odd dimensions 1..17 and matching coefficients");
+    for (double v : k.coefficients)
+        if (!std::isfinite(v) || std::abs(v) > 65536)
+            throw std::invalid_argument("convolution coefficients must be finite with magnitude <=65536");
+}
+void validate_clarity_settings(const ClaritySettings& s) {
+    if (!std::isfinite(s.amount) || std::abs(s.amount) > 1 || s.radius < 1 || s.radius > 8)
+        throw std::invalid_argument("clarity requires finite amount [-1,1] and radius 1..8");
+}
+void validate_texture_settings(const TextureSettings& s) {
+    if (!std::isfinite(s.amount) || std::abs(s.amount) > 1 || s.scale < 1 || s.scale > 4)
+        throw std::invalid_argument("texture requires finite amount [-1,1] and scale 1..4");
+}
+void validate_sharpen_settings(const SharpenSettings& s) {
+    if (!std::isfinite(s.amount) || s.amount < 0 || s.amount > 2 || s.radius < 1 || s.radius > 3)
+        throw std::invalid_argument("sharpen requires finite amount 0..2 and radius 1..3");
+}
+
+StencilNode::StencilNode(std::shared_ptr<const Node> input, Rect native_bounds, const char* name)
+    : input_(std::move(input)), native_bounds_(native_bounds), name_(name) {
+    bounded_rect(native_bounds_);
+    const std::string n(name);
+    if (!input_)
+        throw std::invalid_argument(n == "clarity" || n == "texture" ? n + " requires input"
+                                                                     : n + " requires scene-linear working RGB");
+    if (!scene_linear(input_->output_descriptor()))
+        throw std::invalid_argument(n + " requires scene-linear working RGB");
+    space_ = space_code(input_->output_descriptor());
+}
+bool StencilNode::supports_level(RenderLevel level) const noexcept {
+    return (level_any_native(level) || level_reduced(level)) && input_->supports_level(level);
+}
+Rect StencilNode::input_region(Rect output, Rect source_bounds) const {
+    return input_region_level(output, source_bounds, {});
+}
+Rect StencilNode::input_region_level(Rect output, Rect source_bounds, RenderLevel level) const {
+    const Rect image = level_bounds(native_bounds_, level);
+    if (!same(source_bounds, image) || !supports_level(level))
+        throw std::invalid_argument(std::string(name_) + (std::string(name_) == "sharpen"
+                                                               ? " source bounds or render level differ"
+                                                               : " source bounds or level differ"));
+    return spatial_expanded(output, image, halo_x(), halo_y());
+}
+
+ClarityNode::ClarityNode(std::shared_ptr<const Node> input, Rect native_bounds, ClaritySettings settings)
+    : StencilNode((validate_clarity_settings(settings), std::move(input)), native_bounds, "clarity"),
+      settings_(settings) {}
+TextureNode::TextureNode(std::shared_ptr<const Node> input, Rect native_bounds, TextureSettings settings)
+    : StencilNode((validate_texture_settings(settings), std::move(input)), native_bounds, "texture"),
+      settings_(settings) {}
+SharpenNode::SharpenNode(std::shared_ptr<const Node> input, Rect native_bounds, SharpenSettings settings)
+    : StencilNode((validate_sharpen_settings(settings), std::move(input)), native_bounds, "sharpen"),
+      settings_(settings) {}
+ConvolutionNode::ConvolutionNode(std::shared_ptr<const Node> input, Rect native_bounds, ConvolutionKernel kernel)
+    : StencilNode((validate_convolution_kernel(kernel), std::move(input)), native_bounds, "convolution"),
+      kernel_(std::move(kernel)) {
+    identity_ = true;
+    const size_t center = kernel_.coefficients.size() / 2;
+    for (size_t i = 0; i < kernel_.coefficients.size(); ++i)
+        if (kernel_.coefficients[i] != (i == center ? 1.0 : 0.0)) identity_ = false;
+}
+
 // ------------------------------------------------------------- GeometryOps
 
 void validate_rotate_settings(const RotateSettings& s) {
@@ -808,6 +876,7 @@ struct Executor {
         if (auto* gf = dynamic_cast<const WorkingYGuidedFilterNode*>(&node)) return eval_gf(*gf, r, level);
         if (auto* cr = dynamic_cast<const CubicResizeNode*>(&node)) return eval_cubic(*cr, r, level);
         if (auto* ro = dynamic_cast<const RotateNode*>(&node)) return eval_rotate(*ro, r, level);
+        if (auto* st = dynamic_cast<const StencilNode*>(&node)) return eval_stencil(*st, r, level);
         if (dynamic_cast<const DeviceNode*>(&node)) return eval(node, r, level);
         return upload(node, r, level);
     }
@@ -858,6 +927,32 @@ struct Executor {
         const re_rect window{support.x - ib.x, support.y - ib.y, support.width, support.height};
         check(re_cubic_resize_window(in->data, in->stride, window, ib.width, ib.height, cr.settings().width,
                                      cr.settings().height, to_re(r), level.mip, out->data, out->stride, s));
+        return out;
+    }
+
+    // SpatialOps.cpp:343-383, 410-495, 509-620, 637-697: render the input over
+    // the node's `needed` region, then one stencil launch.
+    DevPtr eval_stencil(const StencilNode& st, Rect r, RenderLevel level) {
+        const Rect image = level_bounds(st.native_bounds(), level);
+        const Rect needed = st.input_region_level(r, image, level);
+        DevPtr in = eval(*st.input_node(), needed, level);
+        auto out = std::make_unique<DevImage>(r, s);
+        const re_rect w = to_re(needed), im = to_re(image), o = to_re(r);
+        const uint32_t space = st.working_space();
+        if (auto* p = dynamic_cast<const SharpenNode*>(&st))
+            check(re_sharpen_window(in->data, in->stride, w, im, o, p->settings().amount, p->settings().radius,
+                                    out->data, out->stride, s));
+        else if (auto* p = dynamic_cast<const ClarityNode*>(&st))
+            check(re_clarity_window(in->data, in->stride, w, im, o, p->settings().amount, p->settings().radius,
+                                    space, out->data, out->stride, s));
+        else if (auto* p = dynamic_cast<const TextureNode*>(&st))
+            check(re_texture_window(in->data, in->stride, w, im, o, p->settings().amount, p->settings().scale,
+                                    space, out->data, out->stride, s));
+        else if (auto* p = dynamic_cast<const ConvolutionNode*>(&st))
+            check(re_convolution_window(in->data, in->stride, w, im, o, p->kernel().width, p->kernel().height,
+                                        p->kernel().coefficients.data(), out->data, out->stride, s));
+        else
+            throw std::logic_error("unknown stencil node");
         return out;
     }
 

@@ -487,6 +487,32 @@ def histogram_rgb(rgb, bins: int = 256, lower: float = 0.0, upper: float = 1.0, 
     return out
 
 
+def stencil(kind: str, rgb, window, image, output, amount: float = 0.0, radius: int = 1,
+            working_space: int = PROPHOTO, kernel=None, stream=None):
+    """SharpenNode / ClarityNode / TextureNode / ConvolutionNode::render_level
+    on a CUDA float tensor holding the image rectangle `window`: returns the
+    output rectangle.  `radius` is the scale for "texture"; "convolution"
+    takes `kernel`, a 2-D array of odd sizes (flipped when applied)."""
+    o = _rect(output)
+    out = rgb.new_empty((o.height, o.width, 3))
+    args = (_dev(rgb), rgb.stride(0), _rect(window), _rect(image), o)
+    tail = (_dev(out), out.stride(0), C.c_void_p(_stream_ptr(stream)))
+    L = lib()
+    if kind == "sharpen":
+        check(L.re_sharpen_window(*args, float(amount), radius, *tail))
+    elif kind == "clarity":
+        check(L.re_clarity_window(*args, float(amount), radius, working_space, *tail))
+    elif kind == "texture":
+        check(L.re_texture_window(*args, float(amount), radius, working_space, *tail))
+    elif kind == "convolution":
+        k = np.ascontiguousarray(kernel, dtype=np.float64)
+        check(L.re_convolution_window(*args, k.shape[1], k.shape[0], k.ctypes.data_as(C.POINTER(C.c_double)),
+                                      *tail))
+    else:
+        raise ValueError(f"unknown stencil {kind}")
+    return out
+
+
 def cubic_resize(rgb, out_w: int, out_h: int, output=None, mip: int = 0, stream=None):
     h, w = int(rgb.shape[0]), int(rgb.shape[1])
     output = output or (0, 0, *request_bounds((0, 0, out_w, out_h), mip, PREVIEW if mip else FINAL)[2:])

@@ -39,6 +39,10 @@ OP_GUIDED_FILTER = 10
 OP_CUBIC_RESIZE = 11
 OP_ROTATE = 12
 OP_WORKING_SPACE_CONVERT = 13
+OP_SHARPEN = 14          # amount, radius (reference library only)
+OP_CLARITY = 15          # amount, radius
+OP_TEXTURE = 16          # amount, scale
+OP_CONVOLUTION = 17      # width, height, coefficients (row-major)
 
 ERRORS = {1: "invalid_argument", 2: "out_of_range", 3: "domain_error", 4: "length_error",
           5: "overflow_error", 6: "cancelled", 9: "logic_error", 10: "runtime_error"}
@@ -500,6 +504,8 @@ class Reference:
                                                u32p]
         L.refshim_guided_filter.argtypes = [f32p, u32p, u32p, u32p, C.c_uint32, C.c_double, C.c_int,
                                             f32p]
+        L.refshim_stencil_raster.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t, f64p, u32p,
+                                             C.c_uint32, C.c_uint32, C.c_uint32, f32p]
         L.refshim_histogram_raster.argtypes = [C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t, i32p, C.c_int,
                                                f64p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                                C.c_double, C.c_double, C.POINTER(C.c_uint64),
@@ -600,6 +606,27 @@ class Reference:
             _ptr(self._u32(image), C.c_uint32), radius, eps, space, _ptr(out, C.c_float)))
         return out
 
+
+    STENCILS = {"sharpen": 0, "clarity": 1, "texture": 2, "convolution": 3}
+
+    def stencil(self, kind, pixels, viewport, amount=0.0, radius=1, kernel=None, tile=256, mip=0, quality=1,
+                space=0):
+        """SharpenNode / ClarityNode / TextureNode (radius = scale) /
+        ConvolutionNode over a raster source, rendered through render_image."""
+        pixels = _f32(pixels)
+        h, w = pixels.shape[:2]
+        if kind == "convolution":
+            k = np.asarray(kernel, np.float64)
+            params = np.concatenate([[k.shape[1], k.shape[0]], k.reshape(-1)])
+        else:
+            params = np.array([amount, radius], np.float64)
+        params = np.ascontiguousarray(params, np.float64)
+        vp = self._u32(viewport)
+        out = np.zeros((int(vp[3]), int(vp[2]), 3), np.float32)
+        self._check(self.lib.refshim_stencil_raster(
+            self.STENCILS[kind], w, h, space, _ptr(pixels, C.c_float), pixels.size, _ptr(params, C.c_double),
+            _ptr(vp, C.c_uint32), tile, mip, quality, _ptr(out, C.c_float)))
+        return out
 
     def histogram(self, pixels, viewport, bins=256, lower=0.0, upper=1.0, ops=(), tile=256, mip=0, quality=1,
                   space=0):

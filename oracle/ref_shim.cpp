@@ -34,6 +34,10 @@ enum Op : std::int32_t {
     OP_TONE = 5, OP_OUTPUT_CLIP = 6, OP_SRGB_ENCODE = 7, OP_DISPLAY_TAG = 8,
     OP_CURVES_EXT = 9, OP_GUIDED_FILTER = 10, OP_CUBIC_RESIZE = 11, OP_ROTATE = 12,
     OP_WORKING_SPACE_CONVERT = 13,
+    OP_SHARPEN = 14,
+    OP_CLARITY = 15,
+    OP_TEXTURE = 16,
+    OP_CONVOLUTION = 17,
 };
 
 // The reference's own tests retag linear sRGB as display-linear sRGB with an
@@ -163,6 +167,23 @@ std::shared_ptr<const Node> build_chain(std::shared_ptr<const Node> node, Rect& 
         case OP_WORKING_SPACE_CONVERT:
             node = std::make_shared<WorkingSpaceConvertNode>(node, static_cast<WorkingSpace>(int(p[0])));
             p += 1; break;
+        case OP_SHARPEN:
+            node = std::make_shared<SharpenNode>(node, bounds, SharpenSettings{p[0], std::uint32_t(p[1])});
+            p += 2; break;
+        case OP_CLARITY:
+            node = std::make_shared<ClarityNode>(node, bounds, ClaritySettings{p[0], std::uint32_t(p[1])});
+            p += 2; break;
+        case OP_TEXTURE:
+            node = std::make_shared<TextureNode>(node, bounds, TextureSettings{p[0], std::uint32_t(p[1])});
+            p += 2; break;
+        case OP_CONVOLUTION: {
+            ConvolutionKernel k;
+            k.width = std::uint32_t(p[0]);
+            k.height = std::uint32_t(p[1]);
+            k.coefficients.assign(p + 2, p + 2 + std::size_t(k.width) * k.height);
+            node = std::make_shared<ConvolutionNode>(node, bounds, k);
+            p += 2 + std::size_t(k.width) * k.height; break;
+        }
         default: throw std::invalid_argument("shim: unknown op");
         }
     }
@@ -292,6 +313,38 @@ int refshim_histogram_raster(std::uint32_t width, std::uint32_t height, int spac
             extrema[c] = ch.minimum.value_or(0.0f);
             extrema[3 + c] = ch.maximum.value_or(0.0f);
         }
+    });
+}
+
+// Sharpen (kind 0: amount, radius), Clarity (1: amount, radius), Texture (2:
+// amount, scale) or Convolution (3: width, height, coefficients...) over a
+// raster source (SpatialOps.cpp:319-701), rendered through render_image.
+int refshim_stencil_raster(int kind, std::uint32_t width, std::uint32_t height, int space, const float* pixels,
+                           std::size_t count, const double* params, const std::uint32_t* viewport,
+                           std::uint32_t tile_size, std::uint32_t mip, std::uint32_t quality, float* out) {
+    return guarded([&] {
+        RasterMetadata m{width, height, 0, static_cast<WorkingSpace>(space)};
+        RasterImage image(m, std::vector<float>(pixels, pixels + count));
+        const Rect bounds{0, 0, width, height};
+        std::shared_ptr<const Node> src = std::make_shared<RasterSourceNode>(image), node;
+        const auto u = [](double v) { return static_cast<std::uint32_t>(v); };
+        switch (kind) {
+        case 0: node = std::make_shared<SharpenNode>(src, bounds, SharpenSettings{params[0], u(params[1])}); break;
+        case 1: node = std::make_shared<ClarityNode>(src, bounds, ClaritySettings{params[0], u(params[1])}); break;
+        case 2: node = std::make_shared<TextureNode>(src, bounds, TextureSettings{params[0], u(params[1])}); break;
+        case 3: {
+            ConvolutionKernel k;
+            k.width = u(params[0]);
+            k.height = u(params[1]);
+            k.coefficients.assign(params + 2, params + 2 + std::size_t(k.width) * k.height);
+            node = std::make_shared<ConvolutionNode>(src, bounds, k);
+            break;
+        }
+        default: throw std::invalid_argument("shim: unknown stencil");
+        }
+        RenderRequest req{{viewport[0], viewport[1], viewport[2], viewport[3]}, tile_size,
+                          {mip, static_cast<RenderQuality>(quality)}};
+        copy_out(Renderer{}.render_image(*node, bounds, req), out);
     });
 }
 

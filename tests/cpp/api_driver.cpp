@@ -370,6 +370,95 @@ void histogram_checks(const std::shared_ptr<const Node>& graph_node, Rect area) 
     }
 }
 
+// --------------------------------------------------------------- stencils
+
+// Sharpen, Clarity, Texture and Convolution over the working chain: outputs
+// at mip 0 over stencil_vp and over the whole mip 1 level (compared with the
+// reference on the pytest side), tile independence, pass-through cases and
+// the nodes' validation.
+void stencil_checks(const std::string& dir, const std::map<std::string, std::vector<double>>& P,
+                    const std::shared_ptr<const Node>& working, Rect area) {
+    Renderer renderer;
+    const auto& sp = P.at("sharpen");
+    const auto& cl = P.at("clarity");
+    const auto& tx = P.at("texture");
+    const auto& cv = P.at("convolution");
+    ConvolutionKernel k;
+    k.width = (uint32_t)cv[0];
+    k.height = (uint32_t)cv[1];
+    k.coefficients.assign(cv.begin() + 2, cv.end());
+    const std::vector<std::pair<std::string, std::shared_ptr<const Node>>> nodes = {
+        {"sharpen", std::make_shared<SharpenNode>(working, area, SharpenSettings{sp[0], (uint32_t)sp[1]})},
+        {"clarity", std::make_shared<ClarityNode>(working, area, ClaritySettings{cl[0], (uint32_t)cl[1]})},
+        {"texture", std::make_shared<TextureNode>(working, area, TextureSettings{tx[0], (uint32_t)tx[1]})},
+        {"convolution", std::make_shared<ConvolutionNode>(working, area, k)}};
+    const Rect vp = rect_of(P.at("stencil_vp"));
+    const RenderLevel mip1{1, RenderQuality::Preview};
+    const Rect level1{0, 0, (area.width + 1) / 2, (area.height + 1) / 2};
+    for (const auto& [name, node] : nodes) {
+        const Tile t = renderer.render_image(*node, area, RenderRequest{vp, 4096});
+        emit(dir, "stencil_" + name, t.bounds, t.rgb, "f32");
+        const Tile m = renderer.render_image(*node, area, RenderRequest{level1, 4096, mip1});
+        emit(dir, "stencil_" + name + "_mip1", m.bounds, m.rgb, "f32");
+        std::vector<float> tiled(t.rgb.size());
+        renderer.render_tiles(*node, area, RenderRequest{vp, 13}, [&](const Tile& tile) {
+            for (uint32_t row = 0; row < tile.bounds.height; ++row)
+                std::memcpy(tiled.data() + ((size_t)(tile.bounds.y - vp.y + row) * vp.width + tile.bounds.x - vp.x) * 3,
+                            tile.rgb.data() + (size_t)row * tile.bounds.width * 3,
+                            (size_t)tile.bounds.width * 3 * sizeof(float));
+        });
+        check(bit_equal(tiled, t.rgb), "stencil_tiles_equal_whole_" + name);
+        check(node->output_descriptor() == working->output_descriptor(), "stencil_descriptor_" + name);
+        expect_throw<std::invalid_argument>(
+            [&] { (void)node->input_region_level(vp, Rect{0, 0, area.width, area.height}, {}); },
+            "stencil_rejects_other_bounds_" + name);
+        expect_throw<std::out_of_range>(
+            [&] { (void)node->input_region(Rect{area.x + area.width - 2, area.y, 5, 5}, area); },
+            "stencil_rejects_outside_" + name);
+        check(node->supports_level(mip1) && node->supports_level({0, RenderQuality::Preview}) &&
+                  !node->supports_level({1, RenderQuality::Final}),
+              "stencil_levels_" + name);
+    }
+    // pass-through: zero amounts and an identity kernel return the input pixels
+    const Tile in = renderer.render_image(*working, area, RenderRequest{vp, 4096});
+    ConvolutionKernel ident{3, 3, {0, 0, 0, 0, 1, 0, 0, 0, 0}};
+    const std::vector<std::shared_ptr<const Node>> passes = {
+        std::make_shared<SharpenNode>(working, area, SharpenSettings{0.0, 3}),
+        std::make_shared<ClarityNode>(working, area, ClaritySettings{0.0, 8}),
+        std::make_shared<TextureNode>(working, area, TextureSettings{0.0, 4}),
+        std::make_shared<ConvolutionNode>(working, area, ident)};
+    bool same_pixels = true;
+    for (const auto& n : passes) {
+        same_pixels &= bit_equal(renderer.render_image(*n, area, RenderRequest{vp, 4096}).rgb, in.rgb);
+        const Rect r = n->input_region(vp, area);
+        same_pixels &= r.x == vp.x && r.y == vp.y && r.width == vp.width && r.height == vp.height;
+    }
+    check(same_pixels, "stencil_pass_through");
+    // settings and input validation
+    expect_throw<std::invalid_argument>([&] { SharpenNode(working, area, SharpenSettings{2.5, 1}); },
+                                        "sharpen_rejects_amount");
+    expect_throw<std::invalid_argument>([&] { SharpenNode(working, area, SharpenSettings{1.0, 4}); },
+                                        "sharpen_rejects_radius");
+    expect_throw<std::invalid_argument>([&] { ClarityNode(working, area, ClaritySettings{-1.5, 3}); },
+                                        "clarity_rejects_amount");
+    expect_throw<std::invalid_argument>([&] { ClarityNode(working, area, ClaritySettings{0.5, 9}); },
+                                        "clarity_rejects_radius");
+    expect_throw<std::invalid_argument>([&] { TextureNode(working, area, TextureSettings{0.5, 5}); },
+                                        "texture_rejects_scale");
+    expect_throw<std::invalid_argument>([&] { ConvolutionNode(working, area, ConvolutionKernel{2, 3, {1, 1, 1, 1, 1, 1}}); },
+                                        "convolution_rejects_even");
+    expect_throw<std::invalid_argument>([&] { ConvolutionNode(working, area, ConvolutionKernel{3, 1, {1, 1e6, 1}}); },
+                                        "convolution_rejects_coefficient");
+    expect_throw<std::invalid_argument>([&] { ClarityNode(nullptr, area, ClaritySettings{0.5, 3}); },
+                                        "clarity_requires_input");
+    expect_throw<std::invalid_argument>(
+        [&] { SharpenNode(std::make_shared<SrgbEncodeNode>(std::make_shared<WorkingToSrgbNode>(working)), area,
+                          SharpenSettings{1.0, 1}); },
+        "sharpen_requires_working_rgb");
+    expect_throw<std::invalid_argument>([&] { TextureNode(working, Rect{0, 0, 0, 4}, TextureSettings{0.5, 1}); },
+                                        "texture_rejects_empty_bounds");
+}
+
 int run_render(const std::string& dir) {
     const auto P = read_params(dir + "/params.txt");
     const RawImage raw = make_raw(P, dir);
@@ -657,6 +746,7 @@ int run_render(const std::string& dir) {
                 "scheduler_rejects_zero_tile");
         }
     }
+    stencil_checks(dir, P, ctw, area);
     histogram_checks(graph.output_node(), area);
     return failures ? 1 : 0;
 }

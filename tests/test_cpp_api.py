@@ -96,6 +96,11 @@ PARAMS = {
     "rotate_vp_mip2": [2, 3, 25, 18],
     "raster_meta": [45, 37, 0],
     "raster_recipe": [0.5, 2.2],
+    "stencil_vp": [12, 10, 70, 60],
+    "sharpen": [1.3, 2],
+    "clarity": [0.6, 5],
+    "texture": [-0.7, 3],
+    "convolution": [5, 3] + [round(0.05 * (i % 7) - 0.1, 3) for i in range(15)],
 }
 
 
@@ -132,7 +137,7 @@ def _outputs(tmp, lines):
 
 
 @pytest.mark.gpu
-def test_cpp_renders_match_oracle(driver, oracle, tmp_path):
+def test_cpp_renders_match_oracle(driver, oracle, reference, tmp_path):
     spec, raster = _inputs(str(tmp_path))
     lines = _run([driver, "render", str(tmp_path)])
     assert sum(ln.startswith("CHECK") for ln in lines) >= 30
@@ -196,6 +201,19 @@ def test_cpp_renders_match_oracle(driver, oracle, tmp_path):
     native = oracle.mip_native_region((0, 0, area[2], area[3]), 2, rect)
     want = oracle.mip_reduce(oracle.rotate(rot, src, native), native, 2, rect)
     within_tolerance(a, want, lsb16=False)
+
+    # stencils over Menon -> WB -> exposure -> camera-to-ProPhoto, against the
+    # reference library's nodes over its own render of the same chain
+    base = [Op(O.OP_WB, s[:3]), Op(O.OP_EXPOSURE, [s[3]]), Op(O.OP_CAMERA_TO_WORKING, CAMERA + [0])]
+    codes = {"sharpen": O.OP_SHARPEN, "clarity": O.OP_CLARITY, "texture": O.OP_TEXTURE,
+             "convolution": O.OP_CONVOLUTION}
+    for name, code in codes.items():
+        ops = base + [Op(code, PARAMS[name])]
+        rect, a = got["stencil_" + name]
+        assert rect == tuple(PARAMS["stencil_vp"])
+        assert bits_equal(a, reference.render_raw(spec, True, ops, rect)), name
+        rect, a = got["stencil_" + name + "_mip1"]
+        assert bits_equal(a, reference.render_raw(spec, True, ops, rect, mip=1, quality=0)), name
 
     # raster graph, sRGB preview
     stops, gamma = PARAMS["raster_recipe"]
