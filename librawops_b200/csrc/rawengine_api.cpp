@@ -996,7 +996,7 @@ Tile DeviceNode::render_level(Rect bounds, RenderLevel level) const {
 // ------------------------------------------------------------------ graphs
 
 // RawEngine.cpp:1306-1333 (the ICC display output needs the LittleCMS backend,
-// which is outside this build: IccDisplay is rejected as unsupported)
+// which this library does not include: IccDisplay is rejected as unsupported)
 ImageGraph::ImageGraph(RawImage image, GraphRecipe recipe)
     : raw_image_(std::move(image)), source_bounds_(raw_image_->metadata().active_area), recipe_(recipe) {
     auto node = std::make_shared<RawUnpackNode>(*raw_image_);
@@ -1006,7 +1006,7 @@ ImageGraph::ImageGraph(RawImage image, GraphRecipe recipe)
         linear = std::make_shared<CameraToWorkingNode>(linear, *recipe.camera_color, source_bounds_);
     if (recipe.output_mode == OutputMode::SrgbPreview) linear = std::make_shared<WorkingToSrgbNode>(linear);
     else if (recipe.output_mode != OutputMode::LegacyBounded)
-        throw std::invalid_argument("ICC display output is not available in this build");
+        throw std::invalid_argument("ICC display output is not available in this library");
     auto tone = std::make_shared<ToneCurveNode>(linear, recipe.tone_shoulder, recipe.tone_gamma);
     output_ = recipe.output_mode == OutputMode::SrgbPreview
                   ? std::static_pointer_cast<const Node>(std::make_shared<SrgbEncodeNode>(tone))
@@ -1028,7 +1028,7 @@ ImageGraph::ImageGraph(std::shared_ptr<const Node> source, Rect bounds, GraphRec
     std::shared_ptr<const Node> linear = std::make_shared<ExposureNode>(source, recipe.exposure_stops);
     if (recipe.output_mode == OutputMode::SrgbPreview) linear = std::make_shared<WorkingToSrgbNode>(linear);
     else if (recipe.output_mode != OutputMode::LegacyBounded)
-        throw std::invalid_argument("ICC display output is not available in this build");
+        throw std::invalid_argument("ICC display output is not available in this library");
     auto tone = std::make_shared<ToneCurveNode>(linear, recipe.tone_shoulder, recipe.tone_gamma);
     output_ = recipe.output_mode == OutputMode::SrgbPreview
                   ? std::static_pointer_cast<const Node>(std::make_shared<SrgbEncodeNode>(tone))

@@ -59,11 +59,13 @@ struct Geo {
 
 __device__ __forceinline__ void flag(uint32_t* status, uint32_t key) { atomicMax(status, key); }
 
-// Stages this CTA's tile grown by (hx, hy), clipped to the window, as RGB
-// floats at smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c].
+// Stages this CTA's tile grown by (hx, hy), clipped to the window and to the
+// output grown by the halo (the reference's `needed` region, which a tile
+// reaching past the output's right or bottom edge must not read beyond), as
+// RGB floats at smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c].
 __device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, float* smem, int sx0, int sy0) {
-    const int x0 = max(G.wx, sx0), x1 = min(G.wx + G.ww, sx0 + ST_TILE + 2 * hx);
-    const int y0 = max(G.wy, sy0), y1 = min(G.wy + G.wh, sy0 + ST_TILE + 2 * hy);
+    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * hx), G.ox + G.ow + hx);
+    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * hy), G.oy + G.oh + hy);
     const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) * 3 : 0;
     bool bad = false;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -81,10 +83,10 @@ __device__ __forceinline__ double working_y(float r, float g, float b, double wr
     return __dadd_rn(__dadd_rn(Gc, __dmul_rn(wr, __dsub_rn(R, Gc))), __dmul_rn(wb, __dsub_rn(B, Gc)));
 }
 
-// Stages working Y (binary64) of the tile grown by h, clipped to the window.
+// Stages working Y (binary64) of the tile grown by h, clipped like stage_rgb.
 __device__ __forceinline__ void stage_y(const Geo& G, int h, double wr, double wb, double* plane, int sx0, int sy0) {
-    const int x0 = max(G.wx, sx0), x1 = min(G.wx + G.ww, sx0 + ST_TILE + 2 * h);
-    const int y0 = max(G.wy, sy0), y1 = min(G.wy + G.wh, sy0 + ST_TILE + 2 * h);
+    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * h), G.ox + G.ow + h);
+    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * h), G.oy + G.oh + h);
     const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) : 0;
     bool bad = false;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {

@@ -11,6 +11,7 @@
 // The checks mirror the reference's own core, spatial, geometry and scheduler
 // tests (tests/core_tests.cpp, spatial_ops_tests.cpp, rotate_tests.cpp,
 // cubic_resize_tests.cpp of tylermcm/librawops) on this path.
+#include <rawengine/EditOps.hpp>
 #include <rawengine/GeometryOps.hpp>
 #include <rawengine/ImageAnalysis.hpp>
 #include <rawengine/RawEngine.hpp>
@@ -459,6 +460,186 @@ void stencil_checks(const std::string& dir, const std::map<std::string, std::vec
                                         "texture_rejects_empty_bounds");
 }
 
+// ------------------------------------------------------ operation factory
+
+EditValue num(double v) { return EditValue{v}; }
+EditValue integer(std::int64_t v) { return EditValue{v}; }
+EditValue str(const char* v) { return EditValue{std::string(v)}; }
+EditValue list(std::initializer_list<double> v) {
+    EditValue::Array a;
+    for (double x : v) a.push_back(num(x));
+    return EditValue{a};
+}
+EditOperation operation(const char* type, EditValue::Object params,
+                        EditDomain out = EditDomain::SceneLinearProPhotoD50) {
+    EditOperation op;
+    op.id = std::string("op-") + type;
+    op.type_id = type;
+    op.parameters = std::move(params);
+    op.output_domain = out;
+    op.inputs = {{"image", "source"}};
+    return op;
+}
+EditValue knots(const std::vector<CurvePoint>& k) {
+    EditValue::Array a;
+    for (const auto& p : k) a.push_back(EditValue{EditValue::Array{num(p.x), num(p.y)}});
+    return EditValue{a};
+}
+
+// Chains built by build_operation render exactly as the same chains built
+// from the node constructors (EditGraph.cpp:1655-1733).
+void factory_checks(const std::map<std::string, std::vector<double>>& P, const RawImage& raw, Rect area) {
+    Renderer renderer;
+    const auto cam = camera(P, WorkingSpace::LinearProPhotoD50);
+    EditValue::Array m;
+    for (double v : cam.camera_to_xyz_d50) m.push_back(num(v));
+    auto same_render = [&](const Node& a, const Node& b, Rect bounds, RenderRequest req) {
+        return bit_equal(renderer.render_image(a, bounds, req).rgb, renderer.render_image(b, bounds, req).rgb) &&
+               a.output_descriptor() == b.output_descriptor();
+    };
+    auto menon = std::make_shared<RawUnpackNode>(raw, RawDemosaicIdentity{"rawengine.menon_base", 1});
+    const WorkingSpace pp = WorkingSpace::LinearProPhotoD50;
+    // point chain: WB -> camera-to-working -> curves -> sRGB
+    std::shared_ptr<const Node> f = build_operation(
+        operation("rawengine.white_balance", {{"red_gain", num(1.9)}, {"green_gain", integer(1)}, {"blue_gain", num(1.4)}}),
+        menon, pp, area);
+    f = build_operation(operation("rawengine.exposure", {{"stops", num(0.25)}}), f, pp, area);
+    f = build_operation(operation("rawengine.camera_to_working", {{"matrix", EditValue{m}}}), f, pp, area);
+    const std::vector<CurvePoint> curve{{0, 0}, {0.3, 0.4}, {0.7, 0.75}, {1, 1}};
+    f = build_operation(operation("rawengine.curves_extended",
+                                  {{"master", knots(curve)}, {"red", knots({{0, 0}, {1, 1}})},
+                                   {"green", knots({{0, 0}, {0.5, 0.55}, {1, 1}})}, {"blue", knots({{0, 0}, {1, 1}})},
+                                   {"interpolation", str("shape_preserving_cubic")}}),
+                        f, pp, area);
+    std::shared_ptr<const Node> d = std::make_shared<WhiteBalanceNode>(menon, 1.9f, 1.0f, 1.4f);
+    d = std::make_shared<ExposureNode>(d, 0.25f);
+    d = std::make_shared<CameraToWorkingNode>(d, cam, area);
+    ExtendedCurvesSettings cs;
+    cs.master.knots = curve;
+    cs.channels[1].knots = {{0, 0}, {0.5, 0.55}, {1, 1}};
+    cs.interpolation = CurveInterpolation::ShapePreservingCubic;
+    d = std::make_shared<ExtendedCurvesNode>(d, cs);
+    const Rect vp{area.x + 5, area.y + 4, 60, 45};
+    const RenderLevel mip1{1, RenderQuality::Preview};
+    check(same_render(*f, *d, area, RenderRequest{vp, 32}) &&
+              same_render(*f, *d, area, RenderRequest{{0, 0, 30, 20}, 32, mip1}),
+          "factory_point_chain");
+    const auto working_f = f, working_d = d;
+    auto srgb_f = build_operation(operation("rawengine.srgb_encode", {}),
+                                  build_operation(operation("rawengine.tone_curve", {{"shoulder", num(0.3)}, {"gamma", num(2.2)}}),
+                                                  build_operation(operation("rawengine.working_to_srgb", {}), f, pp, area),
+                                                  pp, area),
+                                  pp, area);
+    auto srgb_d = std::make_shared<SrgbEncodeNode>(
+        std::make_shared<ToneCurveNode>(std::make_shared<WorkingToSrgbNode>(d), 0.3f, 2.2f));
+    check(same_render(*srgb_f, *srgb_d, area, RenderRequest{vp, 32}), "factory_srgb_chain");
+    // spatial, stencil and geometry operations over the working image
+    struct Case {
+        const char* name;
+        std::shared_ptr<const Node> f, d;
+    };
+    const Rect image{0, 0, area.width, area.height};
+    ConvolutionKernel k{3, 3, {0.0, -0.25, 0.0, -0.25, 2.0, -0.25, 0.0, -0.25, 0.0}};
+    EditValue::Array kc;
+    for (double v : k.coefficients) kc.push_back(num(v));
+    const uint32_t cw = (area.width + 1) / 2, ch = (area.height + 2) / 3;
+    std::vector<Case> cases = {
+        {"guided_filter",
+         build_operation(operation("rawengine.guided_filter_working_y", {{"radius", integer(3)}, {"epsilon", num(0.001)}}),
+                         working_f, pp, area),
+         std::make_shared<WorkingYGuidedFilterNode>(working_d, area, WorkingYGuidedFilterSettings{3, 0.001})},
+        {"sharpen", build_operation(operation("rawengine.sharpen", {{"amount", num(0.8)}, {"radius", integer(2)}}),
+                                    working_f, pp, area),
+         std::make_shared<SharpenNode>(working_d, area, SharpenSettings{0.8, 2})},
+        {"clarity", build_operation(operation("rawengine.clarity", {{"amount", num(-0.4)}, {"radius", integer(4)}}),
+                                    working_f, pp, area),
+         std::make_shared<ClarityNode>(working_d, area, ClaritySettings{-0.4, 4})},
+        {"texture", build_operation(operation("rawengine.texture", {{"amount", num(0.5)}, {"scale", integer(2)}}),
+                                    working_f, pp, area),
+         std::make_shared<TextureNode>(working_d, area, TextureSettings{0.5, 2})},
+        {"convolution",
+         build_operation(operation("rawengine.convolution", {{"width", integer(3)}, {"height", integer(3)},
+                                                             {"coefficients", EditValue{kc}}, {"border", str("replicate")}}),
+                         working_f, pp, area),
+         std::make_shared<ConvolutionNode>(working_d, area, k)},
+        {"working_space_convert",
+         build_operation(operation("rawengine.working_space_convert", {}, EditDomain::SceneLinearRec2020D65), working_f, pp,
+                         area),
+         std::make_shared<WorkingSpaceConvertNode>(working_d, WorkingSpace::LinearRec2020D65)},
+        {"output_clip", build_operation(operation("rawengine.output_clip", {}), working_f, pp, area),
+         std::make_shared<OutputClipNode>(working_d)},
+    };
+    for (const auto& c : cases)
+        check(same_render(*c.f, *c.d, area, RenderRequest{vp, 32}), std::string("factory_") + c.name);
+    auto cubic_f = build_operation(operation("rawengine.cubic_resize", {{"width", integer(cw)}, {"height", integer(ch)}}),
+                                   working_f, pp, area);
+    auto cubic_d = std::make_shared<CubicResizeNode>(working_d, area, CubicResizeSettings{cw, ch});
+    check(same_render(*cubic_f, *cubic_d, Rect{0, 0, cw, ch}, RenderRequest{{0, 0, cw, ch}, 32}), "factory_cubic");
+    auto rot_f = build_operation(operation("rawengine.rotate", {{"angle_degrees", num(-23.5)}}), working_f, pp, area);
+    auto rot_d = std::make_shared<RotateNode>(working_d, area, RotateSettings{-23.5});
+    check(same_render(*rot_f, *rot_d, image, RenderRequest{{3, 2, 40, 30}, 32}), "factory_rotate");
+    // the legacy fixed chain, both output modes
+    auto bil = std::make_shared<RawUnpackNode>(raw);
+    for (const char* mode : {"legacy_bounded", "srgb_preview"}) {
+        EditValue::Object recipe{{"red_gain", num(1.7)},      {"green_gain", num(1.0)},  {"blue_gain", num(1.3)},
+                                 {"exposure_stops", num(0.4)}, {"tone_shoulder", num(0.25)}, {"tone_gamma", num(2.0)},
+                                 {"output_mode", str(mode)}};
+        const bool srgb = std::string(mode) == "srgb_preview";
+        if (srgb) {
+            recipe.emplace("camera_to_xyz_d50", EditValue{m});
+            recipe.emplace("camera_target", str("linear_prophoto_d50"));
+        }
+        auto lf = build_operation(operation("rawengine.legacy.fixed_chain", {{"recipe", EditValue{recipe}}}), bil, pp, area);
+        std::shared_ptr<const Node> ld = std::make_shared<ExposureNode>(std::make_shared<WhiteBalanceNode>(bil, 1.7f, 1.0f, 1.3f), 0.4f);
+        if (srgb) ld = std::make_shared<WorkingToSrgbNode>(std::make_shared<CameraToWorkingNode>(ld, cam));
+        auto tone = std::make_shared<ToneCurveNode>(ld, 0.25f, 2.0f);
+        ld = srgb ? std::static_pointer_cast<const Node>(std::make_shared<SrgbEncodeNode>(tone))
+                  : std::static_pointer_cast<const Node>(std::make_shared<OutputClipNode>(tone));
+        check(same_render(*lf, *ld, area, RenderRequest{vp, 32}), std::string("factory_legacy_") + mode);
+    }
+    // a disabled operation is its input
+    auto off = operation("rawengine.exposure", {{"stops", num(3.0)}});
+    off.enabled = false;
+    check(build_operation(off, working_f, pp, area) == working_f, "factory_disabled_passes_input");
+}
+
+// Factory rejections (host only).
+void factory_validation(const std::shared_ptr<const Node>& working, Rect area) {
+    const WorkingSpace pp = WorkingSpace::LinearProPhotoD50;
+    auto rejects = [&](const EditOperation& op, const std::string& name) {
+        expect_throw<std::invalid_argument>([&] { (void)build_operation(op, working, pp, area); }, name);
+    };
+    rejects(operation("rawengine.vibrance", {{"amount", num(0.2)}}), "factory_rejects_unsupported_type");
+    rejects(operation("rawengine.exposure", {}), "factory_rejects_missing_scalar");
+    rejects(operation("rawengine.exposure", {{"stops", num(1e300)}}), "factory_rejects_float32_range");
+    rejects(operation("rawengine.sharpen", {{"amount", num(0.5)}}), "factory_rejects_sharpen_fields");
+    rejects(operation("rawengine.sharpen", {{"amount", num(0.5)}, {"radius", num(2.0)}}), "factory_rejects_float_radius");
+    rejects(operation("rawengine.clarity", {{"amount", num(2.0)}, {"radius", integer(2)}}), "factory_rejects_clarity_amount");
+    rejects(operation("rawengine.guided_filter_working_y", {{"radius", num(2.5)}, {"epsilon", num(0.01)}}),
+            "factory_rejects_fractional_gf_radius");
+    rejects(operation("rawengine.convolution", {{"width", integer(1)}, {"height", integer(1)}, {"coefficients", list({1})},
+                                                {"border", str("zero")}}),
+            "factory_rejects_border");
+    rejects(operation("rawengine.curves_extended", {{"master", knots({{0, 0}, {1, 1}})}, {"red", knots({{0, 0}, {1, 1}})},
+                                                    {"green", knots({{0, 0}, {1, 1}})}, {"blue", knots({{0, 0}, {1, 1}})},
+                                                    {"interpolation", str("spline")}}),
+            "factory_rejects_interpolation");
+    rejects(operation("rawengine.camera_to_working", {{"matrix", list({1, 0, 0})}}), "factory_rejects_matrix_size");
+    rejects(operation("rawengine.working_space_convert", {}, EditDomain::DisplayEncodedSrgb), "factory_rejects_target");
+    auto masked = operation("rawengine.exposure", {{"stops", num(1.0)}});
+    masked.masks = {{"mask", "brush"}};
+    rejects(masked, "factory_rejects_masks");
+    auto blended = operation("rawengine.exposure", {{"stops", num(1.0)}});
+    blended.opacity = 0.5;
+    rejects(blended, "factory_rejects_opacity");
+    EditValue::Object recipe{{"red_gain", num(1)},       {"green_gain", num(1)},    {"blue_gain", num(1)},
+                             {"exposure_stops", num(0)}, {"tone_shoulder", num(0.2)}, {"tone_gamma", num(2)},
+                             {"output_mode", str("legacy_bounded")}, {"unknown", num(1)}};
+    rejects(operation("rawengine.legacy.fixed_chain", {{"recipe", EditValue{recipe}}}), "factory_rejects_legacy_field");
+    check(descriptor_domain(working->output_descriptor()) == EditDomain::SceneLinearProPhotoD50,
+          "factory_descriptor_domain");
+}
+
 int run_render(const std::string& dir) {
     const auto P = read_params(dir + "/params.txt");
     const RawImage raw = make_raw(P, dir);
@@ -747,6 +928,7 @@ int run_render(const std::string& dir) {
         }
     }
     stencil_checks(dir, P, ctw, area);
+    factory_checks(P, raw, area);
     histogram_checks(graph.output_node(), area);
     return failures ? 1 : 0;
 }
@@ -882,6 +1064,9 @@ int run_validate() {
             },
             "node_graph_has_no_raw_image");
     }
+    factory_validation(std::make_shared<CameraToWorkingNode>(
+                           bil, CameraColorTransform{{1, 0, 0, 0, 1, 0, 0, 0, 1}, WorkingSpace::LinearProPhotoD50}, area),
+                       area);
     // scheduler argument checks (no work is queued)
     {
         expect_throw<std::invalid_argument>([&] { (void)TileScheduler(0, 4); }, "scheduler_zero_workers");
