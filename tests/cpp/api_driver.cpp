@@ -416,8 +416,8 @@ void stencil_checks(const std::string& dir, const std::map<std::string, std::vec
         expect_throw<std::out_of_range>(
             [&] { (void)node->input_region(Rect{area.x + area.width - 2, area.y, 5, 5}, area); },
             "stencil_rejects_outside_" + name);
-        check(node->supports_level(mip1) && node->supports_level({0, RenderQuality::Preview}) &&
-                  !node->supports_level({1, RenderQuality::Final}),
+        check(node->supports_level(mip1) && node->supports_level({}) && !node->supports_level({1, RenderQuality::Final}) &&
+                  node->supports_level({0, RenderQuality::Preview}) == working->supports_level({0, RenderQuality::Preview}),
               "stencil_levels_" + name);
     }
     // pass-through: zero amounts and an identity kernel return the input pixels
@@ -566,8 +566,12 @@ void factory_checks(const std::map<std::string, std::vector<double>>& P, const R
          build_operation(operation("rawengine.working_space_convert", {}, EditDomain::SceneLinearRec2020D65), working_f, pp,
                          area),
          std::make_shared<WorkingSpaceConvertNode>(working_d, WorkingSpace::LinearRec2020D65)},
-        {"output_clip", build_operation(operation("rawengine.output_clip", {}), working_f, pp, area),
-         std::make_shared<OutputClipNode>(working_d)},
+        {"tone_output_clip",
+         build_operation(operation("rawengine.output_clip", {}),
+                         build_operation(operation("rawengine.tone_curve", {{"shoulder", num(0.2)}, {"gamma", num(1.8)}}),
+                                         working_f, pp, area),
+                         pp, area),
+         std::make_shared<OutputClipNode>(std::make_shared<ToneCurveNode>(working_d, 0.2f, 1.8f))},
     };
     for (const auto& c : cases)
         check(same_render(*c.f, *c.d, area, RenderRequest{vp, 32}), std::string("factory_") + c.name);
