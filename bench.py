@@ -499,22 +499,23 @@ def _config_legs(render, workloads, torch, dev, stream, peak, reps):
 
 
 def _mixed_batch(render, workloads, torch, dev, stream, reps):
-    """The mixed batch (16 RAWs, ~3,000 tiles, mip 0/1/2): batched persistent
-    launch vs the same requests launched one by one, device time per pass."""
+    """The mixed batch (16 RAWs, ~3,000 tiles, mip 0/1/2, a fifth of the
+    viewports through a cubic resize to a 2048 long edge or a rotation):
+    batched persistent launch vs the same requests launched one by one,
+    device time per pass."""
     images, recipes, tiles = workloads.mixed_batch()
     imgs = []
     for im in images:
         meta = render.Metadata(im.width, im.height, im.stride, im.pattern, im.phase[0], im.phase[1], im.active,
                                im.black, (im.white,) * 4)
         imgs.append(render.Image(meta, render.synthetic_samples(im, device=dev)))
-    pipes = [workloads.mixed_pipeline(im, r) for im, r in zip(images, recipes)]
     sizes = [t.viewport[2] * t.viewport[3] * 3 for t in tiles]
     arena = torch.empty(sum(sizes), dtype=torch.float32, device=dev)
     outs, off = [], 0
     for t, n in zip(tiles, sizes):
         outs.append(arena[off:off + n].view(t.viewport[3], t.viewport[2], 3))
         off += n
-    reqs = [(imgs[t.image], pipes[t.recipe], t.viewport, t.mip, t.quality, o) for t, o in zip(tiles, outs)]
+    reqs = workloads.mixed_requests(render, imgs, images, recipes, tiles, outs)
     batch = render.Batch().plan(reqs)
     with torch.cuda.stream(stream):
         tuned = batch.autotune(reps=3, stream=stream)
@@ -538,6 +539,7 @@ def _mixed_batch(render, workloads, torch, dev, stream, reps):
     algo = info["raw_bytes"] + info["output_bytes"]
     out_px = info["output_pixels"]
     result = {"requests": info["requests"], "reduced_requests": info["reduced_requests"],
+              "geometry_requests": info["geometry_requests"],
               "tiles_queued": info["tiles"], "output_mpix": round(out_px / 1e6, 2),
               "native_mpix": round(info["native_pixels"] / 1e6, 2),
               "batched_ms": round(batched_ms, 4), "per_request_ms": round(per_ms, 4),

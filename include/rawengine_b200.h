@@ -79,6 +79,23 @@ RE_API re_status re_image_create(re_raw_metadata* meta, const uint16_t* samples,
 RE_API re_status re_image_wrap_device(re_raw_metadata* meta, const uint16_t* device_samples,
                                       size_t count, re_image** out);
 RE_API re_status re_image_destroy(re_image* image);
+
+/* Source ingest (SourceFingerprint.cpp:65-101): the canonical content
+ * fingerprint, SHA-256 of the reference's byte stream (version tag, metadata
+ * little-endian, the active area's samples row by row), into digest[32].
+ * re_fingerprint_raw normalizes *meta like re_image_create.  The raster form
+ * hashes width, height, working space (0 ProPhoto D50, 1 Rec.2020 D65) and
+ * the bits of every float (row stride in pixels, 0 = width). */
+RE_API re_status re_fingerprint_raw(re_raw_metadata* meta, const uint16_t* samples, size_t count,
+                                    uint8_t digest[32]);
+RE_API re_status re_fingerprint_raster(uint32_t width, uint32_t height, size_t row_stride_pixels,
+                                       uint32_t working_space, const float* pixels, uint8_t digest[32]);
+/* re_image_create whose upload runs while the fingerprint is computed: the
+ * plane goes to the device in chunks through pinned staging buffers, each
+ * chunk hashed on the host while its copy is in flight.  No counterpart in
+ * the reference (its sources stay in host memory). */
+RE_API re_status re_image_create_fingerprinted(re_raw_metadata* meta, const uint16_t* samples, size_t count,
+                                               re_image** out, uint8_t digest[32]);
 RE_API re_status re_image_metadata(const re_image* image, re_raw_metadata* out);
 
 /* Metadata normalization/validation only (no device work): RawEngine.cpp:223-250. */
@@ -274,6 +291,19 @@ typedef struct re_batch_item {
     uint32_t mip, quality;
     float* out;                 /* device memory */
     size_t out_row_stride;      /* floats, >= 3 * viewport.width */
+    /* Geometry requests (CubicResizeNode / RotateNode over a RAW chain,
+     * GeometryOps.cpp:42-174, 346-513): `desc` renders the RAW source's point
+     * stages at native resolution (its anchor is ignored) over the active
+     * area, whose extent is the geometry's input; the geometry maps it to its
+     * canvas (cubic: canvas_width x canvas_height; rotation: the input's
+     * extent) at level `mip` (1/2 with quality Preview: native then the
+     * footprint average); then the stages of `post` (point stages only, may
+     * be NULL) run at the level.  viewport is in canvas level coordinates.
+     * geometry 0 = a plain RAW request (the fields below are ignored). */
+    uint32_t geometry;          /* 0 none, 1 cubic resize, 2 rotation */
+    uint32_t canvas_width, canvas_height;
+    double angle_degrees;
+    const re_render_desc* post;
 } re_batch_item;
 
 typedef struct re_batch_options {
@@ -295,13 +325,15 @@ typedef struct re_batch_info {
     uint64_t native_pixels, output_pixels;
     uint64_t raw_bytes, output_bytes;    /* algorithmic: 2 B per native pixel, 12 B per output pixel */
     re_batch_options options;
+    uint32_t geometry_requests;          /* requests with a cubic resize or rotation */
 } re_batch_info;
 
 typedef struct re_batch re_batch;
 
 RE_API re_status re_batch_create(re_batch** out);
 RE_API re_status re_batch_destroy(re_batch* batch);
-/* Validates every item like re_render_raw_async, merges requests of one
+/* Validates every item like re_render_raw_async (geometry items like
+ * re_cubic_resize_window / re_rotate_window), merges requests of one
  * image, description, level and row stride whose viewports tile a rectangle
  * and whose outputs lie where one render of it would write (the pixels are the
  * same either way), lays out the tile queue and the reduction blocks, uploads

@@ -39,6 +39,7 @@ EXPORTS = [
     "re_diff_point_grad_count", "re_diff_detail_forward", "re_diff_detail_backward",
     "re_histogram_reset", "re_histogram_rgb", "re_histogram_extremum",
     "re_sharpen_window", "re_clarity_window", "re_texture_window", "re_convolution_window",
+    "re_fingerprint_raw", "re_fingerprint_raster", "re_image_create_fingerprinted",
 ]
 
 
@@ -83,7 +84,9 @@ class RenderStats(C.Structure):
 
 class BatchItem(C.Structure):
     _fields_ = [("image", C.c_void_p), ("desc", C.POINTER(RenderDesc)), ("viewport", Rect), ("mip", C.c_uint32),
-                ("quality", C.c_uint32), ("out", C.c_void_p), ("out_row_stride", C.c_size_t)]
+                ("quality", C.c_uint32), ("out", C.c_void_p), ("out_row_stride", C.c_size_t),
+                ("geometry", C.c_uint32), ("canvas_width", C.c_uint32), ("canvas_height", C.c_uint32),
+                ("angle_degrees", C.c_double), ("post", C.POINTER(RenderDesc))]
 
 
 class BatchOptions(C.Structure):
@@ -96,7 +99,7 @@ class BatchInfo(C.Structure):
                 ("tiles", C.c_uint32),
                 ("reduce_blocks", C.c_uint32), ("grid", C.c_uint32), ("native_pixels", C.c_uint64),
                 ("output_pixels", C.c_uint64), ("raw_bytes", C.c_uint64), ("output_bytes", C.c_uint64),
-                ("options", BatchOptions)]
+                ("options", BatchOptions), ("geometry_requests", C.c_uint32)]
 
 
 class DiffPointParams(C.Structure):
@@ -182,6 +185,9 @@ def lib() -> C.CDLL:
                                        vp]
         L.re_histogram_extremum.argtypes = [C.c_uint64, C.c_int, C.POINTER(C.c_float)]
         L.re_histogram_extremum.restype = C.c_int
+        L.re_fingerprint_raw.argtypes = [C.POINTER(RawMetadata), vp, sz, vp]
+        L.re_fingerprint_raster.argtypes = [u32, u32, sz, u32, vp, vp]
+        L.re_image_create_fingerprinted.argtypes = [C.POINTER(RawMetadata), vp, sz, C.POINTER(vp), vp]
         L.re_sharpen_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, vp, sz, vp]
         L.re_clarity_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, u32, vp, sz, vp]
         L.re_texture_window.argtypes = [vp, sz, Rect, Rect, Rect, C.c_double, u32, u32, vp, sz, vp]

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "re_batch.cuh"
+#include "re_geometry.cuh"
 
 namespace re {
 cudaError_t launch_demosaic(uint32_t demosaic, const DevRaw& raw, int ox, int oy, int ow, int oh,
@@ -40,6 +41,7 @@ void set_last_error(const std::string& msg);
 re_status render_plan(const re_image* img, const re_render_desc* desc, re_rect viewport, uint32_t mip,
                       uint32_t quality, DevProgram& P, re_rect& native, const DevRaw** raw);
 re_status status_key_to_error(uint32_t key);
+re_status stage_program(const re_render_desc* desc, DevProgram& P);
 }  // namespace re
 
 using namespace re;
@@ -64,9 +66,23 @@ struct LaunchGroup {
     uint32_t grid;
 };
 
+// One geometry request as the per-request form launches it: its support was
+// rendered by the RAW request listed with the others; then the geometry
+// passes, then (reduce) the footprint average and the later stages.
+struct GeoSingle {
+    GeoRequest request;
+    bool reduce;
+    DevProgram post;
+    uint32_t mip;
+    re_rect viewport;
+    float* out;
+    size_t out_stride;
+};
+
 struct re_batch {
     BatchShape shape{};
-    std::vector<re_batch_item> items;
+    std::vector<re_batch_item> items;      // RAW requests, geometry supports included
+    std::vector<re_batch_item> given;      // the caller's requests
     std::vector<PerRequest> singles;       // the requests as given
     std::vector<PerRequest> directs;       // the merged renders
     bool direct = false;                   // dispatch 3: plain launches of the merged renders
@@ -82,6 +98,15 @@ struct re_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool planned = false;
+    // geometry requests: tables and scratch in their own device block
+    char* geo = nullptr;
+    size_t geo_cap = 0;
+    const GeoRequest* geo_requests = nullptr;
+    const GeoBlock* geo_pass1 = nullptr;
+    const GeoBlock* geo_pass2 = nullptr;
+    uint32_t geo_n1 = 0, geo_n2 = 0;
+    std::vector<LaunchGroup> geo_groups;   // footprint averages and later stages (reduce launches)
+    std::vector<GeoSingle> geo_singles;
 };
 
 namespace {
@@ -150,11 +175,38 @@ re_status launch_singles(re_batch* b, const std::vector<PerRequest>& list, cudaS
     return RE_OK;
 }
 
+// The geometry passes of every geometry request, then their footprint
+// averages and later stages (after the RAW renders of their supports).
+re_status enqueue_geometry(re_batch* b, cudaStream_t stream) {
+    if (b->geo_n1 || b->geo_n2)
+        BT_CUDA(launch_geometry_batch(b->geo_requests, b->geo_pass1, b->geo_n1, b->geo_pass2, b->geo_n2, b->head,
+                                      stream));
+    for (const LaunchGroup& g : b->geo_groups) BT_CUDA(launch_batch_group(g.params, 0, true, stream));
+    return RE_OK;
+}
+
 re_status enqueue(re_batch* b, cudaStream_t stream) {
-    if (b->direct) return launch_singles(b, b->directs, stream);
+    if (b->direct) {
+        re_status s = launch_singles(b, b->directs, stream);
+        return s ? s : enqueue_geometry(b, stream);
+    }
     BT_CUDA(cudaMemsetAsync(b->head, 0, b->head_words * sizeof(uint32_t), stream));
     for (const LaunchGroup& g : b->groups) BT_CUDA(launch_batch_group(g.params, g.grid, false, stream));
+    re_status s = enqueue_geometry(b, stream);
+    if (s) return s;
     for (const LaunchGroup& g : b->groups) BT_CUDA(launch_batch_group(g.params, 0, true, stream));
+    return RE_OK;
+}
+
+// The per-request form of the geometry requests (after launch_singles).
+re_status launch_geo_singles(re_batch* b, cudaStream_t stream) {
+    for (const GeoSingle& q : b->geo_singles) {
+        BT_CUDA(launch_geometry_single(q.request, b->head, stream));
+        if (q.reduce)
+            BT_CUDA(launch_mip_reduce(q.request.out, q.request.nw, q.request.nh, (size_t)q.request.out_stride,
+                                      (int)q.mip, (int)q.viewport.width, (int)q.viewport.height, 0,
+                                      (int)q.post.count, q.post, q.out, q.out_stride, b->head, stream, nullptr));
+    }
     return RE_OK;
 }
 
@@ -208,6 +260,227 @@ std::vector<re_batch_item> merge_items(std::vector<re_batch_item> v) {
     return v;
 }
 
+// Plans the geometry requests of a batch (GeometryOps.cpp:42-174, 346-513):
+// each one's input support becomes a RAW request (appended to `supports`)
+// rendered into the batch's geometry block, the geometry passes of all of
+// them run as two launches over a block table, and the requests that reduce
+// to mip 1/2 or have later stages get reduction tasks in their own launch
+// groups.  Status pointers of those groups are set once the batch head exists.
+re_status plan_geometry(re_batch* b, const std::vector<re_batch_item>& items, std::vector<re_batch_item>& supports,
+                        re_batch_info& info) {
+    struct G {
+        size_t item;
+        GeoPlan plan;
+        re_rect area;
+        DevProgram post;
+        bool reduce;
+        size_t o_axes, o_support, o_h, o_native;
+    };
+    std::vector<G> gs;
+    b->geo_singles.clear();
+    b->geo_groups.clear();
+    b->geo_n1 = b->geo_n2 = 0;
+    size_t tables = 0, data = 0;
+    auto take = [](size_t& off, size_t bytes) {
+        const size_t at = off;
+        off = align256(off + bytes);
+        return at;
+    };
+    for (size_t i = 0; i < items.size(); ++i) {
+        const re_batch_item& it = items[i];
+        if (!it.image || !it.desc) return fail(RE_INVALID_ARGUMENT, "null render arguments");
+        if (it.geometry > 2) return fail(RE_INVALID_ARGUMENT, "unknown batch geometry");
+        const bool native_level = it.mip == 0 && it.quality == 1;
+        const bool reduced = (it.mip == 1 || it.mip == 2) && it.quality == 0;
+        if (!native_level && !reduced) return fail(RE_INVALID_ARGUMENT, "node does not support this render level");
+        re_raw_metadata meta{};
+        re_status s = re_image_metadata(it.image, &meta);
+        if (s) return s;
+        G g{};
+        g.item = i;
+        g.area = meta.active_area;
+        s = it.geometry == 1 ? plan_cubic(g.area.width, g.area.height, it.canvas_width, it.canvas_height, it.viewport,
+                                          it.mip, g.plan)
+                             : plan_rotate(g.area.width, g.area.height, it.angle_degrees, it.viewport, it.mip, g.plan,
+                                           false);
+        if (s) return s;
+        DevProgram pre;
+        if ((s = stage_program(it.desc, pre))) return s;
+        std::memset(&g.post, 0, sizeof(g.post));
+        g.post.anchor = -1;
+        if (it.post && (s = stage_program(it.post, g.post))) return s;
+        g.post.anchor = -1;
+        if (!it.viewport.width || !it.viewport.height) continue;
+        if (!it.out) return fail(RE_INVALID_ARGUMENT, "null render arguments");
+        if (it.out_row_stride < (size_t)it.viewport.width * 3)
+            return fail(RE_INVALID_ARGUMENT, "output row stride too small");
+        g.reduce = it.mip != 0 || g.post.count != 0;
+        const re_rect& sp = g.plan.support;
+        g.o_axes = take(tables, (g.plan.xs.size() + g.plan.ys.size()) * sizeof(Axis));
+        g.o_support = take(data, (size_t)sp.width * sp.height * 3 * sizeof(float));
+        g.o_h = take(data, (size_t)g.plan.rows * g.plan.native.width * 3 * sizeof(double));
+        g.o_native = take(data, g.reduce ? (size_t)g.plan.native.width * g.plan.native.height * 3 * sizeof(float) : 0);
+        info.output_pixels += (uint64_t)it.viewport.width * it.viewport.height;
+        info.reduced_requests += it.mip ? 1 : 0;
+        gs.push_back(std::move(g));
+    }
+    info.geometry_requests = (uint32_t)gs.size();
+    if (gs.empty()) return RE_OK;
+    // block tables and reduction groups (host), then one device block:
+    // [requests | pass 1 | pass 2 | groups' tasks | axes] [supports, H, natives]
+    std::vector<GeoRequest> reqs(gs.size());
+    std::vector<GeoBlock> pass1, pass2;
+    struct RGroup {
+        std::map<const re_render_desc*, int> programs;
+        std::vector<DevProgram> program_list;
+        std::vector<ReduceTask> tasks;
+        std::vector<uint32_t> unit_task;
+    };
+    std::vector<RGroup> rgroups;
+    for (size_t k = 0; k < gs.size(); ++k) {
+        const G& g = gs[k];
+        const re_batch_item& it = items[g.item];
+        GeoRequest& R = reqs[k];
+        R = GeoRequest{};
+        R.kind = g.plan.kind;
+        R.nx0 = (int)g.plan.native.x;
+        R.ny0 = (int)g.plan.native.y;
+        R.nw = (int)g.plan.native.width;
+        R.nh = (int)g.plan.native.height;
+        R.src_x0 = (int)g.plan.support.x;
+        R.src_y0 = (int)g.plan.support.y;
+        R.row0 = (int)g.plan.row0;
+        R.rows = (int)g.plan.rows;
+        R.rot = g.plan.rot;
+        R.src_stride = (uint64_t)g.plan.support.width * 3;
+        R.out_stride = g.reduce ? (uint64_t)R.nw * 3 : (uint64_t)it.out_row_stride;
+        const uint32_t bx = (uint32_t)((R.nw + GEO_BW - 1) / GEO_BW);
+        const uint32_t by1 = (uint32_t)(((R.kind == 1 ? R.rows : R.nh) + GEO_BH - 1) / GEO_BH);
+        if (bx > 65535 || by1 > 65535 || (uint32_t)((R.nh + GEO_BH - 1) / GEO_BH) > 65535)
+            return fail(RE_LENGTH_ERROR, "geometry request too large for one batch");
+        for (uint32_t y = 0; y < by1; ++y)
+            for (uint32_t x = 0; x < bx; ++x) pass1.push_back({(uint32_t)k, (uint16_t)x, (uint16_t)y});
+        if (R.kind == 1)
+            for (uint32_t y = 0; y < (uint32_t)((R.nh + GEO_BH - 1) / GEO_BH); ++y)
+                for (uint32_t x = 0; x < bx; ++x) pass2.push_back({(uint32_t)k, (uint16_t)x, (uint16_t)y});
+        if (g.reduce) {
+            if (rgroups.empty() || (!rgroups.back().programs.count(it.post) &&
+                                    rgroups.back().programs.size() == (size_t)BATCH_PROGRAMS))
+                rgroups.emplace_back();
+            RGroup& rg = rgroups.back();
+            if (!rg.programs.count(it.post)) {
+                rg.programs.emplace(it.post, (int)rg.program_list.size());
+                rg.program_list.push_back(g.post);
+            }
+            ReduceTask q{};
+            q.program = rg.programs.at(it.post);
+            q.scale = 1 << it.mip;
+            q.stage_begin = 0;
+            q.stage_end = (int)g.post.count;
+            q.nw = R.nw;
+            q.nh = R.nh;
+            q.ow = (int)it.viewport.width;
+            q.oh = (int)it.viewport.height;
+            q.tiles_x = (q.ow + RD_TW - 1) / RD_TW;
+            q.unit_begin = (uint32_t)rg.unit_task.size();
+            q.native_stride = (uint64_t)R.nw * 3;
+            q.out = it.out;
+            q.out_stride = it.out_row_stride;
+            const uint32_t blocks = (uint32_t)q.tiles_x * (uint32_t)((q.oh + RD_TH - 1) / RD_TH);
+            rg.unit_task.insert(rg.unit_task.end(), blocks, (uint32_t)rg.tasks.size());
+            rg.tasks.push_back(q);   // native pointer filled below
+        }
+    }
+    const size_t o_req = take(tables, reqs.size() * sizeof(GeoRequest));
+    const size_t o_p1 = take(tables, pass1.size() * sizeof(GeoBlock));
+    const size_t o_p2 = take(tables, pass2.size() * sizeof(GeoBlock));
+    std::vector<std::pair<size_t, size_t>> o_rg(rgroups.size());
+    for (size_t r = 0; r < rgroups.size(); ++r) {
+        o_rg[r].first = take(tables, rgroups[r].tasks.size() * sizeof(ReduceTask));
+        o_rg[r].second = take(tables, rgroups[r].unit_task.size() * sizeof(uint32_t));
+    }
+    const size_t total = tables + data;
+    if (total > b->geo_cap) {
+        release_graph(b);
+        if (b->geo) BT_CUDA(cudaFree(b->geo));
+        b->geo = nullptr;
+        b->geo_cap = 0;
+        BT_CUDA(cudaMalloc(&b->geo, total));
+        b->geo_cap = total;
+    }
+    char* base = b->geo;
+    char* dbase = base + tables;
+    std::vector<char> host(tables);
+    // fill device pointers, supports, reduction tasks
+    size_t rgi = 0, rti = 0;
+    for (size_t k = 0; k < gs.size(); ++k) {
+        const G& g = gs[k];
+        const re_batch_item& it = items[g.item];
+        GeoRequest& R = reqs[k];
+        R.src = reinterpret_cast<const float*>(dbase + g.o_support);
+        if (R.kind == 1) {
+            Axis* ax = reinterpret_cast<Axis*>(base + g.o_axes);
+            R.ax = ax;
+            R.ay = ax + g.plan.xs.size();
+            std::memcpy(host.data() + g.o_axes, g.plan.xs.data(), g.plan.xs.size() * sizeof(Axis));
+            std::memcpy(host.data() + g.o_axes + g.plan.xs.size() * sizeof(Axis), g.plan.ys.data(),
+                        g.plan.ys.size() * sizeof(Axis));
+            R.H = reinterpret_cast<double*>(dbase + g.o_h);
+        }
+        R.out = g.reduce ? reinterpret_cast<float*>(dbase + g.o_native) : it.out;
+        re_batch_item sup{};
+        sup.image = it.image;
+        sup.desc = it.desc;
+        sup.viewport = {g.area.x + g.plan.support.x, g.area.y + g.plan.support.y, g.plan.support.width,
+                        g.plan.support.height};
+        sup.mip = 0;
+        sup.quality = 1;
+        sup.out = reinterpret_cast<float*>(dbase + g.o_support);
+        sup.out_row_stride = (size_t)g.plan.support.width * 3;
+        supports.push_back(sup);
+        GeoSingle q{};
+        q.request = R;
+        q.reduce = g.reduce;
+        q.post = g.post;
+        q.mip = it.mip;
+        q.viewport = it.viewport;
+        q.out = it.out;
+        q.out_stride = it.out_row_stride;
+        b->geo_singles.push_back(q);
+        if (g.reduce) {
+            while (rti == rgroups[rgi].tasks.size()) {
+                ++rgi;
+                rti = 0;
+            }
+            rgroups[rgi].tasks[rti++].native = R.out;
+        }
+    }
+    std::memcpy(host.data() + o_req, reqs.data(), reqs.size() * sizeof(GeoRequest));
+    std::memcpy(host.data() + o_p1, pass1.data(), pass1.size() * sizeof(GeoBlock));
+    std::memcpy(host.data() + o_p2, pass2.data(), pass2.size() * sizeof(GeoBlock));
+    for (size_t r = 0; r < rgroups.size(); ++r) {
+        std::memcpy(host.data() + o_rg[r].first, rgroups[r].tasks.data(), rgroups[r].tasks.size() * sizeof(ReduceTask));
+        std::memcpy(host.data() + o_rg[r].second, rgroups[r].unit_task.data(),
+                    rgroups[r].unit_task.size() * sizeof(uint32_t));
+        LaunchGroup lg{};
+        BatchParams& A = lg.params;
+        std::memset(&A, 0, sizeof(A));
+        for (size_t i = 0; i < rgroups[r].program_list.size(); ++i) A.programs[i] = rgroups[r].program_list[i];
+        A.rtasks = reinterpret_cast<const ReduceTask*>(base + o_rg[r].first);
+        A.runit_task = reinterpret_cast<const uint32_t*>(base + o_rg[r].second);
+        A.runits = (uint32_t)rgroups[r].unit_task.size();
+        A.menon_policy = 1;
+        b->geo_groups.push_back(lg);
+    }
+    BT_CUDA(cudaMemcpy(base, host.data(), tables, cudaMemcpyHostToDevice));
+    b->geo_requests = reinterpret_cast<const GeoRequest*>(base + o_req);
+    b->geo_pass1 = reinterpret_cast<const GeoBlock*>(base + o_p1);
+    b->geo_pass2 = reinterpret_cast<const GeoBlock*>(base + o_p2);
+    b->geo_n1 = (uint32_t)pass1.size();
+    b->geo_n2 = (uint32_t)pass2.size();
+    return RE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -223,6 +496,7 @@ re_status re_batch_destroy(re_batch* b) {
     release_graph(b);
     if (b->capture) cudaStreamDestroy(b->capture);
     if (b->dev) cudaFree(b->dev);
+    if (b->geo) cudaFree(b->geo);
     delete b;
     return RE_OK;
 }
@@ -231,7 +505,9 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
     if (!b || (count && !items)) return fail(RE_INVALID_ARGUMENT, "null batch arguments");
     if (count > (1u << 24)) return fail(RE_LENGTH_ERROR, "too many batch requests");
     b->planned = false;
-    std::vector<re_batch_item> copy(items, items + count);
+    std::vector<re_batch_item> given(items, items + count), copy, geometry;
+    for (const re_batch_item& it : given) (it.geometry ? geometry : copy).push_back(it);
+    const size_t n_plain = copy.size();
     // 1. validate and describe every request
     struct Req {
         size_t item;
@@ -243,6 +519,13 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         uint32_t tiles_x, tiles;
     };
     re_batch_info info{};
+    // 0. geometry requests: their supports join the RAW requests
+    {
+        std::vector<re_batch_item> supports;
+        re_status s = plan_geometry(b, geometry, supports, info);
+        if (s) return s;
+        copy.insert(copy.end(), supports.begin(), supports.end());
+    }
     auto describe = [&](const re_batch_item& it, size_t index, Req& r) -> re_status {
         if (!it.image || !it.desc) return fail(RE_INVALID_ARGUMENT, "null render arguments");
         r = Req{};
@@ -269,7 +552,7 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
     // the requests as given (validated; the per-request form renders these)
     std::vector<Req> orig;
     std::vector<re_batch_item> valid;
-    for (size_t i = 0; i < count; ++i) {
+    for (size_t i = 0; i < copy.size(); ++i) {
         Req r;
         re_status s = describe(copy[i], i, r);
         if (s) return s;
@@ -277,10 +560,13 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         orig.push_back(r);
         valid.push_back(copy[i]);
         info.native_pixels += (uint64_t)r.native.width * r.native.height;
-        info.output_pixels += (uint64_t)copy[i].viewport.width * copy[i].viewport.height;
-        info.reduced_requests += copy[i].mip ? 1 : 0;
+        if (i < n_plain) {   // a support's pixels are intermediate, not output
+            info.output_pixels += (uint64_t)copy[i].viewport.width * copy[i].viewport.height;
+            info.reduced_requests += copy[i].mip ? 1 : 0;
+            ++info.requests;
+        }
     }
-    info.requests = (uint32_t)orig.size();
+    info.requests += info.geometry_requests;
     // the renders the batch performs: adjacent requests merged
     const std::vector<re_batch_item> merged = merge_items(valid);
     std::vector<Req> reqs(merged.size());
@@ -475,10 +761,17 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
         grid_total += groups[gi].grid;
     }
     b->groups = std::move(groups);
+    for (LaunchGroup& g : b->geo_groups) {
+        g.params.status = b->head;
+        g.params.queue = b->head;
+        g.params.dispatch = opt.dispatch;
+    }
     b->units = (uint32_t)tiles;
     b->runits = 0;
     for (const GroupTables& T : tabs) b->runits += (uint32_t)T.runit_task.size();
+    for (const LaunchGroup& g : b->geo_groups) b->runits += g.params.runits;
     b->items = std::move(copy);
+    b->given = std::move(given);
     b->opt = opt;
     info.tiles = b->units;
     info.reduce_blocks = b->runits;
@@ -532,7 +825,8 @@ re_status re_batch_plan(re_batch* b, const re_batch_item* items, size_t count, c
 
 re_status re_batch_launch_per_request(re_batch* b, void* stream_) {
     if (!b || !b->planned) return fail(RE_INVALID_ARGUMENT, "batch is not planned");
-    return launch_singles(b, b->singles, (cudaStream_t)stream_);
+    re_status s = launch_singles(b, b->singles, (cudaStream_t)stream_);
+    return s ? s : launch_geo_singles(b, (cudaStream_t)stream_);
 }
 
 re_status re_batch_launch(re_batch* b, void* stream_) {
@@ -565,7 +859,7 @@ re_status re_batch_autotune(re_batch* b, uint32_t reps, void* stream_, re_batch_
     if (!b || !b->planned) return fail(RE_INVALID_ARGUMENT, "batch is not planned");
     if (!reps) reps = 5;
     cudaStream_t stream = (cudaStream_t)stream_;
-    const std::vector<re_batch_item> items = b->items;
+    const std::vector<re_batch_item> items = b->given;
     const uint32_t graph = b->opt.use_graph;
     std::vector<re_batch_options> cands;
     for (uint32_t order = 0; order <= 1; ++order) {

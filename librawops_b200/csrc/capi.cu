@@ -703,6 +703,21 @@ re_status render_plan(const re_image* img, const re_render_desc* desc, re_rect v
     return RE_OK;
 }
 re_status status_key_to_error(uint32_t key) { return status_from_key(key); }
+re_status stage_program(const re_render_desc* desc, DevProgram& P) { return build_program(desc, P); }
+
+// An image that owns an already uploaded device plane (metadata normalized by the caller).
+re_status image_adopt_device(re_raw_metadata* meta, uint16_t* device_samples, size_t count, re_image** out) {
+    re_status s = re_raw_metadata_normalize(meta, count);
+    if (s) return s;
+    auto* img = new (std::nothrow) re_image;
+    if (!img) return fail(RE_LENGTH_ERROR, "out of host memory");
+    img->meta = *meta;
+    img->dev = device_samples;
+    img->owned = true;
+    img->raw = make_dev_raw(*meta, device_samples);
+    *out = img;
+    return RE_OK;
+}
 }  // namespace re
 
 extern "C" {

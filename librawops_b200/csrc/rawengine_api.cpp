@@ -23,6 +23,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <limits>
+#include <list>
 #include <map>
 #include <mutex>
 #include <queue>
@@ -30,6 +31,7 @@
 
 #include <cuda_runtime.h>
 
+#include "rawengine/EditOps.hpp"
 #include "rawengine/ImageAnalysis.hpp"
 #include "rawengine/Operators.hpp"
 #include "rawengine_b200.h"
@@ -717,13 +719,19 @@ struct DevImage {
     size_t stride = 0;  // floats per row
     Rect bounds;
     cudaStream_t stream = nullptr;
+    std::shared_ptr<const float> shared;   // a cached tile read in place (not freed here)
     DevImage(Rect r, cudaStream_t s) : stride((size_t)r.width * 3), bounds(r), stream(s) {
         if (r.width && r.height)
             check_cuda(re::scratch_alloc((void**)&data, (size_t)r.width * r.height * 3 * sizeof(float), s),
                        "device tile");
     }
+    // A read-only view of a contiguous device tile; the executor never writes
+    // into an image it evaluated, so a cached tile can be used without a copy.
+    DevImage(Rect r, cudaStream_t s, std::shared_ptr<const float> tile)
+        : data(const_cast<float*>(tile.get())), stride((size_t)r.width * 3), bounds(r), stream(s),
+          shared(std::move(tile)) {}
     ~DevImage() {
-        if (data) cudaFreeAsync(data, stream);
+        if (data && !shared) cudaFreeAsync(data, stream);
     }
     DevImage(const DevImage&) = delete;
     DevImage& operator=(const DevImage&) = delete;
@@ -877,6 +885,7 @@ struct Executor {
         if (auto* cr = dynamic_cast<const CubicResizeNode*>(&node)) return eval_cubic(*cr, r, level);
         if (auto* ro = dynamic_cast<const RotateNode*>(&node)) return eval_rotate(*ro, r, level);
         if (auto* st = dynamic_cast<const StencilNode*>(&node)) return eval_stencil(*st, r, level);
+        if (auto* cn = dynamic_cast<const CachedNode*>(&node)) return eval_cached(*cn, r, level);
         if (dynamic_cast<const DeviceNode*>(&node)) return eval(node, r, level);
         return upload(node, r, level);
     }
@@ -928,6 +937,15 @@ struct Executor {
         check(re_cubic_resize_window(in->data, in->stride, window, ib.width, ib.height, cr.settings().width,
                                      cr.settings().height, to_re(r), level.mip, out->data, out->stride, s));
         return out;
+    }
+
+    // A cached node: the cache's device tile for exactly this rectangle and
+    // level, read in place (rendered through the input on a miss).
+    DevPtr eval_cached(const CachedNode& cn, Rect r, RenderLevel level) {
+        check_cancel();
+        if (!r.width || !r.height) return std::make_unique<DevImage>(r, s);
+        DeviceTile t = cn.cache()->render_device(*cn.input_node(), cn.signature(), r, level);
+        return std::make_unique<DevImage>(r, s, std::move(t.rgb));
     }
 
     // SpatialOps.cpp:343-383, 410-495, 509-620, 637-697: render the input over
@@ -1361,6 +1379,10 @@ namespace {
 struct RawLowering {
     const re_image* image = nullptr;
     re_render_desc desc{};
+    // a cubic resize or rotation between the RAW chain and later point stages
+    uint32_t geometry = 0, canvas_width = 0, canvas_height = 0;
+    double angle = 0;
+    re_render_desc post{};
 };
 
 bool lower_raw_chain(const Node& node, RenderLevel level, RawLowering& out) {
@@ -1391,6 +1413,51 @@ bool lower_raw_chain(const Node& node, RenderLevel level, RawLowering& out) {
         return false;
     }
     out.desc = sl.desc;
+    return true;
+}
+
+// A request whose chain is point nodes over one CubicResizeNode or RotateNode
+// over a RAW point chain (whose extent is the geometry's input bounds),
+// lowered to a geometry item: the RAW chain at native resolution, the
+// geometry, the point stages after it.
+bool lower_geometry_chain(const Node& node, RenderLevel level, RawLowering& out) {
+    if (!node.supports_level(level)) return false;
+    std::vector<const PointNode*> chain;
+    const Node* cur = &node;
+    while (auto* p = dynamic_cast<const PointNode*>(cur)) {
+        chain.push_back(p);
+        cur = p->input().get();
+    }
+    std::reverse(chain.begin(), chain.end());
+    const Node* input = nullptr;
+    Rect bounds;
+    if (auto* cr = dynamic_cast<const CubicResizeNode*>(cur)) {
+        out.geometry = 1;
+        out.canvas_width = cr->settings().width;
+        out.canvas_height = cr->settings().height;
+        input = cr->input_node();
+        bounds = cr->input_bounds();
+    } else if (auto* ro = dynamic_cast<const RotateNode*>(cur)) {
+        out.geometry = 2;
+        out.angle = ro->angle();
+        input = ro->input_node();
+        bounds = ro->input_bounds();
+    } else {
+        return false;
+    }
+    if (!input || !cur->supports_level(level) || !lower_raw_chain(*input, {}, out)) return false;
+    const Node* src = input;
+    while (auto* p = dynamic_cast<const PointNode*>(src)) src = p->input().get();
+    auto* raw = dynamic_cast<const RawUnpackNode*>(src);
+    if (!raw || !same(raw->image().metadata().active_area, bounds)) return false;
+    StageList post;
+    post.desc.anchor = -1;
+    try {
+        for (const PointNode* p : chain) add_stage(post, p, false, {});
+    } catch (...) {
+        return false;
+    }
+    out.post = post.desc;
     return true;
 }
 
@@ -1429,6 +1496,131 @@ Tile DeviceTile::to_host() const {
         check_cuda(cudaMemcpy(t.rgb.data(), rgb.get(), t.rgb.size() * sizeof(float), cudaMemcpyDeviceToHost),
                    "device tile download");
     return t;
+}
+
+// --------------------------------------------------------------- TileCache
+
+struct TileCache::Impl {
+    struct Key {
+        std::array<std::uint8_t, 32> signature{};
+        std::array<std::uint32_t, 4> bounds{};
+        std::uint32_t mip = 0;
+        RenderQuality quality = RenderQuality::Final;
+        auto operator<=>(const Key&) const = default;
+    };
+    struct Entry {
+        DeviceTile tile;
+        std::list<Key>::iterator recency;
+        std::size_t charged = 0;
+    };
+    std::size_t max_bytes = 0, used = 0, hits = 0, misses = 0;
+    std::uint64_t generation = 0;
+    std::map<Key, Entry> entries;
+    std::list<Key> recency;
+    mutable std::mutex mu;
+};
+
+TileCache::TileCache(std::size_t max_bytes) : impl_(std::make_unique<Impl>()) { impl_->max_bytes = max_bytes; }
+TileCache::~TileCache() = default;
+
+namespace {
+// One tile of `node` in device memory: device nodes through the executor,
+// other nodes through their own render_level, validated as the reference
+// validates cache tiles (EditGraph.cpp:46-52), then uploaded.
+DeviceTile render_to_device(const Node& node, Rect bounds, RenderLevel level) {
+    cudaStream_t s = thread_stream();
+    const size_t row = (size_t)bounds.width * 3;
+    DeviceTile d{bounds, nullptr, node.output_descriptor()};
+    auto block = device_block(row * bounds.height * sizeof(float), s);
+    if (dynamic_cast<const DeviceNode*>(&node)) {
+        Executor ex{s, nullptr};
+        DevPtr img = ex.eval(node, bounds, level);
+        if (bounds.width && bounds.height)
+            check_cuda(cudaMemcpy2DAsync(block.get(), row * sizeof(float), img->data, img->stride * sizeof(float),
+                                         row * sizeof(float), bounds.height, cudaMemcpyDeviceToDevice, s),
+                       "cache tile");
+    } else {
+        const Tile t = node.render_level(bounds, level);
+        const uint64_t pixels = (uint64_t)bounds.width * bounds.height;
+        if (!same(t.bounds, bounds) || t.descriptor != node.output_descriptor() || t.rgb.size() != pixels * 3)
+            throw std::domain_error("node returned an invalid cache tile");
+        if (!t.rgb.empty())
+            check_cuda(cudaMemcpyAsync(block.get(), t.rgb.data(), t.rgb.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, s),
+                       "cache tile");
+    }
+    check_cuda(cudaStreamSynchronize(s), "cache tile");
+    d.rgb = block;
+    return d;
+}
+}  // namespace
+
+// EditGraph.cpp:23-80
+DeviceTile TileCache::render_device(const Node& node, std::array<std::uint8_t, 32> signature, Rect bounds,
+                                    RenderLevel level) {
+    if (level.mip > 31 || (level.quality != RenderQuality::Preview && level.quality != RenderQuality::Final))
+        throw std::invalid_argument("invalid cache render level");
+    if (!node.supports_level(level)) throw std::invalid_argument("node does not support this cache render level");
+    Impl& m = *impl_;
+    const Impl::Key key{signature, {bounds.x, bounds.y, bounds.width, bounds.height}, level.mip, level.quality};
+    std::uint64_t generation;
+    {
+        std::lock_guard<std::mutex> lock(m.mu);
+        if (auto found = m.entries.find(key); found != m.entries.end()) {
+            ++m.hits;
+            m.recency.splice(m.recency.begin(), m.recency, found->second.recency);
+            return found->second.tile;
+        }
+        ++m.misses;
+        generation = m.generation;
+    }
+    DeviceTile tile = render_to_device(node, bounds, level);
+    constexpr std::size_t entry_charge = 256;
+    const std::size_t floats = (std::size_t)bounds.width * bounds.height * 3;
+    if (!floats || floats > (m.max_bytes - std::min(m.max_bytes, entry_charge)) / sizeof(float)) return tile;
+    const std::size_t charge = entry_charge + floats * sizeof(float);
+    std::lock_guard<std::mutex> lock(m.mu);
+    if (generation != m.generation) return tile;
+    if (auto found = m.entries.find(key); found != m.entries.end()) {
+        ++m.hits;
+        m.recency.splice(m.recency.begin(), m.recency, found->second.recency);
+        return found->second.tile;
+    }
+    while (m.used > m.max_bytes - charge) {
+        const auto oldest = std::prev(m.recency.end());
+        m.used -= m.entries.at(*oldest).charged;
+        m.entries.erase(*oldest);
+        m.recency.erase(oldest);
+    }
+    m.recency.push_front(key);
+    m.entries.emplace(key, Impl::Entry{tile, m.recency.begin(), charge});
+    m.used += charge;
+    return tile;
+}
+
+Tile TileCache::render(const Node& node, std::array<std::uint8_t, 32> signature, Rect bounds, RenderLevel level) {
+    return render_device(node, signature, bounds, level).to_host();
+}
+
+TileCache::Stats TileCache::stats() const {
+    std::lock_guard<std::mutex> lock(impl_->mu);
+    return {impl_->entries.size(), impl_->used, impl_->hits, impl_->misses};
+}
+
+void TileCache::clear() {
+    std::lock_guard<std::mutex> lock(impl_->mu);
+    ++impl_->generation;
+    impl_->entries.clear();
+    impl_->recency.clear();
+    impl_->used = 0;
+    impl_->hits = 0;
+    impl_->misses = 0;
+}
+
+CachedNode::CachedNode(std::shared_ptr<const Node> input, std::shared_ptr<TileCache> cache,
+                       std::array<std::uint8_t, 32> signature)
+    : input_(std::move(input)), cache_(std::move(cache)), signature_(signature) {
+    if (!input_ || !cache_) throw std::invalid_argument("cached node requires an input and a cache");
 }
 
 // Pending requests sit in one ordered map keyed by (descending priority,
@@ -1645,7 +1837,8 @@ private:
             const Rect vp = r->request.viewport;
             const bool batchable = lane.batch && lane.stream && vp.width && vp.height &&
                                    dynamic_cast<const DeviceNode*>(r->node.get()) &&
-                                   lower_raw_chain(*r->node, r->request.level, L);
+                                   (lower_raw_chain(*r->node, r->request.level, L) ||
+                                    lower_geometry_chain(*r->node, r->request.level, (L = RawLowering{})));
             if (batchable) {
                 lowered.push_back(L);
                 batched.push_back(r.get());
@@ -1671,11 +1864,27 @@ private:
                 block = device_block(floats * sizeof(float), lane.stream);
                 for (size_t i = 0; i < batched.size(); ++i) {
                     const Request& r = *batched[i];
-                    const re_render_desc*& shared = programs[desc_key(lowered[i].desc)];
-                    if (!shared) shared = &lowered[i].desc;
-                    items[i] = re_batch_item{lowered[i].image, shared, to_re(r.request.viewport),
-                                             r.request.level.mip, (uint32_t)r.request.level.quality,
-                                             block.get() + offset[i], (size_t)r.request.viewport.width * 3};
+                    const RawLowering& L = lowered[i];
+                    const re_render_desc*& shared = programs[desc_key(L.desc)];
+                    if (!shared) shared = &L.desc;
+                    re_batch_item& it = items[i];
+                    it = re_batch_item{};
+                    it.image = L.image;
+                    it.desc = shared;
+                    it.viewport = to_re(r.request.viewport);
+                    it.mip = r.request.level.mip;
+                    it.quality = (uint32_t)r.request.level.quality;
+                    it.out = block.get() + offset[i];
+                    it.out_row_stride = (size_t)r.request.viewport.width * 3;
+                    if (L.geometry) {
+                        it.geometry = L.geometry;
+                        it.canvas_width = L.canvas_width;
+                        it.canvas_height = L.canvas_height;
+                        it.angle_degrees = L.angle;
+                        const re_render_desc*& post = programs["post" + desc_key(L.post)];
+                        if (!post) post = &L.post;
+                        it.post = post;
+                    }
                 }
                 re_batch_options opt{};
                 opt.dispatch = 2;

@@ -355,13 +355,27 @@ def synthetic_samples(img, device="cuda"):
                                   stride=img.stride, black=img.black, white=img.white, device=device)
 
 
+@dataclass
+class Geometry:
+    """A cubic resize (kind "cubic", canvas (w, h)) or rotation (kind
+    "rotate", angle in degrees) between a RAW chain and later point stages
+    (`post`, a Pipeline of point stages or None), for batch requests."""
+    kind: str
+    canvas: tuple = (0, 0)
+    angle: float = 0.0
+    post: Optional["Pipeline"] = None
+
+
 class Batch:
     """Many render requests drained by one persistent kernel (re_batch_*).
 
-    requests: (image, pipeline, viewport, mip, quality, out) with `out` a CUDA
-    float32 tensor of shape (h, w, 3) (row stride from the tensor).  The batch
-    keeps references to the images, pipelines' descriptions and outputs it was
-    planned with."""
+    requests: (image, pipeline, viewport, mip, quality, out[, geometry]) with
+    `out` a CUDA float32 tensor of shape (h, w, 3) (row stride from the
+    tensor).  With a Geometry, `pipeline` renders the RAW source at native
+    resolution (the geometry's input), the geometry maps it to its canvas at
+    level `mip`, then geometry.post runs; viewport is in canvas level
+    coordinates.  The batch keeps references to the images, pipelines'
+    descriptions and outputs it was planned with."""
 
     def __init__(self):
         h = C.c_void_p()
@@ -373,12 +387,23 @@ class Batch:
         items = (_capi.BatchItem * max(len(requests), 1))()
         descs = []
         cache = {}
-        for i, (image, pipe, viewport, mip, quality, out) in enumerate(requests):
+        def desc_of(pipe):
             if id(pipe) not in cache:
                 cache[id(pipe)] = pipe.desc()
                 descs.append(cache[id(pipe)])
+            return C.pointer(cache[id(pipe)])
+
+        for i, req in enumerate(requests):
+            image, pipe, viewport, mip, quality, out = req[:6]
+            geo = req[6] if len(req) > 6 else None
             items[i].image = image.handle
-            items[i].desc = C.pointer(cache[id(pipe)])
+            items[i].desc = desc_of(pipe)
+            if geo is not None:
+                items[i].geometry = {"cubic": 1, "rotate": 2}[geo.kind]
+                items[i].canvas_width, items[i].canvas_height = (int(v) for v in geo.canvas)
+                items[i].angle_degrees = float(geo.angle)
+                if geo.post is not None:
+                    items[i].post = desc_of(geo.post)
             items[i].viewport = _rect(viewport)
             items[i].mip = mip
             items[i].quality = quality
@@ -408,6 +433,7 @@ class Batch:
         return {"requests": i.requests, "reduced_requests": i.reduced_requests, "tasks": i.tasks, "tiles": i.tiles,
                 "reduce_blocks": i.reduce_blocks, "grid": i.grid, "native_pixels": i.native_pixels,
                 "output_pixels": i.output_pixels, "raw_bytes": i.raw_bytes, "output_bytes": i.output_bytes,
+                "geometry_requests": i.geometry_requests,
                 "options": {"dispatch": o.dispatch, "ctas_per_sm": o.ctas_per_sm, "order": o.order,
                             "use_graph": o.use_graph}}
 
@@ -510,6 +536,19 @@ def stencil(kind: str, rgb, window, image, output, amount: float = 0.0, radius: 
                                       *tail))
     else:
         raise ValueError(f"unknown stencil {kind}")
+    return out
+
+
+def render_raster(rgb, pipe: "Pipeline", viewport=None, mip: int = 0, quality: int = FINAL, stream=None):
+    """RasterSourceNode over a CUDA float tensor (h, w, 3) followed by the
+    point stages of `pipe` (re_render_raster)."""
+    h, w = int(rgb.shape[0]), int(rgb.shape[1])
+    viewport = viewport or (0, 0, *request_bounds((0, 0, w, h), mip, quality)[2:])
+    o = _rect(viewport)
+    out = rgb.new_empty((o.height, o.width, 3))
+    d = pipe.desc()
+    check(lib().re_render_raster(_dev(rgb), rgb.stride(0), w, h, C.byref(d), o, mip, quality, _dev(out),
+                                 out.stride(0), C.c_void_p(_stream_ptr(stream))))
     return out
 
 

@@ -137,13 +137,19 @@ class MixedTile:
     viewport: tuple
     mip: int
     quality: int
+    geometry: int = 0           # 0 none, 1 cubic resize to `canvas`, 2 rotation by `angle`
+    canvas: tuple = (0, 0)      # geometry canvas at mip 0 (the active area's extent for a rotation)
+    angle: float = 0.0
 
 
 MIXED_SIZES = [(1920, 1080)] * 4 + [(4000, 3000)] * 6 + [(6000, 4000)] * 4 + [(8256, 5504)] * 2
 
 
-def mixed_batch(seed: int = 4, target_tiles: int = 3000):
-    """Images, recipes (one per image) and the tile list of the mixed batch."""
+def mixed_batch(seed: int = 4, target_tiles: int = 3000, geometry_share: float = 0.2):
+    """Images, recipes (one per image) and the tile list of the mixed batch.
+    A share of the viewports (geometry_share) is rendered through a cubic
+    resize to a 2048 long edge or a rotation by a uniform angle in [-45, 45]
+    degrees placed after the camera-to-working stage."""
     rng = np.random.default_rng(seed)
     images, recipes = [], []
     for i, (w, h) in enumerate(MIXED_SIZES):
@@ -173,9 +179,19 @@ def mixed_batch(seed: int = 4, target_tiles: int = 3000):
         level = rng.choice(3, p=[0.5, 0.3, 0.2])
         mip, quality = (0, 1) if level == 0 else (int(level), 0)
         ax, ay, aw, ah = img.active
+        geometry, canvas, angle = 0, (aw, ah), 0.0
+        if geometry_share and rng.uniform() < geometry_share:
+            # cubic resize to a 2048 long edge where the reference accepts it
+            # (at most a fourfold shrink per axis), else a rotation
+            geometry = 1 if max(aw, ah) <= 4 * 2048 and rng.uniform() < 0.5 else 2
+            if geometry == 1:
+                canvas = long_edge_canvas(aw, ah, 2048)
+            else:
+                angle = float(rng.uniform(-45.0, 45.0))
+        cw, ch = canvas
         s = 1 << mip
-        lw, lh = (aw, ah) if mip == 0 else (-(-aw // s), -(-ah // s))
-        ox0, oy0 = (ax, ay) if mip == 0 else (0, 0)
+        lw, lh = (cw, ch) if mip == 0 else (-(-cw // s), -(-ch // s))
+        ox0, oy0 = (ax, ay) if mip == 0 and not geometry else (0, 0)
         vw = max(1, int(lw * rng.uniform(0.05, 0.35)))
         vh = max(1, int(lh * rng.uniform(0.05, 0.35)))
         vx = ox0 + int(rng.integers(0, lw - vw + 1))
@@ -183,8 +199,16 @@ def mixed_batch(seed: int = 4, target_tiles: int = 3000):
         t = int(rng.choice([128, 256, 512, 1024]))
         for y in range(vy, vy + vh, t):
             for x in range(vx, vx + vw, t):
-                tiles.append(MixedTile(i, i, (x, y, min(t, vx + vw - x), min(t, vy + vh - y)), mip, quality))
+                tiles.append(MixedTile(i, i, (x, y, min(t, vx + vw - x), min(t, vy + vh - y)), mip, quality,
+                                       geometry, canvas if geometry else (0, 0), angle))
     return images, recipes, tiles
+
+
+def long_edge_canvas(width: int, height: int, edge: int):
+    """The canvas of a resize whose long edge is `edge`, aspect kept (rounded)."""
+    if width >= height:
+        return edge, max(1, int(round(height * edge / width)))
+    return max(1, int(round(width * edge / height))), edge
 
 
 def mixed_pipeline(image: MixedImage, recipe: MixedRecipe):
@@ -207,9 +231,52 @@ def mixed_pipeline(image: MixedImage, recipe: MixedRecipe):
     return p
 
 
+def mixed_geometry_pipelines(image: MixedImage, recipe: MixedRecipe):
+    """A mixed-batch recipe split around a geometry stage: (pre, post), the
+    RAW source's stages through CameraToWorking (scene-linear ProPhoto, the
+    geometry's input) and the point stages after the geometry."""
+    from .render import CurveSet, Pipeline
+    pre = Pipeline(demosaic=image.demosaic)
+    pre.white_balance(*recipe.wb)
+    post = Pipeline()
+    if recipe.curve is None:
+        pre.exposure(recipe.stops)
+        pre.camera_to_working(recipe.camera_to_xyz, 0)
+        post.working_to_srgb()
+        post.tone_curve(*recipe.tone)
+        post.srgb_encode()
+    else:
+        pre.camera_to_working(recipe.camera_to_xyz, 0)
+        post.exposure(recipe.stops)
+        post.extended_curves(CurveSet(recipe.curve, cubic=True))
+        post.working_to_srgb()
+        post.srgb_encode()
+    return pre, post
+
+
+def mixed_requests(render, imgs, images, recipes, tiles, outs):
+    """Batch request tuples of the mixed batch (render.Batch.plan), geometry
+    tiles included; one pipeline (or pipeline pair) per recipe."""
+    plain, split = {}, {}
+    reqs = []
+    for t, o in zip(tiles, outs):
+        if not t.geometry:
+            if t.recipe not in plain:
+                plain[t.recipe] = mixed_pipeline(images[t.image], recipes[t.recipe])
+            reqs.append((imgs[t.image], plain[t.recipe], t.viewport, t.mip, t.quality, o))
+            continue
+        if t.recipe not in split:
+            split[t.recipe] = mixed_geometry_pipelines(images[t.image], recipes[t.recipe])
+        pre, post = split[t.recipe]
+        geo = render.Geometry("cubic" if t.geometry == 1 else "rotate", t.canvas, t.angle, post)
+        reqs.append((imgs[t.image], pre, t.viewport, t.mip, t.quality, o, geo))
+    return reqs
+
+
 def write_scheduler_spec(path: str, images, recipes, tiles) -> None:
     """The mixed batch as the text spec read by the C++ scheduler driver
-    (tests/cpp/scheduler_driver.cpp): image, recipe and tile lines.  A recipe
+    (tests/cpp/scheduler_driver.cpp): image, recipe and tile lines (a tile's
+    geometry, canvas and angle last).  A recipe
     without a tone curve (the extended-curve recipes) gets the default tone
     shoulder 0.25 and gamma 1 in the C++ chain."""
     with open(path, "w") as f:
@@ -224,4 +291,5 @@ def write_scheduler_spec(path: str, images, recipes, tiles) -> None:
                 r.wb[0], r.wb[1], r.wb[2], r.stops, " ".join(repr(float(v)) for v in np.asarray(r.camera_to_xyz).reshape(9)),
                 shoulder, gamma, len(knots), " ".join("%r %r" % (x, y) for x, y in knots)))
         for t in tiles:
-            f.write("tile %d %d %d %d %d %d %d %d\n" % (t.image, t.recipe, *t.viewport, t.mip, t.quality))
+            f.write("tile %d %d %d %d %d %d %d %d %d %d %d %r\n" % (t.image, t.recipe, *t.viewport, t.mip, t.quality,
+                                                                   t.geometry, *t.canvas, float(t.angle)))

@@ -644,6 +644,108 @@ void factory_validation(const std::shared_ptr<const Node>& working, Rect area) {
           "factory_descriptor_domain");
 }
 
+// ----------------------------------------------------------- tile cache
+
+// A caller Node that counts its renders (a constant per-position image).
+class CountingNode final : public Node {
+public:
+    mutable unsigned calls = 0;
+    bool broken = false;
+    ImageDescriptor output_descriptor() const noexcept override {
+        return ImageDescriptor::scene_linear(WorkingSpace::LinearProPhotoD50);
+    }
+    Tile render(Rect r) const override {
+        ++calls;
+        Tile t{r, std::vector<float>((size_t)r.width * r.height * 3), output_descriptor()};
+        for (size_t i = 0; i < t.rgb.size(); ++i) t.rgb[i] = 0.001f * (float)((r.x + r.y + i) % 997);
+        if (broken) t.rgb.pop_back();
+        return t;
+    }
+};
+
+// TileCache (EditGraph.cpp:23-80 rules) and CachedNode over a device chain.
+void cache_checks(const RawImage& raw, Rect area, const std::map<std::string, std::vector<double>>& P) {
+    std::array<std::uint8_t, 32> sig{};
+    sig[0] = 7;
+    {
+        CountingNode node;
+        TileCache cache(64 * 1024);
+        const Rect r{3, 4, 20, 10};   // 2400 bytes + 256
+        const Tile a = cache.render(node, sig, r);
+        const Tile b = cache.render(node, sig, r);
+        auto st = cache.stats();
+        check(node.calls == 1 && bit_equal(a.rgb, b.rgb) && st.hits == 1 && st.misses == 1 && st.entries == 1 &&
+                  st.used_bytes == 256 + 2400,
+              "cache_hit_after_miss");
+        const DeviceTile d = cache.render_device(node, sig, r);
+        check(node.calls == 1 && bit_equal(d.to_host().rgb, a.rgb), "cache_device_hit");
+        auto other = sig;
+        other[1] = 1;
+        (void)cache.render(node, other, r);
+        (void)cache.render(node, sig, Rect{3, 4, 20, 11});
+        check(node.calls == 3 && cache.stats().entries == 3, "cache_keys_signature_and_bounds");
+        expect_throw<std::invalid_argument>([&] { (void)cache.render(node, sig, r, {32, RenderQuality::Preview}); },
+                                            "cache_rejects_level");
+        expect_throw<std::invalid_argument>([&] { (void)cache.render(node, sig, r, {1, RenderQuality::Preview}); },
+                                            "cache_rejects_unsupported_level");
+        node.broken = true;
+        expect_throw<std::domain_error>([&] { (void)cache.render(node, sig, Rect{0, 0, 3, 3}); },
+                                        "cache_rejects_invalid_tile");
+        node.broken = false;
+        cache.clear();
+        st = cache.stats();
+        check(st.entries == 0 && st.used_bytes == 0 && st.hits == 0 && st.misses == 0, "cache_clear");
+    }
+    {   // LRU eviction within the budget; oversized tiles are not cached
+        CountingNode node;
+        TileCache cache(2 * (256 + 1200) + 100);   // room for two 10x10 tiles
+        const Rect a{0, 0, 10, 10}, b{10, 0, 10, 10}, c{20, 0, 10, 10};
+        (void)cache.render(node, sig, a);
+        (void)cache.render(node, sig, b);
+        (void)cache.render(node, sig, a);   // a most recent
+        (void)cache.render(node, sig, c);   // evicts b
+        const unsigned before = node.calls;
+        (void)cache.render(node, sig, a);
+        (void)cache.render(node, sig, c);
+        const bool kept = node.calls == before;
+        (void)cache.render(node, sig, b);
+        check(kept && node.calls == before + 1 && cache.stats().entries == 2, "cache_lru_eviction");
+        (void)cache.render(node, sig, Rect{0, 0, 40, 40});
+        (void)cache.render(node, sig, Rect{0, 0, 40, 40});
+        check(node.calls == before + 3 && cache.stats().used_bytes <= 2 * (256 + 1200) + 100, "cache_oversized_uncached");
+    }
+    {   // CachedNode: a RAW source kept warm across recipe edits
+        auto cache = std::make_shared<TileCache>(std::size_t(256) << 20);
+        for (int menon = 0; menon <= 1; ++menon) {
+            auto src = std::make_shared<RawUnpackNode>(
+                raw, menon ? RawDemosaicIdentity{"rawengine.menon_base", 1} : RawDemosaicIdentity{});
+            std::array<std::uint8_t, 32> s2 = sig;
+            s2[2] = (std::uint8_t)menon;
+            auto cached = std::make_shared<CachedNode>(src, cache, s2);
+            const auto cam = camera(P, WorkingSpace::LinearProPhotoD50);
+            bool same = true;
+            for (float gain : {1.7f, 2.1f}) {
+                auto chain_of = [&](std::shared_ptr<const Node> in) {
+                    std::shared_ptr<const Node> n = std::make_shared<WhiteBalanceNode>(in, gain, 1.0f, 1.4f);
+                    n = std::make_shared<CameraToWorkingNode>(n, cam, area);
+                    n = std::make_shared<WorkingToSrgbNode>(n);
+                    return std::make_shared<SrgbEncodeNode>(std::make_shared<ToneCurveNode>(n, 0.3f, 2.0f));
+                };
+                auto plain = chain_of(src), warm = chain_of(cached);
+                Renderer renderer;
+                const Rect vp{area.x + 3, area.y + 5, 70, 50};
+                same &= bit_equal(renderer.render_image(*plain, area, RenderRequest{vp, 4096}).rgb,
+                                  renderer.render_image(*warm, area, RenderRequest{vp, 4096}).rgb);
+                const RenderRequest m1{{0, 0, 40, 30}, 4096, {1, RenderQuality::Preview}};
+                same &= bit_equal(renderer.render_image(*plain, area, m1).rgb, renderer.render_image(*warm, area, m1).rgb);
+            }
+            check(same, std::string("cached_node_equals_direct_") + (menon ? "menon" : "bilinear"));
+        }
+        const auto st = cache->stats();
+        check(st.hits == 4 && st.misses == 4, "cached_node_reused_across_edits");
+    }
+}
+
 int run_render(const std::string& dir) {
     const auto P = read_params(dir + "/params.txt");
     const RawImage raw = make_raw(P, dir);
@@ -933,6 +1035,7 @@ int run_render(const std::string& dir) {
     }
     stencil_checks(dir, P, ctw, area);
     factory_checks(P, raw, area);
+    cache_checks(raw, area, P);
     histogram_checks(graph.output_node(), area);
     return failures ? 1 : 0;
 }

@@ -18,7 +18,10 @@
 // Spec lines:
 //   image w h stride pattern phase_x phase_y ax ay aw ah b0 b1 b2 b3 white demosaic seed
 //   recipe wb_r wb_g wb_b stops m0..m8 shoulder gamma nknots x0 y0 ... (nknots 0: tone chain)
-//   tile image recipe x y w h mip quality
+//   tile image recipe x y w h mip quality geometry canvas_w canvas_h angle
+// (geometry 1: a cubic resize to the canvas, 2: a rotation by angle degrees,
+// between the camera-to-working stage and the rest of the recipe)
+#include <rawengine/GeometryOps.hpp>
 #include <rawengine/RawEngine.hpp>
 #include <rawengine/TileScheduler.hpp>
 #include <rawengine/ToneOps.hpp>
@@ -34,6 +37,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <vector>
 
 using namespace rawengine;
@@ -56,6 +60,9 @@ struct TileSpec {
     int image, recipe;
     Rect viewport;
     RenderLevel level;
+    int geometry = 0;
+    uint32_t canvas_w = 0, canvas_h = 0;
+    double angle = 0;
 };
 
 // Deterministic sensor samples: a smooth gradient, a few soft blobs and
@@ -81,15 +88,22 @@ std::vector<uint16_t> synthesize(const RawMetadata& m, uint64_t seed) {
     return s;
 }
 
-std::shared_ptr<const Node> chain(const std::shared_ptr<const Node>& src, const RecipeSpec& r, Rect bounds) {
+std::shared_ptr<const Node> chain(const std::shared_ptr<const Node>& src, const RecipeSpec& r, Rect bounds,
+                                  const TileSpec& geo) {
     std::shared_ptr<const Node> n = std::make_shared<WhiteBalanceNode>(src, r.wb[0], r.wb[1], r.wb[2]);
     CameraColorTransform t;
     t.camera_to_xyz_d50 = r.cam;
+    auto geometry = [&](std::shared_ptr<const Node> in) -> std::shared_ptr<const Node> {
+        if (geo.geometry == 1)
+            return std::make_shared<CubicResizeNode>(in, bounds, CubicResizeSettings{geo.canvas_w, geo.canvas_h});
+        if (geo.geometry == 2) return std::make_shared<RotateNode>(in, bounds, RotateSettings{geo.angle});
+        return in;
+    };
     if (r.knots.empty()) {
         n = std::make_shared<ExposureNode>(n, r.stops);
-        n = std::make_shared<CameraToWorkingNode>(n, t, bounds);
+        n = geometry(std::make_shared<CameraToWorkingNode>(n, t, bounds));
     } else {
-        n = std::make_shared<CameraToWorkingNode>(n, t, bounds);
+        n = geometry(std::make_shared<CameraToWorkingNode>(n, t, bounds));
         n = std::make_shared<ExposureNode>(n, r.stops);
         ExtendedCurvesSettings cs;
         cs.master.knots = r.knots;
@@ -150,7 +164,7 @@ int main(int argc, char** argv) {
                 TileSpec t;
                 uint32_t mip, quality;
                 ss >> t.image >> t.recipe >> t.viewport.x >> t.viewport.y >> t.viewport.width >> t.viewport.height >>
-                    mip >> quality;
+                    mip >> quality >> t.geometry >> t.canvas_w >> t.canvas_h >> t.angle;
                 t.level = RenderLevel{mip, (RenderQuality)quality};
                 tiles.push_back(t);
             }
@@ -165,13 +179,22 @@ int main(int argc, char** argv) {
         if (s.demosaic) id = {"rawengine.menon_base", 1};
         sources.push_back(std::make_shared<RawUnpackNode>(raws.back(), id));
     }
-    std::map<std::pair<int, int>, std::shared_ptr<const Node>> chains;
+    using ChainKey = std::tuple<int, int, int, uint32_t, uint32_t, double>;
+    auto key_of = [](const TileSpec& t) {
+        return ChainKey{t.image, t.recipe, t.geometry, t.canvas_w, t.canvas_h, t.angle};
+    };
+    std::map<ChainKey, std::shared_ptr<const Node>> chains;
     for (const TileSpec& t : tiles) {
-        auto& c = chains[{t.image, t.recipe}];
-        if (!c) c = chain(sources[t.image], recipes[t.recipe], raws[t.image].metadata().active_area);
+        auto& c = chains[key_of(t)];
+        if (!c) c = chain(sources[t.image], recipes[t.recipe], raws[t.image].metadata().active_area, t);
     }
-    auto node_of = [&](const TileSpec& t) { return chains.at({t.image, t.recipe}); };
-    auto bounds_of = [&](const TileSpec& t) { return raws[t.image].metadata().active_area; };
+    auto node_of = [&](const TileSpec& t) { return chains.at(key_of(t)); };
+    auto bounds_of = [&](const TileSpec& t) {
+        const Rect a = raws[t.image].metadata().active_area;
+        if (t.geometry == 1) return Rect{0, 0, t.canvas_w, t.canvas_h};
+        if (t.geometry == 2) return Rect{0, 0, a.width, a.height};
+        return a;
+    };
     uint64_t out_px = 0;
     for (const TileSpec& t : tiles) out_px += (uint64_t)t.viewport.width * t.viewport.height;
 

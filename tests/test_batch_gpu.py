@@ -268,3 +268,127 @@ def test_batch_keeps_row_tiles_apart_when_the_stride_is_too_small():
     for vp, o in zip(vps, outs):
         assert bits_equal(o.cpu().numpy(), render.render(img, pipe, vp))
     batch.close()
+
+
+# ------------------------------------------------------------- geometry requests
+
+def _geometry_tiles(images):
+    """Cubic resizes (enlarge and shrink, up to fourfold) and rotations
+    (including the exact quarter turns and +-45 degrees) of every image, at mip
+    0 Final and mip 1/2 Preview, viewports tiled with edge remainders."""
+    tiles = []
+    angles = [-45.0, -13.7, 0.0, 27.5, 45.0, 90.0]
+    for i, img in enumerate(images):
+        ax, ay, aw, ah = img.active
+        canvases = [workloads.long_edge_canvas(aw, ah, 2 * max(aw, ah) // 3), (aw // 4 + 1, ah // 3 + 1),
+                    (aw + 37, ah + 11)]
+        for k, (mip, quality) in enumerate(((0, 1), (1, 0), (2, 0))):
+            for geometry, canvas, angle in ((1, canvases[(i + k) % 3], 0.0), (2, (aw, ah), angles[(i + k) % 6])):
+                cw, ch = canvas
+                s = 1 << mip
+                lw, lh = (cw, ch) if mip == 0 else (-(-cw // s), -(-ch // s))
+                vw, vh = max(1, int(lw * 0.8)), max(1, int(lh * 0.7))
+                vx, vy = (lw - vw) // 4, (lh - vh) // 2
+                t = [41, 64][(i + k) % 2]
+                for y in range(vy, vy + vh, t):
+                    for x in range(vx, vx + vw, t):
+                        tiles.append(workloads.MixedTile(i, i, (x, y, min(t, vx + vw - x), min(t, vy + vh - y)),
+                                                         mip, quality, geometry, canvas, angle))
+    return tiles
+
+
+def _geometry_single(img, image, recipe, tile):
+    """One geometry request composed of single-request calls over the whole
+    image: the RAW chain over the active area, the geometry over all of it at
+    the request's level, then the later stages on the result."""
+    pre, post = workloads.mixed_geometry_pipelines(image, recipe)
+    ax, ay, aw, ah = image.active
+    working = render.render(img, pre, image.active, out=torch.empty((ah, aw, 3), device="cuda"))
+    if tile.geometry == 1:
+        out = render.cubic_resize(working, *tile.canvas, output=tile.viewport, mip=tile.mip)
+    else:
+        out = render.rotate(working, tile.angle, output=tile.viewport, mip=tile.mip)
+    return render.render_raster(out, post)
+
+
+def test_batch_geometry_requests_equal_composed_single_renders():
+    images, recipes, _ = _small_batch()
+    imgs = _device_images(images)
+    tiles = _geometry_tiles(images)
+    plain = _small_batch()[2][::5]
+    want = [_geometry_single(imgs[t.image], images[t.image], recipes[t.recipe], t).cpu().numpy() for t in tiles]
+    want += [render.render(imgs[t.image], workloads.mixed_pipeline(images[t.image], recipes[t.recipe]), t.viewport,
+                           t.mip, t.quality) for t in plain]
+    tiles = tiles + plain
+    outs = [torch.full((t.viewport[3], t.viewport[2], 3), float("nan"), device="cuda") for t in tiles]
+    reqs = workloads.mixed_requests(render, imgs, images, recipes, tiles, outs)
+    batch = render.Batch()
+    for d, g in ((2, 1), (0, 0), (1, 1), (3, 1)):
+        for o in outs:
+            o.fill_(float("nan"))
+        batch.plan(reqs, dispatch=d, use_graph=bool(g))
+        batch.launch()
+        batch.status()
+        for k, (o, w) in enumerate(zip(outs, want)):
+            assert bits_equal(o.cpu().numpy(), w), (d, k, tiles[k])
+    info = batch.info()
+    n_geo = sum(1 for t in tiles if t.geometry)
+    assert info["geometry_requests"] == n_geo and info["requests"] == len(tiles)
+    assert info["output_pixels"] == sum(t.viewport[2] * t.viewport[3] for t in tiles)
+    for o in outs:
+        o.fill_(float("nan"))
+    batch.launch_per_request()
+    batch.status()
+    for k, (o, w) in enumerate(zip(outs, want)):
+        assert bits_equal(o.cpu().numpy(), w), ("per request", k, tiles[k])
+    batch.close()
+
+
+def test_batch_geometry_matches_reference(reference):
+    """Cubic resize and rotation requests of the batch against the reference
+    library's CubicResizeNode / RotateNode over its own RAW chain: bit for bit
+    for the working image, within the render tolerance after sRGB encoding."""
+    from conftest import within_tolerance
+    from oracle.oracle import (OP_CAMERA_TO_WORKING, OP_CUBIC_RESIZE, OP_EXPOSURE, OP_ROTATE, OP_SRGB_ENCODE,
+                               OP_TONE, OP_WB, OP_WORKING_TO_SRGB, Op, RawSpec)
+    images, recipes, _ = _small_batch()
+    imgs = _device_images(images)
+    cases = []
+    for i in (1, 2, 4, 5):            # tone-curve recipes, bilinear and Menon, inset active areas
+        im, r = images[i], recipes[i]
+        ax, ay, aw, ah = im.active
+        for geometry, canvas, angle in ((1, (aw * 3 // 2, ah * 2 // 3), 0.0), (2, (aw, ah), 33.0 - 11 * i)):
+            for mip, quality in ((0, 1), (1, 0)):
+                s = 1 << mip
+                lw, lh = (canvas[0], canvas[1]) if mip == 0 else (-(-canvas[0] // s), -(-canvas[1] // s))
+                vp = (lw // 5, lh // 4, lw // 2, lh // 2)
+                for srgb in (False, True):
+                    cases.append((i, workloads.MixedTile(i, i, vp, mip, quality, geometry, canvas, angle), srgb))
+    reqs, wants = [], []
+    for i, t, srgb in cases:
+        im, r = images[i], recipes[i]
+        pre, post = workloads.mixed_geometry_pipelines(im, r)
+        if not srgb:
+            post = None
+        out = torch.full((t.viewport[3], t.viewport[2], 3), float("nan"), device="cuda")
+        geo = render.Geometry("cubic" if t.geometry == 1 else "rotate", t.canvas, t.angle, post)
+        reqs.append((imgs[i], pre, t.viewport, t.mip, t.quality, out, geo))
+        spec = RawSpec(im.width, im.height, render.synthetic_samples(im).cpu().numpy().reshape(-1), im.stride,
+                       im.pattern, *im.phase, im.active, im.black, (im.white,) * 4)
+        ops = [Op(OP_WB, list(r.wb)), Op(OP_EXPOSURE, [r.stops]),
+               Op(OP_CAMERA_TO_WORKING, list(np.asarray(r.camera_to_xyz).reshape(9)) + [0])]
+        ops.append(Op(OP_CUBIC_RESIZE, list(t.canvas)) if t.geometry == 1 else Op(OP_ROTATE, [t.angle]))
+        if srgb:
+            ops += [Op(OP_WORKING_TO_SRGB), Op(OP_TONE, list(r.tone)), Op(OP_SRGB_ENCODE)]
+        wants.append((reference.render_raw(spec, bool(im.demosaic), ops, t.viewport, tile=64, mip=t.mip,
+                                           quality=t.quality), srgb))
+    batch = render.Batch().plan(reqs)
+    batch.launch()
+    batch.status()
+    for k, (req, (want, srgb)) in enumerate(zip(reqs, wants)):
+        got = req[5].cpu().numpy()
+        if srgb:
+            within_tolerance(got, want)
+        else:
+            assert bits_equal(got, want), (k, cases[k])
+    batch.close()

@@ -237,7 +237,9 @@ SCHED_SRC = os.path.join(ROOT, "tests", "cpp", "scheduler_driver.cpp")
 def test_scheduler_mixed_batch_equals_direct_renders(tmp_path):
     """TileScheduler drains a mixed batch (RAWs of several sizes, Bayer
     patterns and phases, bilinear and Menon, mip 0/1/2, tiles 128..1024 with
-    edge remainders) into batched device renders: every host and device tile
+    edge remainders, cubic resizes and rotations between the camera-to-working
+    stage and the rest of the recipe) into batched device renders: every host
+    and device tile
     equals Renderer::render_image of the same request bit for bit, and the
     waves really went through the batch."""
     import json
