@@ -87,6 +87,21 @@ class Image:
         self.handle = handle
         self.metadata = Metadata.from_struct(m)
 
+    @classmethod
+    def ingest(cls, meta: Metadata, samples):
+        """A host plane uploaded while its canonical fingerprint is computed
+        (re_image_create_fingerprinted): returns (image, 32-byte digest)."""
+        m = meta.struct()
+        handle = C.c_void_p()
+        digest = (C.c_uint8 * 32)()
+        arr = np.ascontiguousarray(samples, dtype=np.uint16).reshape(-1)
+        check(lib().re_image_create_fingerprinted(C.byref(m), arr.ctypes.data, arr.size, C.byref(handle), digest))
+        img = cls.__new__(cls)
+        img._keep = None
+        img.handle = handle
+        img.metadata = Metadata.from_struct(m)
+        return img, bytes(digest)
+
     @property
     def active_area(self):
         return self.metadata.active_area

@@ -504,6 +504,9 @@ class Reference:
                                                u32p]
         L.refshim_guided_filter.argtypes = [f32p, u32p, u32p, u32p, C.c_uint32, C.c_double, C.c_int,
                                             f32p]
+        L.refshim_fingerprint_raw.argtypes = [u32p, u16p, u16p, C.c_size_t, C.POINTER(C.c_uint8)]
+        L.refshim_fingerprint_raster.argtypes = [C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t,
+                                                 C.POINTER(C.c_uint8)]
         L.refshim_stencil_raster.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t, f64p, u32p,
                                              C.c_uint32, C.c_uint32, C.c_uint32, f32p]
         L.refshim_histogram_raster.argtypes = [C.c_uint32, C.c_uint32, C.c_int, f32p, C.c_size_t, i32p, C.c_int,
@@ -606,6 +609,22 @@ class Reference:
             _ptr(self._u32(image), C.c_uint32), radius, eps, space, _ptr(out, C.c_float)))
         return out
 
+
+    def fingerprint_raw(self, raw: RawSpec) -> bytes:
+        d = np.zeros(32, np.uint8)
+        s = np.ascontiguousarray(raw.samples, dtype=np.uint16)
+        self._check(self.lib.refshim_fingerprint_raw(_ptr(raw.meta_words(), C.c_uint32),
+                                                     _ptr(raw.level_words(), C.c_uint16), _ptr(s, C.c_uint16),
+                                                     s.size, _ptr(d, C.c_uint8)))
+        return d.tobytes()
+
+    def fingerprint_raster(self, pixels, space=0) -> bytes:
+        pixels = _f32(pixels)
+        h, w = pixels.shape[:2]
+        d = np.zeros(32, np.uint8)
+        self._check(self.lib.refshim_fingerprint_raster(w, h, space, _ptr(pixels, C.c_float), pixels.size,
+                                                        _ptr(d, C.c_uint8)))
+        return d.tobytes()
 
     STENCILS = {"sharpen": 0, "clarity": 1, "texture": 2, "convolution": 3}
 

@@ -348,6 +348,25 @@ int refshim_stencil_raster(int kind, std::uint32_t width, std::uint32_t height, 
     });
 }
 
+// RawImage::fingerprint / RasterImage::fingerprint (SourceFingerprint.cpp:65-101).
+int refshim_fingerprint_raw(const std::uint32_t* meta, const std::uint16_t* levels, const std::uint16_t* samples,
+                            std::size_t count, std::uint8_t* digest) {
+    return guarded([&] {
+        RawImage image(metadata_from(meta, levels), std::vector<std::uint16_t>(samples, samples + count));
+        const auto d = fingerprint_raw_source(image);
+        std::memcpy(digest, d.data(), d.size());
+    });
+}
+int refshim_fingerprint_raster(std::uint32_t width, std::uint32_t height, int space, const float* pixels,
+                               std::size_t count, std::uint8_t* digest) {
+    return guarded([&] {
+        RasterImage image(RasterMetadata{width, height, 0, static_cast<WorkingSpace>(space)},
+                          std::vector<float>(pixels, pixels + count));
+        const auto d = fingerprint_raster_source(image);
+        std::memcpy(digest, d.data(), d.size());
+    });
+}
+
 // input_region_level of the LAST op (or of the RAW source when nops == 0):
 // the reference's halo/support planner (RawEngine.cpp:290-297, SpatialOps.cpp:302-310,
 // GeometryOps.cpp:112-118, 426-430).
