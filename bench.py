@@ -495,7 +495,74 @@ def _config_legs(render, workloads, torch, dev, stream, peak, reps):
                                                                                  kernel="guided filter")
     ms = _per_launch_ms(torch, stream, lambda: render.local_statistics(rgb, 16, stream=stream), reps)
     legs["local_statistics_6000x4000_r16"] = _roofline_leg(ms, px, 36, peak, kernel="local statistics")
+    ms = _per_launch_ms(torch, stream, lambda: render.histogram_rgb(rgb, 256, 0.0, 1.0, 512, stream=stream), reps)
+    legs["histogram_rgb_6000x4000_256_bins"] = _roofline_leg(
+        ms, px, 12, peak, kernel="histogram_kernel",
+        note="includes the counter reset and the read-back of 3x256 counts")
+    image = (0, 0, 6000, 4000)
+    for name, kw in _STENCIL_CASES.items():
+        ms = _per_launch_ms(torch, stream, lambda: render.stencil(name.split("_")[0], rgb, image, image, image,
+                                                                   stream=stream, **kw), reps)
+        legs[f"{name}_6000x4000"] = _roofline_leg(ms, px, 24, peak, kernel=f"{name.split('_')[0]}_kernel",
+                                                   note="synchronous call (status read-back included)")
     return legs
+
+
+# Stencil settings timed on the 6000x4000 raster (radius is the scale for texture).
+_STENCIL_CASES = {"sharpen_r2": dict(amount=1.0, radius=2), "clarity_r8": dict(amount=0.5, radius=8),
+                  "texture_s4": dict(amount=0.5, radius=4),
+                  "convolution_5x5": dict(kernel=np.full((5, 5), 1.0 / 25))}
+
+
+def run_case(args):
+    """One workload's kernel launched --warmup + --steps times with nothing
+    else on the device: the command the ncu summaries in profiles/ name.
+    Cases: menon_24mp_srgb, bilinear_6000x4000, gf_r8, gf_r32, ls_r16,
+    histogram_24mp, sharpen_r2, clarity_r8, texture_s4, convolution_5x5,
+    mixed_batch (the batched persistent render of the mixed workload)."""
+    import torch
+    from librawops_b200 import render, synthetic, workloads
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    name = args.case
+    if name in ("menon_24mp_srgb", "bilinear_6000x4000"):
+        w = workloads.menon_24mp() if name.startswith("menon") else workloads.bilinear_1mp(6000, 4000, seed=5)
+        meta = render.Metadata(w.width, w.height, w.stride, w.pattern, *w.phase, w.active, w.black, (w.white,) * 4)
+        img = render.Image(meta, torch.from_numpy(w.samples().reshape(-1).view(np.int16)).to(dev))
+        pipe = workloads.pipeline_for(w)
+        out = torch.empty((w.active[3], w.active[2], 3), dtype=torch.float32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        fn = lambda: render.render_async(img, pipe, w.active, out, status, stream=stream)
+    elif name == "mixed_batch":
+        images, recipes, tiles = workloads.mixed_batch()
+        imgs = []
+        for im in images:
+            meta = render.Metadata(im.width, im.height, im.stride, im.pattern, im.phase[0], im.phase[1], im.active,
+                                   im.black, (im.white,) * 4)
+            imgs.append(render.Image(meta, render.synthetic_samples(im, device=dev)))
+        outs = [torch.empty((t.viewport[3], t.viewport[2], 3), device=dev) for t in tiles]
+        batch = render.Batch().plan(workloads.mixed_requests(render, imgs, images, recipes, tiles, outs))
+        fn = lambda: batch.launch(stream=stream)
+    else:
+        rgb = torch.from_numpy(synthetic.raster(6000, 4000, seed=3)).to(dev)
+        out = torch.empty_like(rgb)
+        image = (0, 0, 6000, 4000)
+        if name in ("gf_r8", "gf_r32"):
+            fn = lambda: render.guided_filter(rgb, int(name[4:]), 1e-3, out=out, stream=stream)
+        elif name == "ls_r16":
+            fn = lambda: render.local_statistics(rgb, 16, stream=stream)
+        elif name == "histogram_24mp":
+            fn = lambda: render.histogram_rgb(rgb, 256, 0.0, 1.0, 512, stream=stream)
+        elif name in _STENCIL_CASES:
+            fn = lambda: render.stencil(name.split("_")[0], rgb, image, image, image, stream=stream,
+                                        **_STENCIL_CASES[name])
+        else:
+            raise SystemExit(f"unknown case {name}")
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup + args.steps):
+            fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": name, "launches": args.warmup + args.steps}))
 
 
 def _mixed_batch(render, workloads, torch, dev, stream, reps):
@@ -595,7 +662,11 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default=None, help="run one workload's kernel only (profiling captures)")
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
