@@ -519,7 +519,8 @@ def run_case(args):
     else on the device: the command the ncu summaries in profiles/ name.
     Cases: menon_24mp_srgb, bilinear_6000x4000, gf_r8, gf_r32, ls_r16,
     histogram_24mp, sharpen_r2, clarity_r8, texture_s4, convolution_5x5,
-    mixed_batch (the batched persistent render of the mixed workload)."""
+    mixed_batch (the batched persistent render of the mixed workload),
+    differentiable (forward and backward of the 8-frame recipe fit)."""
     import torch
     from librawops_b200 import render, synthetic, workloads
     dev = torch.device("cuda", 0)
@@ -533,6 +534,24 @@ def run_case(args):
         out = torch.empty((w.active[3], w.active[2], 3), dtype=torch.float32, device=dev)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         fn = lambda: render.render_async(img, pipe, w.active, out, status, stream=stream)
+    elif name == "differentiable":
+        from librawops_b200 import diff
+        knots = workloads.tone_knots_16()
+        model = diff.RecipeModel((0, 1, 1, 2), [k[0] for k in knots], [k[1] for k in knots], wb=(2.0, 1.0, 1.6),
+                                 stops=0.2, matrix=workloads.CAMERA_TO_PROPHOTO, strength=0.5, radius=16, eps=1e-3,
+                                 device=dev)
+        planes = []
+        for i in range(8):
+            codes = synthetic.bayer_device(4000, 3000, seed=40 + i, pattern=0, black=(512,) * 4, white=16383,
+                                           device=dev)
+            planes.append(((codes.float() - 512.0) / (16383.0 - 512.0)).contiguous())
+        with torch.no_grad():
+            targets = [model(pl) * 1.01 for pl in planes]
+
+        def fn():
+            model.zero_grad(set_to_none=True)
+            loss = sum(torch.mean((model(pl) - t) ** 2) for pl, t in zip(planes, targets)) / len(planes)
+            loss.backward()
     elif name == "mixed_batch":
         images, recipes, tiles = workloads.mixed_batch()
         imgs = []
