@@ -374,6 +374,16 @@ RE_API re_status re_diff_bilinear_forward(const float* plane, size_t plane_row_s
                                           uint32_t height, uint32_t quad, float* rgb, void* stream);
 RE_API re_status re_diff_bilinear_backward(const float* drgb, uint32_t width, uint32_t height, uint32_t quad,
                                            float* dplane, size_t dplane_row_stride, void* stream);
+/* Menon demosaic (MenonDemosaic.cpp:97-173, mirrored borders, binary64) of
+ * the normalized plane, with the direction of every site written to
+ * `directions` (device, width x height bytes, 1 = horizontal; green sites
+ * 1).  The backward is the transpose of the demosaic with those directions
+ * held fixed (the directions' own derivative is zero almost everywhere). */
+RE_API re_status re_diff_menon_forward(const float* plane, size_t plane_row_stride, uint32_t width, uint32_t height,
+                                       uint32_t quad, float* rgb, uint8_t* directions, void* stream);
+RE_API re_status re_diff_menon_backward(const float* drgb, uint32_t width, uint32_t height, uint32_t quad,
+                                        const uint8_t* directions, float* dplane, size_t dplane_row_stride,
+                                        void* stream);
 
 /* WB gains, exposure multiplier, row-major 3x3, then the master curve: knots
  * kx/ky (n of each), Bezier controls c0/c1 (n-1 of each) and the end slopes

@@ -40,6 +40,7 @@ EXPORTS = [
     "re_histogram_reset", "re_histogram_rgb", "re_histogram_extremum",
     "re_sharpen_window", "re_clarity_window", "re_texture_window", "re_convolution_window",
     "re_fingerprint_raw", "re_fingerprint_raster", "re_image_create_fingerprinted",
+    "re_diff_menon_forward", "re_diff_menon_backward",
 ]
 
 
@@ -185,6 +186,8 @@ def lib() -> C.CDLL:
                                        vp]
         L.re_histogram_extremum.argtypes = [C.c_uint64, C.c_int, C.POINTER(C.c_float)]
         L.re_histogram_extremum.restype = C.c_int
+        L.re_diff_menon_forward.argtypes = [vp, sz, u32, u32, u32, vp, vp, vp]
+        L.re_diff_menon_backward.argtypes = [vp, u32, u32, u32, vp, vp, sz, vp]
         L.re_fingerprint_raw.argtypes = [C.POINTER(RawMetadata), vp, sz, vp]
         L.re_fingerprint_raster.argtypes = [u32, u32, sz, u32, vp, vp]
         L.re_image_create_fingerprinted.argtypes = [C.POINTER(RawMetadata), vp, sz, C.POINTER(vp), vp]

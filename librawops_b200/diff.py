@@ -1,6 +1,6 @@
 """Differentiable render: torch.autograd Functions over the CUDA adjoints.
 
-    plane (h, w)  --BilinearDemosaic-->  camera RGB  --PointStages(wb, stops,
+    plane (h, w)  --BilinearDemosaic or MenonDemosaic-->  camera RGB  --PointStages(wb, stops,
     matrix, curve knots)-->  working RGB  --DetailBoost(strength, eps)-->  out
 
 Each Function's forward and backward are the hand-written kernels of
@@ -58,6 +58,42 @@ class BilinearDemosaic(torch.autograd.Function):
         dplane = torch.empty((h, w), dtype=torch.float32, device=grad.device)
         check(lib().re_diff_bilinear_backward(_ptr(grad), w, h, ctx.quad, _ptr(dplane), w, _stream()))
         return dplane, None
+
+
+class MenonDemosaic(torch.autograd.Function):
+    """Menon demosaic of a normalized sensor plane (MenonDemosaic.cpp:97-173,
+    mirrored borders).  The forward decides the directions; the backward is
+    the transpose with those directions frozen."""
+
+    @staticmethod
+    def forward(ctx, plane, quad: int):
+        plane = plane.contiguous()
+        h, w = plane.shape
+        out = torch.empty((h, w, 3), dtype=torch.float32, device=plane.device)
+        dirs = torch.empty((h, w), dtype=torch.uint8, device=plane.device)
+        check(lib().re_diff_menon_forward(_ptr(plane), w, w, h, quad, _ptr(out), _ptr(dirs), _stream()))
+        ctx.save_for_backward(dirs)
+        ctx.quad = quad
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        (dirs,) = ctx.saved_tensors
+        grad = grad.contiguous()
+        h, w = dirs.shape
+        dplane = torch.empty((h, w), dtype=torch.float32, device=grad.device)
+        check(lib().re_diff_menon_backward(_ptr(grad), w, h, ctx.quad, _ptr(dirs), _ptr(dplane), w, _stream()))
+        return dplane, None
+
+
+def menon_directions(plane, quad: int):
+    """The direction map of MenonDemosaic's forward (1 = horizontal)."""
+    plane = plane.contiguous()
+    h, w = plane.shape
+    out = torch.empty((h, w, 3), dtype=torch.float32, device=plane.device)
+    dirs = torch.empty((h, w), dtype=torch.uint8, device=plane.device)
+    check(lib().re_diff_menon_forward(_ptr(plane), w, w, h, quad, _ptr(out), _ptr(dirs), _stream()))
+    return dirs
 
 
 # --------------------------------------------------------------------- curve
@@ -160,16 +196,20 @@ class DetailBoost(torch.autograd.Function):
 # --------------------------------------------------------------------- model
 
 class RecipeModel(torch.nn.Module):
-    """The differentiable render with learnable recipe parameters: WB gains,
+    """The differentiable render (bilinear, or Menon with directions frozen
+    from the forward) with learnable recipe parameters: WB gains,
     exposure stops, the 3x3 camera->working matrix, the master-curve knot values
     (knot positions fixed), the detail-boost strength and the guided filter's
     epsilon (learned as its natural logarithm, float64, so that it stays
     positive)."""
 
     def __init__(self, quad, kx, ky, wb=(1.0, 1.0, 1.0), stops=0.0, matrix=None, strength=0.0, radius=16,
-                 eps=1e-3, space=PROPHOTO, device="cuda"):
+                 eps=1e-3, space=PROPHOTO, device="cuda", demosaic="bilinear"):
         super().__init__()
         f = dict(dtype=torch.float32, device=device)
+        if demosaic not in ("bilinear", "menon"):
+            raise ValueError("demosaic must be 'bilinear' or 'menon'")
+        self.demosaic = demosaic
         self.quad = quad_code(quad)
         self.radius, self.space = radius, space
         self.register_buffer("kx", torch.tensor(kx, **f))
@@ -186,7 +226,7 @@ class RecipeModel(torch.nn.Module):
         return math.exp(float(self.log_eps.detach()))
 
     def forward(self, plane):
-        x = BilinearDemosaic.apply(plane, self.quad)
+        x = (MenonDemosaic if self.demosaic == "menon" else BilinearDemosaic).apply(plane, self.quad)
         v = point_stages(x, self.wb, self.stops, self.matrix, self.kx, self.ky)
         return DetailBoost.apply(v, self.strength, torch.exp(self.log_eps), self.radius, self.space)
 

@@ -10,6 +10,10 @@ the path:
 * bilinear demosaic of the normalized sensor plane over the active area
   (RawEngine.cpp:299-344): own channel = sample, other channels = mean of the
   same-colour samples in the 3x3 clipped to the active area;
+* or Menon demosaic (MenonDemosaic.cpp:97-173) with mirrored borders: the
+  forward decides the directions, and with those directions held fixed the
+  demosaic is linear in the samples, so its adjoint is that linear map's
+  transpose;
 * white balance x_c * g_c (RawEngine.cpp:417-431), exposure * 2^stops
   (RawEngine.cpp:488-500), a 3x3 matrix (RawEngine.cpp:539-545);
 * the master curve of ExtendedCurvesNode with ShapePreservingCubic
@@ -270,19 +274,150 @@ def detail_backward(p: np.ndarray, dout: np.ndarray, r: int, eps: float, k: floa
     return dp, dk, deps
 
 
+# ------------------------------------------------------------------ Menon
+
+def _mirror(i, n):
+    """MenonDemosaic.cpp:60-66: reflection about the edge samples."""
+    i = np.asarray(i)
+    if n == 1:
+        return np.zeros_like(i)
+    period = 2 * (n - 1)
+    f = np.mod(i, period)
+    return np.where(f < n, f, period - f)
+
+
+def _taps(h, w, dx, dy):
+    """Flat indices of the mirrored samples at offset (dx, dy) of every site."""
+    y = _mirror(np.arange(h) + dy, h)[:, None]
+    x = _mirror(np.arange(w) + dx, w)[None, :]
+    return (y * w + x).reshape(-1)
+
+
+CLASSIFIER = [(0, 2, 1.0), (-2, 2, 1.0), (-1, 1, 1.0), (0, 0, 3.0), (-2, 0, 3.0), (-1, -1, 1.0), (0, -2, 1.0),
+              (-2, -2, 1.0)]
+
+
+def menon_directions(s: np.ndarray, quad) -> np.ndarray:
+    """The horizontal flags of MenonDemosaic.cpp:107-147 (1 at green sites)."""
+    h, w = s.shape
+    c = colour_map(h, w, quad)
+    f = s.reshape(-1)
+    at = lambda dx, dy: f[_taps(h, w, dx, dy)].reshape(h, w)
+    gh = 0.5 * (at(-1, 0) + at(1, 0)) + 0.5 * s - 0.25 * (at(-2, 0) + at(2, 0))
+    gv = 0.5 * (at(0, -1) + at(0, 1)) + 0.5 * s - 0.25 * (at(0, -2) + at(0, 2))
+    ng = c != 1
+    ch = np.where(ng, s - gh, 0.0)
+    cv = np.where(ng, s - gv, 0.0)
+    dh = np.abs(ch - ch.reshape(-1)[_taps(h, w, 2, 0)].reshape(h, w))
+    dv = np.abs(cv - cv.reshape(-1)[_taps(h, w, 0, 2)].reshape(h, w))
+
+    def grad(p, dx, dy):   # zero outside the image, no mirror
+        out = np.zeros_like(p)
+        ys, xs = slice(max(0, -dy), min(h, h - dy)), slice(max(0, -dx), min(w, w - dx))
+        yd, xd = slice(max(0, dy), min(h, h + dy)), slice(max(0, dx), min(w, w + dx))
+        out[ys, xs] = p[yd, xd]
+        return out
+    hh = np.zeros_like(s)
+    vv = np.zeros_like(s)
+    for tx, ty, wt in CLASSIFIER:
+        hh = hh + wt * grad(dh, tx, ty)
+        vv = vv + wt * grad(dv, ty, tx)
+    return np.where(ng, (vv >= hh).astype(np.uint8), 1).astype(np.uint8)
+
+
+def menon_forward(s: np.ndarray, quad, horizontal=None):
+    """MenonDemosaic.cpp:97-173 on a float64 plane with mirrored borders;
+    returns (rgb, horizontal).  With `horizontal` given, those directions are
+    used (the linear map the adjoint transposes)."""
+    h, w = s.shape
+    c = colour_map(h, w, quad)
+    if horizontal is None:
+        horizontal = menon_directions(s, quad)
+    f = s.reshape(-1)
+    at = lambda p, dx, dy: p.reshape(-1)[_taps(h, w, dx, dy)].reshape(h, w)
+    gh = 0.5 * (at(f, -1, 0) + at(f, 1, 0)) + 0.5 * s - 0.25 * (at(f, -2, 0) + at(f, 2, 0))
+    gv = 0.5 * (at(f, 0, -1) + at(f, 0, 1)) + 0.5 * s - 0.25 * (at(f, 0, -2) + at(f, 0, 2))
+    green = np.where(c == 1, s, np.where(horizontal == 1, gh, gv))
+    mean = lambda p, dx, dy: 0.5 * (at(p, -dx, -dy) + at(p, dx, dy))
+    red_h = colour_map(h, w + 1, quad)[:, 1:] == 0          # colour(x + 1, y) == R
+    # (green + mean(raw)) - mean(green), in the reference's order
+    along = lambda p, horiz: np.where(horiz, mean(p, 1, 0), mean(p, 0, 1))
+    red = np.where(c == 0, s, np.where(c == 1, (green + along(f, red_h)) - along(green, red_h), 0.0))
+    blue = np.where(c == 2, s, np.where(c == 1, (green + along(f, ~red_h)) - along(green, ~red_h), 0.0))
+    Hd = horizontal == 1
+    rr = np.where(c == 2, (blue + along(red, Hd)) - along(blue, Hd), red)
+    bb = np.where(c == 0, (red + along(blue, Hd)) - along(red, Hd), blue)
+    return np.stack([rr, green, bb], -1), horizontal
+
+
+def _scatter(h, w, g, dx, dy, weight):
+    """Transpose of p -> weight * p[mirror(offset)]: adds weight * g at the tapped sites."""
+    out = np.zeros(h * w)
+    np.add.at(out, _taps(h, w, dx, dy), (weight * g).reshape(-1))
+    return out.reshape(h, w)
+
+
+def menon_backward(dout: np.ndarray, quad, horizontal) -> np.ndarray:
+    """The transpose of the frozen-direction Menon demosaic: d loss / d s."""
+    h, w = horizontal.shape
+    c = colour_map(h, w, quad)
+    dR, dG, dB = dout[..., 0], dout[..., 1], dout[..., 2]
+    H = horizontal == 1
+    # final step: rr = blue + (mean(red) - mean(blue)) at B sites, bb = red - (...) at R sites
+    dd = np.where(c == 2, dR, 0.0) - np.where(c == 0, dB, 0.0)          # d loss / d dred
+    dred = np.where(c != 2, dR, 0.0) + np.where(c == 0, dB, 0.0)
+    dblue = np.where(c != 0, dB, 0.0) + np.where(c == 2, dR, 0.0)
+    for dx, dy, sel in ((1, 0, H), (0, 1, ~H)):
+        g = np.where(sel, dd, 0.0)
+        for sx, sy in ((-dx, -dy), (dx, dy)):
+            dred += _scatter(h, w, g, sx, sy, 0.5)
+            dblue -= _scatter(h, w, g, sx, sy, 0.5)
+    # red / blue at green sites: green + mean(s) - mean(green); own sites: s
+    ds = np.where(c == 0, dred, 0.0) + np.where(c == 2, dblue, 0.0)
+    dgreen = dG + np.where(c == 1, dred + dblue, 0.0)
+    red_h = colour_map(h, w + 1, quad)[:, 1:] == 0
+    for g, along_x in ((np.where(c == 1, dred, 0.0), red_h), (np.where(c == 1, dblue, 0.0), ~red_h)):
+        for dx, dy, sel in ((1, 0, along_x), (0, 1, ~along_x)):
+            gg = np.where(sel, g, 0.0)
+            for sx, sy in ((-dx, -dy), (dx, dy)):
+                ds += _scatter(h, w, gg, sx, sy, 0.5)
+                dgreen -= _scatter(h, w, gg, sx, sy, 0.5)
+    # green: s at green sites, gh or gv elsewhere
+    ds += np.where(c == 1, dgreen, 0.0)
+    dgh = np.where((c != 1) & H, dgreen, 0.0)
+    dgv = np.where((c != 1) & ~H, dgreen, 0.0)
+    for g, ax in ((dgh, 0), (dgv, 1)):
+        ds += 0.5 * g
+        for k, wt in ((1, 0.5), (2, -0.25)):
+            for sgn in (-1, 1):
+                dx, dy = (sgn * k, 0) if ax == 0 else (0, sgn * k)
+                ds += _scatter(h, w, g, dx, dy, wt)
+    return ds
+
+
 # ----------------------------------------------------------------- full model
 
-def render_forward(s, quad, wb, stops, M, kx, ky, r, eps, k, space=0):
-    x = bilinear_forward(s, quad)
+def _demosaic(s, quad, demosaic, horizontal=None):
+    if demosaic == "menon":
+        return menon_forward(s, quad, horizontal)[0]
+    return bilinear_forward(s, quad)
+
+
+def render_forward(s, quad, wb, stops, M, kx, ky, r, eps, k, space=0, demosaic="bilinear", horizontal=None):
+    x = _demosaic(s, quad, demosaic, horizontal)
     v = point_forward(x, wb, stops, M, kx, ky)
     return detail_forward(v, r, eps, k, space)
 
 
-def render_backward(s, dout, quad, wb, stops, M, kx, ky, r, eps, k, space=0):
-    """Gradients of sum(dout * render) w.r.t. (s, wb, stops, M, ky, k, eps)."""
-    x = bilinear_forward(s, quad)
+def render_backward(s, dout, quad, wb, stops, M, kx, ky, r, eps, k, space=0, demosaic="bilinear", horizontal=None):
+    """Gradients of sum(dout * render) w.r.t. (s, wb, stops, M, ky, k, eps);
+    a Menon demosaic's directions are held at `horizontal` (default: the
+    forward's)."""
+    if demosaic == "menon" and horizontal is None:
+        horizontal = menon_directions(s, quad)
+    x = _demosaic(s, quad, demosaic, horizontal)
     v = point_forward(x, wb, stops, M, kx, ky)
     dv, dk, deps = detail_backward(v, dout, r, eps, k, space)
     dx, dwb, dstops, dM, dky = point_backward(x, dv, wb, stops, M, kx, ky)
-    ds = bilinear_backward(dx, quad)
+    ds = menon_backward(dx, quad, horizontal) if demosaic == "menon" else bilinear_backward(dx, quad)
     return ds, dwb, dstops, dM, dky, dk, deps

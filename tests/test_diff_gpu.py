@@ -156,3 +156,65 @@ def test_fit_recipe_recovers_hidden_parameters_at_radius_16():
     assert abs(float(model.strength.detach()) - 0.6) < 0.02, float(model.strength.detach())
     assert np.max(np.abs(model.ky.detach().cpu().numpy() - np.array(KY))) < 0.01
     assert abs(np.log(model.eps / 1e-3)) < 0.25, model.eps
+
+
+def test_menon_demosaic_forward_and_adjoint_match_oracle():
+    """MenonDemosaic (csrc/diff_menon.cu): the forward equals the float64
+    restatement bit for bit after the float32 cast, directions included; the
+    backward equals the transpose with those directions frozen."""
+    from librawops_b200 import diff
+    rng = np.random.default_rng(12)
+    for h, w in ((40, 52), (3, 7), (65, 33)):
+        plane, _ = _case(max(h, 2), max(w, 2), seed=h)
+        plane = plane[:h, :w].copy()
+        for quad in [(0, 1, 1, 2), (1, 0, 2, 1), (1, 2, 0, 1), (2, 1, 1, 0)]:
+            code = diff.quad_code(quad)
+            p = torch.tensor(plane, device="cuda", requires_grad=True)
+            out = diff.MenonDemosaic.apply(p, code)
+            want, H = D.menon_forward(plane.astype(np.float64), quad)
+            assert np.array_equal(out.detach().cpu().numpy().view(np.uint32),
+                                  want.astype(np.float32).view(np.uint32)), (h, w, quad)
+            assert np.array_equal(diff.menon_directions(p.detach(), code).cpu().numpy(), H), (h, w, quad)
+            u = rng.normal(size=(h, w, 3))
+            (out * torch.tensor(u, dtype=torch.float32, device="cuda")).sum().backward()
+            ref = D.menon_backward(u.astype(np.float32).astype(np.float64), quad, H)
+            assert _rel(p.grad.cpu().numpy(), ref) < 1e-6, (h, w, quad)
+
+
+def test_gradients_with_menon_demosaic():
+    """The full model with a Menon demosaic: every parameter gradient against
+    the float64 adjoint and FP64 central differences, directions frozen at the
+    forward's (their own derivative is zero almost everywhere)."""
+    from librawops_b200 import diff
+    plane, dout = _case(seed=3)
+    m = diff.RecipeModel(QUAD, KX, KY, wb=(1.9, 1.0, 1.5), stops=0.4, matrix=MATRIX, strength=0.5, radius=3,
+                         eps=1e-3, demosaic="menon")
+    p = torch.tensor(plane, device="cuda", requires_grad=True)
+    out = m(p)
+    (out * torch.tensor(dout, dtype=torch.float32, device="cuda")).sum().backward()
+    H = diff.menon_directions(p.detach(), m.quad).cpu().numpy()
+    args = dict(quad=QUAD, wb=m.wb.detach().double().cpu().numpy(), stops=float(m.stops.detach()),
+                M=np.array(MATRIX), kx=np.array(KX), ky=m.ky.detach().double().cpu().numpy(), r=m.radius,
+                eps=m.eps, k=float(m.strength.detach()), demosaic="menon", horizontal=H)
+    assert _rel(out.detach().cpu().numpy(), D.render_forward(plane.astype(np.float64), **args)) < 1e-5
+    ref = D.render_backward(plane.astype(np.float64), dout, **args)
+    got = [p.grad, m.wb.grad, m.stops.grad, m.matrix.grad, m.ky.grad, m.strength.grad, m.log_eps.grad / m.eps]
+    for name, g, r in zip(["plane", "wb", "stops", "matrix", "ky", "strength", "eps"], got, ref):
+        assert _rel(g.detach().cpu().numpy(), r) < 1e-3, name
+
+    def f(**kw):
+        a = dict(args)
+        s = kw.pop("s", plane.astype(np.float64))
+        a.update(kw)
+        return float((D.render_forward(s, **a) * dout).sum())
+
+    step = 1e-3
+    fd_wb = [(f(wb=args["wb"] + step * e) - f(wb=args["wb"] - step * e)) / (2 * step) for e in np.eye(3)]
+    assert _rel(m.wb.grad.cpu().numpy(), fd_wb) < 1e-3
+    for (yy, xx) in [(0, 0), (0, 51), (39, 0), (20, 25), (1, 1), (38, 50)]:
+        sp, sm = plane.astype(np.float64).copy(), plane.astype(np.float64).copy()
+        sp[yy, xx] += step
+        sm[yy, xx] -= step
+        fd = (f(s=sp) - f(s=sm)) / (2 * step)
+        g = float(p.grad[yy, xx])
+        assert abs(g - fd) <= 1e-3 * max(abs(fd), 1e-2 * float(np.abs(ref[0]).max())), (yy, xx, g, fd)
