@@ -21,8 +21,8 @@
 // at 2^31 - 1 (viewports beyond 2^31 pixels break signed-zero ties among the
 // later pixels by position instead).
 //
-// Layout and work split: the image is interleaved float32 RGB rows; each
-// thread takes whole pixels in a grid-stride loop (a warp reads 384
+// Layout and work split: the image is interleaved float32 RGB rows; rows are
+// dealt to CTAs and a row's pixels to its threads (a warp reads 384
 // contiguous bytes), counts into per-CTA shared-memory bins when 3 * bins
 // fit (bins <= 4096), else straight into the global 64-bit counters, and keeps
 // its tallies and extremum keys in registers; each CTA reduces those and
@@ -53,7 +53,7 @@ struct HistParams {
     uint32_t tile;          // traversal tile size (>= max(width, height) for one tile)
     uint64_t first_index;   // traversal index of the region's first pixel
     uint32_t bins;
-    double lower, upper, span;
+    double lower, upper, span, scale;   // scale = bins / span (rounded)
     unsigned long long* counts;    // [3][bins]
     unsigned long long* tallies;   // under[3], over[3], nonfinite[3]
     unsigned long long* extrema;   // min key[3], max key[3]
@@ -69,6 +69,21 @@ __device__ __forceinline__ uint64_t traversal(const HistParams& P, uint32_t x, u
     const uint32_t y0 = y / T * T, x0 = x / T * T;
     const uint32_t th = min(T, P.height - y0), tw = min(T, P.width - x0);
     return P.first_index + (uint64_t)y0 * P.width + (uint64_t)x0 * th + (uint64_t)(y - y0) * tw + (x - x0);
+}
+
+// The reference's bin min(bins - 1, uint32((double(s) - lower) / span * bins)).
+// The quotient-then-product is first approximated by one product with
+// bins / span (both forms are within 4 ulp of the exact value, ~3e-11 for
+// 65536 bins); when that lies more than 2^-30 from an integer both floor to
+// the same bin, otherwise the reference's division is evaluated exactly.
+__device__ __forceinline__ uint32_t bin_of(const HistParams& P, double d) {
+    const double x = __dsub_rn(d, P.lower);
+    const double a = __dmul_rn(x, P.scale);
+    const double f = floor(a);
+    double t = a;
+    // (also taken when bins / span overflowed, so a is infinite or NaN)
+    if (!(a - f >= 0x1p-30 && f + 1.0 - a >= 0x1p-30)) t = __dmul_rn(__ddiv_rn(x, P.span), (double)P.bins);
+    return min(P.bins - 1, __double2uint_rz(t));
 }
 
 __device__ __forceinline__ unsigned long long warp_min(unsigned long long v) {
@@ -96,39 +111,44 @@ __global__ void __launch_bounds__(HIST_THREADS) histogram_kernel(HistParams P) {
     }
     unsigned long long kmin[3] = {~0ull, ~0ull, ~0ull}, kmax[3] = {0ull, 0ull, 0ull};
     uint32_t tally[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const uint64_t pixels = (uint64_t)P.width * P.height;
-    for (uint64_t p = blockIdx.x * (uint64_t)HIST_THREADS + threadIdx.x; p < pixels;
-         p += (uint64_t)gridDim.x * HIST_THREADS) {
-        const uint32_t y = (uint32_t)(p / P.width), x = (uint32_t)(p - (uint64_t)y * P.width);
-        const float* px = P.rgb + (size_t)y * P.stride + (size_t)x * 3;
-        const float v[3] = {__ldcs(px), __ldcs(px + 1), __ldcs(px + 2)};
-        const uint64_t idx = min(traversal(P, x, y), (uint64_t)0x7fffffffu);
+    // rows are dealt to CTAs, a row's pixels to the CTA's threads (coalesced)
+    for (uint32_t y = blockIdx.x; y < P.height; y += gridDim.x) {
+        const float* row = P.rgb + (size_t)y * P.stride;
+        for (uint32_t x = threadIdx.x; x < P.width; x += HIST_THREADS) {
+            const float v[3] = {__ldcs(row + (size_t)x * 3), __ldcs(row + (size_t)x * 3 + 1),
+                                __ldcs(row + (size_t)x * 3 + 2)};
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float s = v[c];
-            if (!isfinite(s)) {
-                ++tally[6 + c];
-                continue;
+            for (int c = 0; c < 3; ++c) {
+                const float s = v[c];
+                if (!isfinite(s)) {
+                    ++tally[6 + c];
+                    continue;
+                }
+                // the traversal index only decides between equal values, so it
+                // is formed only when this sample ties or beats an extremum
+                const uint32_t code = order_code(s);
+                if (code <= (uint32_t)(kmin[c] >> 32) || code >= (uint32_t)(kmax[c] >> 32)) {
+                    const unsigned long long hi = (unsigned long long)code << 32;
+                    const unsigned long long sign = __float_as_uint(s) >> 31;
+                    const uint64_t idx = min(traversal(P, x, y), (uint64_t)0x7fffffffu);
+                    kmin[c] = min(kmin[c], hi | (idx << 1) | sign);
+                    kmax[c] = max(kmax[c], hi | ((0x7fffffffull - idx) << 1) | sign);
+                }
+                const double d = (double)s;
+                if (d < P.lower) {
+                    ++tally[c];
+                    continue;
+                }
+                if (d > P.upper) {
+                    ++tally[3 + c];
+                    continue;
+                }
+                const uint32_t bin = bin_of(P, d);
+                if (SHARED)
+                    atomicAdd(&sbins[c * P.bins + bin], 1u);
+                else
+                    atomicAdd(&P.counts[(size_t)c * P.bins + bin], 1ull);
             }
-            const unsigned long long code = (unsigned long long)order_code(s) << 32;
-            const unsigned long long sign = __float_as_uint(s) >> 31;
-            kmin[c] = min(kmin[c], code | (idx << 1) | sign);
-            kmax[c] = max(kmax[c], code | ((0x7fffffffull - idx) << 1) | sign);
-            const double d = (double)s;
-            if (d < P.lower) {
-                ++tally[c];
-                continue;
-            }
-            if (d > P.upper) {
-                ++tally[3 + c];
-                continue;
-            }
-            const double t = __dmul_rn(__ddiv_rn(__dsub_rn(d, P.lower), P.span), (double)P.bins);
-            const uint32_t bin = min(P.bins - 1, __double2uint_rz(t));
-            if (SHARED)
-                atomicAdd(&sbins[c * P.bins + bin], 1u);
-            else
-                atomicAdd(&P.counts[(size_t)c * P.bins + bin], 1ull);
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -212,15 +232,14 @@ re_status re_histogram_rgb(const float* rgb, size_t row_stride, uint32_t width, 
     P.lower = lower;
     P.upper = upper;
     P.span = span;
+    P.scale = (double)bins / span;
     P.counts = reinterpret_cast<unsigned long long*>(counts);
     P.tallies = reinterpret_cast<unsigned long long*>(tallies);
     P.extrema = reinterpret_cast<unsigned long long*>(extrema);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint64_t pixels = (uint64_t)width * height;
-    const unsigned grid =
-        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((pixels + HIST_THREADS - 1) / HIST_THREADS, (uint64_t)sms * 8));
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(height, (uint64_t)sms * 8));
     cudaStream_t s = (cudaStream_t)stream_;
     if (bins <= HIST_SMEM_BINS) {
         const size_t smem = (size_t)3 * bins * sizeof(uint32_t);

@@ -231,24 +231,58 @@ __global__ void __launch_bounds__(PT_THREADS) point_bwd_kernel(const float* __re
             const float go = dy[i * 3 + r];
             float d = 1.0f;
             if (n) {
+                // this sample's contributions to the curve gradients: key -1
+                // (left extrapolation: ky[0], s_first), -2 (right: ky[n-1],
+                // s_last) or the segment k (ky[k], ky[k+1], c0[k], c1[k])
+                int key;
+                double w0, w1, w2 = 0.0, w3 = 0.0;
                 if (v < C.kx[0]) {
                     d = K.s_first;
-                    atomicAdd(&G.ky[0], (double)go);
-                    atomicAdd(&G.s[0], (double)go * (double)(v - C.kx[0]));
+                    key = -1;
+                    w0 = (double)go;
+                    w1 = (double)go * (double)(v - C.kx[0]);
                 } else if (v > C.kx[n - 1]) {
                     d = K.s_last;
-                    atomicAdd(&G.ky[n - 1], (double)go);
-                    atomicAdd(&G.s[1], (double)go * (double)(v - C.kx[n - 1]));
+                    key = -2;
+                    w0 = (double)go;
+                    w1 = (double)go * (double)(v - C.kx[n - 1]);
                 } else {
                     const int k = segment(C, n, v);
                     const float h = C.kx[k + 1] - C.kx[k];
                     const float t = (v - C.kx[k]) / h, u = 1.0f - t;
                     const float y0 = C.ky[k], a = C.c0[k], b = C.c1[k], y1 = C.ky[k + 1];
                     d = 3.0f * (u * u * (a - y0) + 2.0f * u * t * (b - a) + t * t * (y1 - b)) / h;
-                    atomicAdd(&G.ky[k], (double)(go * u * u * u));
-                    atomicAdd(&G.ky[k + 1], (double)(go * t * t * t));
-                    atomicAdd(&G.c0[k], (double)(go * 3.0f * u * u * t));
-                    atomicAdd(&G.c1[k], (double)(go * 3.0f * u * t * t));
+                    key = k;
+                    w0 = (double)(go * u * u * u);
+                    w1 = (double)(go * t * t * t);
+                    w2 = (double)(go * 3.0f * u * u * t);
+                    w3 = (double)(go * 3.0f * u * t * t);
+                }
+                // Lanes of a warp mostly share a few keys: each group of equal
+                // keys sums its contributions by shuffles and its first lane
+                // adds them to shared memory, instead of one atomic per lane.
+                const unsigned group = __match_any_sync(__activemask(), key);
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                for (unsigned m = group; m; m &= m - 1) {
+                    const int src = __ffs(m) - 1;
+                    s0 += __shfl_sync(group, w0, src);
+                    s1 += __shfl_sync(group, w1, src);
+                    s2 += __shfl_sync(group, w2, src);
+                    s3 += __shfl_sync(group, w3, src);
+                }
+                if ((threadIdx.x & 31) == __ffs(group) - 1) {
+                    if (key == -1) {
+                        atomicAdd(&G.ky[0], s0);
+                        atomicAdd(&G.s[0], s1);
+                    } else if (key == -2) {
+                        atomicAdd(&G.ky[n - 1], s0);
+                        atomicAdd(&G.s[1], s1);
+                    } else {
+                        atomicAdd(&G.ky[key], s0);
+                        atomicAdd(&G.ky[key + 1], s1);
+                        atomicAdd(&G.c0[key], s2);
+                        atomicAdd(&G.c1[key], s3);
+                    }
                 }
             }
             g[r] = go * d;

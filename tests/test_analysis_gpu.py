@@ -74,3 +74,19 @@ def test_histogram_24mp_with_nonfinite_and_signed_zeros(bins):
     img[0, 5000, 1] = 0.0
     for tile in (512, 0):
         _same(_gpu(img, bins, -0.25, 1.25, tile), restated(img, bins, -0.25, 1.25, tile))
+
+
+@pytest.mark.parametrize("bins,lower,upper", [(7, -0.3, 1.1), (1000, 0.0, 1.0), (65536, -2.0, 3.0), (3, 0.1, 0.4)])
+def test_histogram_bin_edges_exact(bins, lower, upper):
+    """Samples on and next to every bin edge (the kernel approximates the
+    bin with one product and falls back to the reference's division near an
+    edge) land where the reference's expression puts them."""
+    span = upper - lower
+    k = np.arange(0, bins + 1, max(1, bins // 500), dtype=np.float64)
+    edges = (lower + k / bins * span).astype(np.float32)
+    near = np.concatenate([edges, np.nextafter(edges, np.float32(np.inf)), np.nextafter(edges, np.float32(-np.inf))])
+    rng = np.random.default_rng(bins)
+    vals = np.concatenate([near, rng.uniform(lower, upper, 20000).astype(np.float32)])
+    n = vals.size - vals.size % 3
+    img = vals[:n].reshape(1, -1, 3)
+    _same(_gpu(img, bins, lower, upper, 0), restated(img, bins, lower, upper, 0))
