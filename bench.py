@@ -301,6 +301,7 @@ def run_ours(args, rank, world, local_rank):
     except Exception as e:   # no host compiler
         scheduler = {"error": str(e)[-300:]}
     differentiable = _differentiable(torch, dev, reps=3)
+    directions = _menon_direction_counts(render, img, w)
 
     # end-to-end through the public API: each step uploads its Bayer frame from
     # pinned host memory, renders it and reads the RGB back into pinned host
@@ -390,6 +391,7 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": "menon_kernel" if tuned["dispatch"] == 3 else "batch_render_kernel",
                      "kernel_ms": round(kernel_ms, 5)},
         "configs": configs,
+        "menon_directions": directions,
         "differentiable": differentiable,
         "cpu_baseline": cpu,
         "e2e": {"value": round(world * pixels / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s",
@@ -635,6 +637,18 @@ def _mixed_batch(render, workloads, torch, dev, stream, reps):
     batch.close()
     del arena
     return result
+
+
+def _menon_direction_counts(render, img, w):
+    """Direction decisions of the frame under both Menon policies: the
+    binary64 policy's exact ties (v == h, decided horizontal as in the
+    reference) and the binary32 policy's decisions inside its proved error
+    band, re-decided in binary64; the two maps are equal."""
+    a, ties = render.menon_directions(img, w.active, render.MENON)
+    b, rechecks = render.menon_directions(img, w.active, render.MENON_FAST)
+    aw, ah = w.active[2], w.active[3]
+    return {"decisions": aw * ah // 2, "binary64_exact_ties": int(ties), "binary32_rechecked_near_ties": int(rechecks),
+            "maps_equal": bool((a == b).all().item())}
 
 
 def _differentiable(torch, dev, reps):
