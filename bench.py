@@ -293,15 +293,6 @@ def run_ours(args, rank, world, local_rank):
     batch.status(stream=stream)
     whole_ms = timed(lambda: render.render_async(img, pipe, w.active, out, status, stream=stream), reps)
     render.status_from_device(int(status.item()))
-    mixed = _mixed_batch(render, workloads, torch, dev, stream, reps=max(3, min(args.steps, 20)))
-    peak, peak_kind = _peaks()
-    configs = _config_legs(render, workloads, torch, dev, stream, peak, reps=max(3, min(args.steps, 10)))
-    try:
-        scheduler = _scheduler_leg(workloads)
-    except Exception as e:   # no host compiler
-        scheduler = {"error": str(e)[-300:]}
-    differentiable = _differentiable(torch, dev, reps=3)
-    directions = _menon_direction_counts(render, img, w)
 
     # end-to-end through the public API: each step uploads its Bayer frame from
     # pinned host memory, renders it and reads the RGB back into pinned host
@@ -353,6 +344,16 @@ def run_ours(args, rank, world, local_rank):
     total_ms, e2e_ms = float(stats[0]), float(stats[1])
     if rank != 0:
         return
+    # the other workloads and legs: rank 0 only, after the last collective
+    mixed = _mixed_batch(render, workloads, torch, dev, stream, reps=max(3, min(args.steps, 20)))
+    peak, peak_kind = _peaks()
+    configs = _config_legs(render, workloads, torch, dev, stream, peak, reps=max(3, min(args.steps, 10)))
+    try:
+        scheduler = _scheduler_leg(workloads)
+    except Exception as e:   # no host compiler
+        scheduler = {"error": str(e)[-300:]}
+    differentiable = _differentiable(torch, dev, reps=3)
+    directions = _menon_direction_counts(render, img, w)
     ms_per_step = total_ms / args.steps
     value = world * pixels / (ms_per_step * 1e-3) / 1e6
     kernel_ms = statistics.mean(launch_ms)
@@ -497,10 +498,20 @@ def _config_legs(render, workloads, torch, dev, stream, peak, reps):
                                                                                  kernel="guided filter")
     ms = _per_launch_ms(torch, stream, lambda: render.local_statistics(rgb, 16, stream=stream), reps)
     legs["local_statistics_6000x4000_r16"] = _roofline_leg(ms, px, 36, peak, kernel="local statistics")
-    ms = _per_launch_ms(torch, stream, lambda: render.histogram_rgb(rgb, 256, 0.0, 1.0, 512, stream=stream), reps)
+    from librawops_b200 import _capi
+    import ctypes
+    L = _capi.lib()
+    counters = torch.empty(3 * 256 + 15, dtype=torch.int64, device=dev)
+    cp = [ctypes.c_void_p(counters.data_ptr() + 8 * o) for o in (0, 3 * 256, 3 * 256 + 9)]
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def hist():
+        _capi.check(L.re_histogram_reset(256, *cp, sp))
+        _capi.check(L.re_histogram_rgb(ctypes.c_void_p(rgb.data_ptr()), rgb.stride(0), 6000, 4000, 512, 0, 256,
+                                       0.0, 1.0, *cp, sp))
+    ms = _per_launch_ms(torch, stream, hist, reps)
     legs["histogram_rgb_6000x4000_256_bins"] = _roofline_leg(
-        ms, px, 12, peak, kernel="histogram_kernel",
-        note="includes the counter reset and the read-back of 3x256 counts")
+        ms, px, 12, peak, kernel="histogram_kernel", note="counter reset (memsets) and the histogram kernel")
     image = (0, 0, 6000, 4000)
     for name, kw in _STENCIL_CASES.items():
         ms = _per_launch_ms(torch, stream, lambda: render.stencil(name.split("_")[0], rgb, image, image, image,

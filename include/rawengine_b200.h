@@ -362,8 +362,9 @@ RE_API re_status re_batch_autotune(re_batch* batch, uint32_t reps, void* stream,
 /* Forward kernels of the render path with the recipe as parameters, and their
  * hand-written adjoints (vector-Jacobian products), for fitting recipes by
  * gradient descent.  No counterpart in the reference, which has no gradients;
- * the forward arithmetic restates RawEngine.cpp:299-344 (bilinear),
- * :417-431/488-500/539-545 (WB, exposure, 3x3), ToneOps.cpp:795-844 (the
+ * the forward arithmetic restates RawEngine.cpp:299-344 (bilinear) or
+ * MenonDemosaic.cpp:97-173 (Menon), RawEngine.cpp:417-431/488-500/539-545
+ * (WB, exposure, 3x3), ToneOps.cpp:795-844 (the
  * master curve, shape-preserving cubic) and SpatialOps.cpp:168-287 (the
  * working-Y guided filter, used as a detail boost v + k (v - GF(v))).  All
  * buffers are DEVICE memory; images are contiguous float32 (h, w, 3); the

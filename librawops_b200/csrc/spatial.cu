@@ -582,9 +582,11 @@ struct GfLaunch {
     void (*kernel)(GfParams);
 };
 
-// MINB CTAs per SM: two for r <= 16, where each CTA's ring of a/b row sums
-// is at most 183 KB; one above, so that the rings of all resident CTAs
-// (up to 400 KB each at r = 32) stay well inside the 126 MB L2.
+// MINB CTAs per SM.  Up to r = 32, two CTAs of 256 columns and 4-row blocks
+// (each CTA's ring of a/b row sums is at most 400 KB, so the resident rings
+// fill most of the 126 MB L2 at r = 32, yet the second CTA per SM still wins:
+// 2.08 ms against 2.88 ms for one CTA of 8-row blocks on 6000x4000); one CTA
+// of 512 columns above.
 template <int NT, int R, int K, int MINB>
 GfLaunch gf_plan(GfParams P, int sms) {
     GfLaunch L;
@@ -605,7 +607,7 @@ GfLaunch gf_plan(GfParams P, int sms) {
 
 GfLaunch gf_choose(const GfParams& P, int sms) {
     if (P.r <= 16) return gf_plan<256, 4, 8, 2>(P, sms);
-    if (P.r <= 32) return gf_plan<256, 8, 16, 1>(P, sms);
+    if (P.r <= 32) return gf_plan<256, 4, 8, 2>(P, sms);
     return gf_plan<512, 4, 16, 1>(P, sms);
 }
 

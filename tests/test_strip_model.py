@@ -13,7 +13,7 @@ from librawops_b200 import synthetic
 
 GF_CASES = [  # width, height, radius, NT, R, K
     (600, 150, 3, 256, 4, 8), (250, 70, 8, 256, 4, 8), (40, 30, 2, 256, 4, 8), (7, 5, 1, 256, 4, 8),
-    (300, 90, 16, 256, 4, 8), (300, 150, 32, 256, 8, 16), (1, 1, 0, 256, 4, 8)]
+    (300, 90, 16, 256, 4, 8), (300, 150, 32, 256, 4, 8), (300, 150, 32, 256, 8, 16), (1, 1, 0, 256, 4, 8)]
 
 
 @pytest.mark.parametrize("w,h,r,nt,rows,k", GF_CASES)
