@@ -272,9 +272,9 @@ re_status build_program(const re_render_desc* d, DevProgram& P) {
             f[0] = h.c[0].identity ? 1.0f : 0.0f;
             f[1] = (float)h.c[0].n;
             f[2] = (float)h.c[0].ncells;
-            f[3] = h.c[0].xf[0];
-            f[4] = h.c[0].x0c;
-            f[5] = h.c[0].inv_dx;
+            f[3] = h.c[0].key_grid ? 1.0f : 0.0f;
+            std::memcpy(&f[4], &h.c[0].grid_p, sizeof(float));
+            std::memcpy(&f[5], &h.c[0].grid_q, sizeof(float));
             for (int c = 0; c < 3; ++c) f[6 + c] = h.c[c + 1].identity ? 1.0f : 0.0f;
         }
     }
@@ -553,10 +553,8 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
             d.xeq[i] = (double)rn == x[i] ? rn : NAN;
             d.y[i] = (float)y[i];
         }
-        double min_h = INFINITY;
         for (uint32_t i = 0; i + 1 < n; ++i) {
             const double h = x[i + 1] - x[i];
-            min_h = std::min(min_h, h);
             const double p0 = y[i] + (h * tangent[i]) / 3, p1 = y[i + 1] - (h * tangent[i + 1]) / 3;
             d.slope[i] = (float)slope[i];
             d.inv_h[i] = (float)(1.0 / h);
@@ -588,40 +586,87 @@ re_status re_curve_set_create(uint32_t interpolation, const uint32_t counts[4], 
         };
         linear_rec(n - 1, n - 1, d.slope[n - 2]);
         linear_rec(n, 0, d.slope[0]);
-        // Uniform cells at most a quarter of the narrowest segment wide: every
-        // cell names the segment one cell to its left and the knot ending it.
-        // A float sample's computed cell is within one of its true cell, so the
-        // samples reaching a cell span at most three cells -- less than any
-        // segment -- and one comparison with that knot finds the sample's
-        // segment; each cell is checked for this below.  Curves needing more
-        // than 4096 cells keep the binary search.
-        const double span = x[n - 1] - x[0];
-        const double cells = std::ceil(span / (0.25 * min_h));
-        d.ncells = 0;
-        if (cells >= 1 && cells <= 4096) {
-            const uint32_t nc = (uint32_t)cells;
-            const double dx = span / nc;
-            // record of a sample at or above the first knot: knots 1..n-1 at or below it
-            auto rec_of = [&](double u) {
-                uint32_t r = 0;
-                while (r + 1 < n && (double)d.xf[r + 1] <= u) ++r;
-                return r;
-            };
+        // Segment lookup grids, in one record format: a cell holds the one knot
+        // its samples can meet (+inf if none) with the records below and at or
+        // above it.  Two grids are tried and the one with fewer cells kept; a
+        // curve that fits neither in 4096 cells keeps the binary search.
+        //  * key grid: cells uniform in curve_key, so they narrow toward zero
+        //    like a tone curve's knots.  The widest cells that put no two knots
+        //    in one cell win; the base is the highest that leaves knot 0 alone
+        //    in cell 0 (lower samples land there too), and the last knot's cell
+        //    is the last (higher samples land there).
+        //  * uniform grid over [x0, x_last], cells a quarter of the narrowest
+        //    segment: a float sample's computed cell is within one of its true
+        //    cell, so the samples reaching cell c lie in cells c-1..c+1, a span
+        //    holding at most one knot (x0 for cell 0, x_last for the last).
+        std::vector<CurveCell> key_cells, uniform_cells;
+        int32_t key_base = 0;
+        uint32_t key_shift = 0;
+        for (int shift = 30; shift >= 0 && key_cells.empty(); --shift) {
+            const int64_t base = (int64_t)curve_key(d.xf[1]) - (int64_t(1) << shift);
+            if (base < INT32_MIN) continue;
+            auto cell_of = [&](uint32_t i) { return ((int64_t)curve_key(d.xf[i]) - base) >> shift; };
             bool ok = true;
+            for (uint32_t i = 1; i < n && ok; ++i)
+                ok = cell_of(i) > (i > 1 ? cell_of(i - 1) : 0) && cell_of(i) < CURVE_CELLS;
+            if (!ok) continue;
+            key_cells.assign((size_t)cell_of(n - 1) + 1, CurveCell{});
+            key_cells[0] = CurveCell{d.xf[0], (uint16_t)n, 0};   // below knot 0: left extrapolation
+            int64_t prev = 0;
+            for (uint32_t i = 1; i < n; ++i) {
+                const int64_t c = cell_of(i);
+                for (int64_t e = prev + 1; e < c; ++e) key_cells[e] = CurveCell{INFINITY, (uint16_t)(i - 1), (uint16_t)(i - 1)};
+                key_cells[c] = CurveCell{d.xf[i], (uint16_t)(i - 1), (uint16_t)i};   // above the last knot: record n-1
+                prev = c;
+            }
+            key_base = (int32_t)base;
+            key_shift = (uint32_t)shift;
+        }
+        const double span = x[n - 1] - x[0];
+        double min_h = INFINITY;
+        for (uint32_t i = 0; i + 1 < n; ++i) min_h = std::min(min_h, x[i + 1] - x[i]);
+        const double cells = std::ceil(span / (0.25 * min_h));
+        double dx = 0.0;
+        if (cells >= 1 && cells <= CURVE_CELLS) {
+            const uint32_t nc = (uint32_t)cells;
+            dx = span / nc;
+            uniform_cells.resize(nc);
             for (uint32_t c = 0; c < nc; ++c) {
-                const double left = x[0] + (double(c) - 1.0) * dx;
-                uint32_t seg = 0;
-                while (seg + 2 < n && (double)d.xf[seg + 1] <= left) ++seg;
-                d.cell[c].seg = seg;
-                d.cell[c].next = d.xf[seg + 1];
-                const uint32_t hi = c + 2 >= nc ? n - 1 : rec_of(x[0] + (double(c) + 2.0) * dx);
-                if (hi > seg + 1) ok = false;
+                const double lo = x[0] + (double(c) - 1.0) * dx, hi = x[0] + (double(c) + 2.0) * dx;
+                int knot = -1, inside = 0;
+                for (uint32_t i = 0; i < n; ++i)
+                    if ((double)d.xf[i] >= lo && (double)d.xf[i] < hi) {
+                        knot = (int)i;
+                        ++inside;
+                    }
+                if (inside > 1) {
+                    uniform_cells.clear();
+                    break;
+                }
+                if (inside) {
+                    uniform_cells[c] = CurveCell{d.xf[knot], (uint16_t)(knot ? knot - 1 : (int)n), (uint16_t)knot};
+                } else {
+                    uint32_t seg = 0;
+                    while (seg + 2 < n && (double)d.xf[seg + 1] <= lo) ++seg;
+                    uniform_cells[c] = CurveCell{INFINITY, (uint16_t)seg, (uint16_t)seg};
+                }
             }
-            if (ok) {
-                d.ncells = nc;
-                d.x0c = d.xn[0];
-                d.inv_dx = (float)(1.0 / dx);
-            }
+        }
+        d.ncells = 0;
+        const bool use_key = !key_cells.empty() && (uniform_cells.empty() || key_cells.size() <= uniform_cells.size());
+        if (use_key) {
+            d.key_grid = 1;
+            d.grid_p = (uint32_t)key_base;
+            d.grid_q = key_shift;
+            d.ncells = (uint32_t)key_cells.size();
+            std::copy(key_cells.begin(), key_cells.end(), d.cell);
+        } else if (!uniform_cells.empty()) {
+            d.key_grid = 0;
+            const float x0c = d.xn[0], inv_dx = (float)(1.0 / dx);
+            std::memcpy(&d.grid_p, &x0c, sizeof x0c);
+            std::memcpy(&d.grid_q, &inv_dx, sizeof inv_dx);
+            d.ncells = (uint32_t)uniform_cells.size();
+            std::copy(uniform_cells.begin(), uniform_cells.end(), d.cell);
         }
     }
     cudaError_t e = cudaMalloc(&cs->dev, sizeof(DevCurveSet));

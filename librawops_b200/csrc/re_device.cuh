@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "rawengine_b200.h"
@@ -179,15 +180,30 @@ __host__ __device__ __forceinline__ int mirror_coord(int v, int origin, int size
 
 // ---------------------------------------------------------------- curves
 
-// A cell of the uniform lookup grid: a segment at or below every sample that
-// falls in the cell, and the RU-rounded knot where that segment ends (a sample
-// at or above it starts one segment later).
+// A cell of the lookup grid: the knot (RU-rounded) that falls in the cell,
+// +inf if none, and the records of the samples below and at or above it.
 constexpr int CURVE_RECS = 288;   // 258 records, padded to whole cache lines
 
 struct __align__(8) CurveCell {
     float next;
-    uint32_t seg;
+    uint16_t below, above;
 };
+constexpr int CURVE_CELLS = 4096;
+
+// Order-preserving integer key of a float: its bit pattern with the magnitude
+// bits of negative values inverted (-0 is folded to +0 first, so the two zeros
+// share a key as they compare equal).  Uniform within each binade, a key step
+// doubles in width from one binade to the next.
+__host__ __device__ inline int32_t curve_key(float v) {
+#ifdef __CUDA_ARCH__
+    const int32_t i = __float_as_int(__fadd_rn(v, 0.0f));
+#else
+    const float z = v + 0.0f;
+    int32_t i;
+    std::memcpy(&i, &z, sizeof i);
+#endif
+    return i < 0 ? i ^ 0x7FFFFFFF : i;
+}
 
 // One ExtendedCurves curve prepared for float32 evaluation (ToneOps.cpp:795-832).
 // Knot x are rounded UP to float so that `v < xf` equals the reference's
@@ -205,16 +221,21 @@ struct DevCurve {
     float slope[256];         // segment slopes (linear segments and extrapolation)
     float4 coef[256];         // power-basis cubic per segment: c0 + t(c1 + t(c2 + t c3))
     float inv_h[256];         // 1 / (x[i+1] - x[i])
-    // O(1) segment lookup: `ncells` uniform cells over [x0, x_last] (0 = none).
+    // O(1) segment lookup (0 cells: none, the binary search over xf).  Key
+    // grid: cell c holds the keys [p + c 2^q, p + (c+1) 2^q) (p, q as int32 and
+    // uint32), lower keys fall in cell 0 and higher ones in the last.  Uniform
+    // grid: a sample's cell is (v - p) * q (p, q the bits of floats) truncated
+    // and clamped.  One comparison with the cell's knot finds the record.
     // Record r (0..n-2 the segments, n-1 the right and n the left linear
     // extrapolation) is p(s) = e0 + s(e1 + s(e2 + s e3)), s = v - anchor[r];
     // each field is its own 128-byte aligned array, so a warp's gather of one
     // field over a short curve touches a single cache line.
     uint32_t ncells;
-    float x0c, inv_dx, pad2;
+    uint32_t key_grid;
+    uint32_t grid_p, grid_q;
     alignas(128) float anchor[CURVE_RECS];
     alignas(128) float e[4][CURVE_RECS];
-    CurveCell cell[4096];
+    CurveCell cell[CURVE_CELLS];
 };
 
 struct DevCurveSet {

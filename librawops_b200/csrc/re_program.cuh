@@ -39,23 +39,30 @@ __device__ __forceinline__ float curve_map(const Curve* __restrict__ c, float v)
     return k.x + t * (k.y + t * (k.z + t * k.w));
 }
 
-// Cell lookup (DevCurve::ncells > 0) of M samples at once: the cell gives a
-// segment at or below the sample and the knot ending it, one comparison with
-// that knot finds the sample's segment (the host sized the cells for it; the
-// RU-rounded knots make the float comparison equal the reference's double
-// one), and one power-basis polynomial evaluates the segment.  Extrapolation
-// and linear curves are records of the same form.  The loads of all M samples
-// are issued before any of them is used.
+// The lookup-grid cell of sample v (DevCurve: key grid or uniform grid).
+__device__ __forceinline__ unsigned curve_cell(float v, unsigned ncells, bool key_grid, uint32_t p, uint32_t q) {
+    if (key_grid) {
+        const int32_t k = curve_key(v);
+        return k < (int32_t)p ? 0u : min(((unsigned)k - p) >> q, ncells - 1u);
+    }
+    const int c = __float2int_rz((v - __uint_as_float(p)) * __uint_as_float(q));
+    return (unsigned)min(max(c, 0), (int)ncells - 1);
+}
+
+// Cell lookup (DevCurve::ncells > 0) of M samples at once: the sample's cell
+// gives the one knot it can meet and the records either side of it, one
+// comparison with that knot (RU-rounded, so the float comparison equals the
+// reference's double one) picks the record, and one power-basis polynomial
+// evaluates it.  Extrapolation and linear curves are records of the same
+// form.  The loads of all M samples are issued before any of them is used.
 template <int M>
-__device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, int n, int ncells, float xf0,
-                                               float x0c, float inv_dx, float* v) {
+__device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, unsigned ncells, bool key_grid,
+                                               uint32_t p, uint32_t q, float* v) {
     int rec[M];
 #pragma unroll
     for (int i = 0; i < M; ++i) {
-        int cell = __float2int_rz((v[i] - x0c) * inv_dx);
-        cell = min(max(cell, 0), ncells - 1);
-        const uint2 e = __ldg(reinterpret_cast<const uint2*>(&c->cell[cell]));
-        rec[i] = v[i] < xf0 ? n : (int)e.y + (v[i] >= __uint_as_float(e.x) ? 1 : 0);
+        const uint2 e = __ldg(reinterpret_cast<const uint2*>(&c->cell[curve_cell(v[i], ncells, key_grid, p, q)]));
+        rec[i] = (int)(v[i] >= __uint_as_float(e.x) ? e.y >> 16 : e.y & 0xFFFFu);
     }
     float s[M], e0[M], e1[M], e2[M], e3[M];
 #pragma unroll
@@ -75,7 +82,7 @@ __device__ __forceinline__ void curve_lookup_n(const DevCurve* __restrict__ c, i
 
 __device__ __forceinline__ float curve_cells(const DevCurve* __restrict__ c, float v) {
     float x[1] = {v};
-    curve_lookup_n<1>(c, (int)c->n, (int)c->ncells, __ldg(&c->xf[0]), c->x0c, c->inv_dx, x);
+    curve_lookup_n<1>(c, c->ncells, c->key_grid != 0, c->grid_p, c->grid_q, x);
     return x[0];
 }
 
@@ -177,21 +184,21 @@ __device__ __forceinline__ void apply_stages(const DevProgram& P, int begin, int
 }
 
 // The master curve with its lookup scalars from the stage's parameters
-// (f[0] identity, f[1] knots, f[2] cells, f[3] first knot, f[4] cell origin,
-// f[5] 1/cell width; build_program fills them).
+// (f[0] identity, f[1] knots, f[2] cells, f[3] key grid, f[4] and f[5] the
+// bits of the grid's p and q; build_program fills them).
 struct MasterCurve {
     const DevCurve* c;
-    int n, ncells;
-    float xf0, x0c, inv_dx;
+    unsigned ncells;
+    bool key_grid;
+    uint32_t p, q;
     bool identity;
     __device__ __forceinline__ void load(const DevCurve* curve, const float* f) {
         c = curve;
         identity = f[0] != 0.0f;
-        n = (int)f[1];
-        ncells = (int)f[2];
-        xf0 = f[3];
-        x0c = f[4];
-        inv_dx = f[5];
+        ncells = (unsigned)f[2];
+        key_grid = f[3] != 0.0f;
+        p = __float_as_uint(f[4]);
+        q = __float_as_uint(f[5]);
     }
     // maps v[0..M) in place
     template <int M>
@@ -202,7 +209,7 @@ struct MasterCurve {
             for (int i = 0; i < M; ++i) v[i] = curve_map(c, v[i]);
             return;
         }
-        curve_lookup_n<M>(c, n, ncells, xf0, x0c, inv_dx, v);
+        curve_lookup_n<M>(c, ncells, key_grid, p, q, v);
     }
 };
 

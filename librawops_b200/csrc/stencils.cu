@@ -5,7 +5,7 @@
 // rectangle grown by the stencil's halo and clipped to the image, the
 // reference's `needed` region) and writes the output rectangle.  A CTA owns a
 // 16 x 16 output tile: it stages the tile plus its halo from the window in
-// shared memory (RGB as float32, or working Y as binary64), flags any
+// shared memory (RGB or working Y, as binary64), flags any
 // non-finite staged sample, and each thread evaluates one output pixel with
 // the reference's binary64 operations in the reference's order:
 //   Sharpen      per channel, the ordered sum over the clipped square of
@@ -62,8 +62,9 @@ __device__ __forceinline__ void flag(uint32_t* status, uint32_t key) { atomicMax
 // Stages this CTA's tile grown by (hx, hy), clipped to the window and to the
 // output grown by the halo (the reference's `needed` region, which a tile
 // reaching past the output's right or bottom edge must not read beyond), as
-// RGB floats at smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c].
-__device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, float* smem, int sx0, int sy0) {
+// RGB values at smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c], widened to
+// binary64 once here (exactly) rather than at every tap that reads them.
+__device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, double* smem, int sx0, int sy0) {
     const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * hx), G.ox + G.ow + hx);
     const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * hy), G.oy + G.oh + hy);
     const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) * 3 : 0;
@@ -72,7 +73,7 @@ __device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, float* s
         const int c = i % 3, p = i / 3, x = x0 + p % w, y = y0 + p / w;
         const float v = G.in[(size_t)(y - G.wy) * G.in_stride + (size_t)(x - G.wx) * 3 + c];
         bad |= !isfinite(v);
-        smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c] = v;
+        smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c] = (double)v;
     }
     if (bad) flag(G.status, KEY_INPUT);
 }
@@ -120,7 +121,7 @@ __device__ __forceinline__ bool my_pixel(const Geo& G, int& x, int& y) {
 
 // SpatialOps.cpp:667-697
 __global__ void __launch_bounds__(ST_TILE* ST_TILE) sharpen_kernel(Geo G, double amount, int radius) {
-    __shared__ float tile[ST_SPAN * ST_SPAN * 3];
+    __shared__ double tile[ST_SPAN * ST_SPAN * 3];
     const int sx0 = G.ox + blockIdx.x * ST_TILE - radius, sy0 = G.oy + blockIdx.y * ST_TILE - radius;
     stage_rgb(G, radius, radius, tile, sx0, sy0);
     __syncthreads();
@@ -131,12 +132,12 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) sharpen_kernel(Geo G, double
     const double count = (double)((right - left + 1) * (bottom - top + 1));
     float* o = G.out + (size_t)(y - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
     for (int c = 0; c < 3; ++c) {
-        const float cf = tile[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c];
-        const double center = cf;
+        const double center = tile[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c];
+        const float cf = (float)center;   // exact: the value came from a float
         double sum = 0.0;
         for (int yy = top; yy <= bottom; ++yy)
             for (int xx = left; xx <= right; ++xx)
-                sum = __dadd_rn(sum, __dsub_rn((double)tile[((yy - sy0) * ST_SPAN + (xx - sx0)) * 3 + c], center));
+                sum = __dadd_rn(sum, __dsub_rn(tile[((yy - sy0) * ST_SPAN + (xx - sx0)) * 3 + c], center));
         const double detail = -__ddiv_rn(sum, count);
         if (detail == 0.0) {
             o[c] = cf;
@@ -254,7 +255,7 @@ struct ConvKernel {
 
 // SpatialOps.cpp:354-383
 __global__ void __launch_bounds__(ST_TILE* ST_TILE) convolution_kernel(Geo G, const __grid_constant__ ConvKernel K) {
-    __shared__ float tile[ST_SPAN * ST_SPAN * 3];
+    __shared__ double tile[ST_SPAN * ST_SPAN * 3];
     __shared__ double coef[CONV_MAX * CONV_MAX];
     const int kw = K.w, kh = K.h, hx = kw / 2, hy = kh / 2;
     for (int i = threadIdx.x; i < kw * kh; i += blockDim.x) coef[i] = K.k[i];
@@ -269,10 +270,10 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) convolution_kernel(Geo G, co
         const int yy = min(max(y + hy - ky, G.iy), bottom);
         for (int kx = 0; kx < kw; ++kx) {
             const int xx = min(max(x + hx - kx, G.ix), right);
-            const float* s = tile + ((yy - sy0) * ST_SPAN + (xx - sx0)) * 3;
+            const double* s = tile + ((yy - sy0) * ST_SPAN + (xx - sx0)) * 3;
             const double wgt = coef[ky * kw + kx];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) sum[c] = __dadd_rn(sum[c], __dmul_rn(wgt, (double)s[c]));
+            for (int c = 0; c < 3; ++c) sum[c] = __dadd_rn(sum[c], __dmul_rn(wgt, s[c]));
         }
     }
     float* o = G.out + (size_t)(y - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
