@@ -19,6 +19,8 @@ namespace re {
 
 constexpr int BL_TW = 64, BL_TH = 16, BL_THREADS = 256;
 constexpr int BL_SW = BL_TW + 2, BL_SH = BL_TH + 2;
+// a batched bilinear tile's curve tables follow its sample tile in shared memory
+constexpr size_t BL_CURVE_OFFSET = (sizeof(float) * BL_SW * BL_SH + 15) / 16 * 16;
 
 // Colour of quad position k = 2*j + i for the four Bayer layouts (RGGB, BGGR, GRBG, GBRG).
 __host__ __device__ constexpr int pat(int l, int k) {
@@ -38,7 +40,7 @@ __host__ __device__ constexpr int pat(int l, int k) {
 template <int L>
 __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0, int y0, int ox, int oy, int ow,
                                               int oh, int stage_end, const DevProgram& P, float* __restrict__ out,
-                                              size_t out_stride, uint32_t& err) {
+                                              size_t out_stride, uint32_t& err, const SmemCurve* sc, int sc_stage) {
     // The tile's row span inside the viewport and 16-byte aligned (the same
     // for the whole block): adjacent lanes pair up per row and the pair's four
     // pixels (48 bytes) leave as three aligned 16-byte stores.
@@ -84,7 +86,7 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
             G[k] = keep[k] ? rgb[1] : 0.0f;
             B[k] = keep[k] ? rgb[2] : 0.0f;
         }
-        apply_stages_n<4, 6>(P, 0, stage_end, R, G, B, err);
+        apply_stages_n<4, 6>(P, 0, stage_end, R, G, B, err, sc, sc_stage);
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int y = y0 + 2 * qy + j;
@@ -123,7 +125,7 @@ __device__ __forceinline__ void bilinear_fast(const float (*tile)[BL_SW], int x0
 __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw& raw, int x0, int y0,
                                              int ox, int oy, int ow, int oh, int layout, int stage_end,
                                              const DevProgram& P, float* __restrict__ out, size_t out_stride,
-                                             uint32_t& err) {
+                                             uint32_t& err, SmemCurve* sc) {
     // interior: the halo's even-aligned quads lie inside the active area
     const bool interior = x0 - 2 >= raw.ax && y0 - 2 >= raw.ay && x0 + BL_TW + 2 <= raw.ax + raw.aw &&
                           y0 + BL_TH + 2 <= raw.ay + raw.ah;
@@ -140,13 +142,14 @@ __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw&
             tile[sy][sx] = v;
         }
     }
+    const int sc_stage = interior ? stage_curve_smem(*sc, P, 0, stage_end) : -1;
     __syncthreads();
     if (interior) {
         switch (layout) {
-        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
-        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err); break;
+        case 0: bilinear_fast<0>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, sc, sc_stage); break;
+        case 1: bilinear_fast<1>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, sc, sc_stage); break;
+        case 2: bilinear_fast<2>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, sc, sc_stage); break;
+        default: bilinear_fast<3>(tile, x0, y0, ox, oy, ow, oh, stage_end, P, out, out_stride, err, sc, sc_stage); break;
         }
         return;
     }
@@ -192,9 +195,10 @@ bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int 
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
     __shared__ __align__(16) float tile[BL_SH][BL_SW];
+    __shared__ SmemCurve curve;
     const int x0 = (ox & ~1) + blockIdx.x * BL_TW, y0 = (oy & ~1) + blockIdx.y * BL_TH;
     uint32_t err = 0;
-    bilinear_cta(tile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err);
+    bilinear_cta(tile, raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P, out, out_stride, err, &curve);
     report(status, err);
 }
 
@@ -546,6 +550,7 @@ struct FastSmemT {
     unsigned smax_bits;          // max |sample| of the footprint (float bits)
     unsigned rechecks;           // entries of `recheck`
     uint16_t recheck[2 * GQN];   // near-tie sites: quad of the r=2 region * 2 + (site B)
+    SmemCurve curve;             // the program's master curve when small (stage_curve_smem)
 };
 using FastSmem = FastSmemT<double>;
 constexpr int FAST_RB_PLANES = 3;   // ng planes holding red and blue at G0, G1 (4 * GQN values)
@@ -669,6 +674,7 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
     // 1. normalized raw (RawEngine.cpp:89-97), r = 6 around the tile, by quad position
     float local_max = 0.0f;
     load_quad_planes<RQW, RQH, MN_THREADS>(S.raw, raw, x0 - 6, y0 - 6, &local_max);
+    const int sc_stage = stage_curve_smem(S.curve, P, 0, stage_end);
     if constexpr (F32) {
         for (int o = 16; o; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
         __syncthreads();   // smax_bits and rechecks are zeroed
@@ -828,7 +834,7 @@ __device__ __forceinline__ void menon_fast(FastSmemT<T>& S, const DevRaw& raw, i
             G[i] = keep[i] ? (float)gg[i] : 0.0f;
             B[i] = keep[i] ? (float)bb[i] : 0.0f;
         }
-        apply_stages_n<2>(P, 0, stage_end, R, G, B, err);
+        apply_stages_n<2>(P, 0, stage_end, R, G, B, err, &S.curve, sc_stage);
         // The tile's row span inside the viewport and 16-byte aligned (the
         // same for every thread of the block): adjacent lanes pair up, and the
         // pair's four pixels (48 bytes) leave as three aligned 16-byte stores --
@@ -1001,7 +1007,7 @@ __device__ __forceinline__ void batch_tile(unsigned char* smem_raw, const BatchP
                   POLICY == 1, nullptr);
     else
         bilinear_cta(reinterpret_cast<float(*)[BL_SW]>(smem_raw), raw, x0, y0, ox, oy, ow, oh, layout, stage_end, P,
-                     out, out_stride, err);
+                     out, out_stride, err, reinterpret_cast<SmemCurve*>(smem_raw + BL_CURVE_OFFSET));
 }
 
 __device__ __forceinline__ void prefetch_unit(BatchUnit* dst, const BatchUnit* src) {
@@ -1067,7 +1073,8 @@ static_assert(BL_THREADS == MN_THREADS, "batched tiles share one block size");
 static_assert(BATCH_MENON_TW == MN_TW && BATCH_MENON_TH == MN_TH && BATCH_BILINEAR_TW == BL_TW &&
                   BATCH_BILINEAR_TH == BL_TH,
               "batch planner tile sizes");
-static_assert(sizeof(MenonShared) >= sizeof(float) * BL_SH * BL_SW, "bilinear tiles fit the batch's shared memory");
+static_assert(sizeof(MenonShared) >= BL_CURVE_OFFSET + sizeof(SmemCurve),
+              "bilinear tiles and their curve tables fit the batch's shared memory");
 
 static_assert(sizeof(BatchParams) <= 32000, "batch launch parameters exceed the 32 KB kernel parameter limit");
 
