@@ -67,13 +67,16 @@ __device__ __forceinline__ void flag(uint32_t* status, uint32_t key) { atomicMax
 __device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, double* smem, int sx0, int sy0) {
     const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * hx), G.ox + G.ow + hx);
     const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * hy), G.oy + G.oh + hy);
-    const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) * 3 : 0;
+    const int n = (x1 - x0) * 3;   // floats of one staged row; a warp copies a row per step
     bool bad = false;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int c = i % 3, p = i / 3, x = x0 + p % w, y = y0 + p / w;
-        const float v = G.in[(size_t)(y - G.wy) * G.in_stride + (size_t)(x - G.wx) * 3 + c];
-        bad |= !isfinite(v);
-        smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c] = (double)v;
+    for (int y = y0 + (int)(threadIdx.x >> 5); n > 0 && y < y1; y += (int)(blockDim.x >> 5)) {
+        const float* src = G.in + (size_t)(y - G.wy) * G.in_stride + (size_t)(x0 - G.wx) * 3;
+        double* dst = smem + ((y - sy0) * ST_SPAN + (x0 - sx0)) * 3;
+        for (int i = (int)(threadIdx.x & 31u); i < n; i += 32) {
+            const float v = src[i];
+            bad |= !isfinite(v);
+            dst[i] = (double)v;
+        }
     }
     if (bad) flag(G.status, KEY_INPUT);
 }
@@ -88,14 +91,16 @@ __device__ __forceinline__ double working_y(float r, float g, float b, double wr
 __device__ __forceinline__ void stage_y(const Geo& G, int h, double wr, double wb, double* plane, int sx0, int sy0) {
     const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * h), G.ox + G.ow + h);
     const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * h), G.oy + G.oh + h);
-    const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) : 0;
+    const int w = x1 - x0;   // at most ST_SPAN: a warp stages a row per step
     bool bad = false;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int x = x0 + i % w, y = y0 + i / w;
-        const float* p = G.in + (size_t)(y - G.wy) * G.in_stride + (size_t)(x - G.wx) * 3;
-        const float r = p[0], g = p[1], b = p[2];
-        bad |= !(isfinite(r) && isfinite(g) && isfinite(b));
-        plane[(y - sy0) * ST_SPAN + (x - sx0)] = working_y(r, g, b, wr, wb);
+    for (int y = y0 + (int)(threadIdx.x >> 5); w > 0 && y < y1; y += (int)(blockDim.x >> 5)) {
+        const float* src = G.in + (size_t)(y - G.wy) * G.in_stride + (size_t)(x0 - G.wx) * 3;
+        double* dst = plane + (y - sy0) * ST_SPAN + (x0 - sx0);
+        for (int i = (int)(threadIdx.x & 31u); i < w; i += 32) {
+            const float r = src[3 * i], g = src[3 * i + 1], b = src[3 * i + 2];
+            bad |= !(isfinite(r) && isfinite(g) && isfinite(b));
+            dst[i] = working_y(r, g, b, wr, wb);
+        }
     }
     if (bad) flag(G.status, KEY_INPUT);
 }
@@ -189,14 +194,17 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) clarity_kernel(Geo G, double
 // ---------------------------------------------------------------- texture
 
 // One axis pass of SpatialOps.cpp:557-587 over the image rectangle
-// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0).
+// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0; at most ST_SPAN
+// columns, so a warp takes one row per step).  The division by the weight is
+// exact scaling for weights 2 and 4 (the correctly rounded product by 1/2 or
+// 1/4 is the correctly rounded quotient); weight 3 divides.
 __device__ __forceinline__ void texture_axis(const Geo& G, const double* src, double* dst, int x0, int x1, int y0,
                                              int y1, bool vertical, int sx0, int sy0) {
-    const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) : 0;
     const int lower = vertical ? G.iy : G.ix, upper = vertical ? G.iy + G.ih : G.ix + G.iw;
     const int step = vertical ? ST_SPAN : 1;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int x = x0 + i % w, y = y0 + i / w;
+    const int x = x0 + (int)(threadIdx.x & 31u);
+    if (x >= x1) return;
+    for (int y = y0 + (int)(threadIdx.x >> 5); y < y1; y += (int)(blockDim.x >> 5)) {
         const int k = (y - sy0) * ST_SPAN + (x - sx0), coord = vertical ? y : x;
         const double center = src[k];
         double sum = 0.0;
@@ -209,7 +217,9 @@ __device__ __forceinline__ void texture_axis(const Geo& G, const double* src, do
             sum = __dadd_rn(sum, __dsub_rn(src[k + step], center));
             ++weight;
         }
-        const double delta = __ddiv_rn(sum, (double)weight);
+        const double delta = weight == 4 ? __dmul_rn(sum, 0.25)
+                             : weight == 2 ? __dmul_rn(sum, 0.5)
+                                           : __ddiv_rn(sum, 3.0);
         dst[k] = delta == 0.0 ? center : __dadd_rn(center, delta);
     }
 }
