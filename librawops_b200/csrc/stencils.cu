@@ -64,14 +64,16 @@ __device__ __forceinline__ void flag(uint32_t* status, uint32_t key) { atomicMax
 // reaching past the output's right or bottom edge must not read beyond), as
 // RGB values at smem[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c], widened to
 // binary64 once here (exactly) rather than at every tap that reads them.
+// TW x TH is the tile, SPAN the staged row pitch in pixels.
+template <int TW = ST_TILE, int TH = ST_TILE, int SPAN = ST_SPAN>
 __device__ __forceinline__ void stage_rgb(const Geo& G, int hx, int hy, double* smem, int sx0, int sy0) {
-    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * hx), G.ox + G.ow + hx);
-    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * hy), G.oy + G.oh + hy);
+    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + TW + 2 * hx), G.ox + G.ow + hx);
+    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + TH + 2 * hy), G.oy + G.oh + hy);
     const int n = (x1 - x0) * 3;   // floats of one staged row; a warp copies a row per step
     bool bad = false;
     for (int y = y0 + (int)(threadIdx.x >> 5); n > 0 && y < y1; y += (int)(blockDim.x >> 5)) {
         const float* src = G.in + (size_t)(y - G.wy) * G.in_stride + (size_t)(x0 - G.wx) * 3;
-        double* dst = smem + ((y - sy0) * ST_SPAN + (x0 - sx0)) * 3;
+        double* dst = smem + ((y - sy0) * SPAN + (x0 - sx0)) * 3;
         for (int i = (int)(threadIdx.x & 31u); i < n; i += 32) {
             const float v = src[i];
             bad |= !isfinite(v);
@@ -87,15 +89,17 @@ __device__ __forceinline__ double working_y(float r, float g, float b, double wr
     return __dadd_rn(__dadd_rn(Gc, __dmul_rn(wr, __dsub_rn(R, Gc))), __dmul_rn(wb, __dsub_rn(B, Gc)));
 }
 
-// Stages working Y (binary64) of the tile grown by h, clipped like stage_rgb.
+// Stages working Y (binary64) of the TILE x TILE tile grown by h, clipped like
+// stage_rgb, at plane[(y - sy0) * SPAN + (x - sx0)].
+template <int TILE = ST_TILE, int SPAN = ST_SPAN>
 __device__ __forceinline__ void stage_y(const Geo& G, int h, double wr, double wb, double* plane, int sx0, int sy0) {
-    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + ST_TILE + 2 * h), G.ox + G.ow + h);
-    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + ST_TILE + 2 * h), G.oy + G.oh + h);
-    const int w = x1 - x0;   // at most ST_SPAN: a warp stages a row per step
+    const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + TILE + 2 * h), G.ox + G.ow + h);
+    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + TILE + 2 * h), G.oy + G.oh + h);
+    const int w = x1 - x0;   // a warp stages a row per step
     bool bad = false;
     for (int y = y0 + (int)(threadIdx.x >> 5); w > 0 && y < y1; y += (int)(blockDim.x >> 5)) {
         const float* src = G.in + (size_t)(y - G.wy) * G.in_stride + (size_t)(x0 - G.wx) * 3;
-        double* dst = plane + (y - sy0) * ST_SPAN + (x0 - sx0);
+        double* dst = plane + (y - sy0) * SPAN + (x0 - sx0);
         for (int i = (int)(threadIdx.x & 31u); i < w; i += 32) {
             const float r = src[3 * i], g = src[3 * i + 1], b = src[3 * i + 2];
             bad |= !(isfinite(r) && isfinite(g) && isfinite(b));
@@ -124,32 +128,84 @@ __device__ __forceinline__ bool my_pixel(const Geo& G, int& x, int& y) {
 
 // ---------------------------------------------------------------- sharpen
 
-// SpatialOps.cpp:667-697
-__global__ void __launch_bounds__(ST_TILE* ST_TILE) sharpen_kernel(Geo G, double amount, int radius) {
-    __shared__ double tile[ST_SPAN * ST_SPAN * 3];
-    const int sx0 = G.ox + blockIdx.x * ST_TILE - radius, sy0 = G.oy + blockIdx.y * ST_TILE - radius;
-    stage_rgb(G, radius, radius, tile, sx0, sy0);
+// Sharpen renders 16 x 64 output tiles: each thread owns four vertically
+// adjacent pixels, so every staged sample it loads serves each of its pixels
+// whose square holds it (radius <= 3: the staged tile is 22 x 70).
+constexpr int SH_MAX_RADIUS = 3, SH_PX = 4, SH_TW = ST_TILE, SH_TH = ST_TILE * SH_PX;
+constexpr int SH_SPAN = SH_TW + 2 * SH_MAX_RADIUS, SH_ROWS = SH_TH + 2 * SH_MAX_RADIUS;
+
+// Sharpen's output for channel value `center` and its window sum
+// (SpatialOps.cpp:688-696).
+__device__ __forceinline__ float sharpen_out(const Geo& G, double center, double sum, double count, double amount) {
+    const float cf = (float)center;   // exact: the value came from a float
+    const double detail = -__ddiv_rn(sum, count);
+    if (detail == 0.0) return cf;
+    const double offset = __dmul_rn(amount, detail);
+    return offset == 0.0 ? cf : to_output(G, __dadd_rn(center, offset));
+}
+
+// SpatialOps.cpp:667-697, radius R.  Each pixel's sum runs over its clipped
+// square in row-major order (rows ascending, then columns), as in the
+// reference.  Where no square of the thread's four pixels is clipped, the
+// thread walks their rows once, holding a row's 2R+1 samples in registers, and
+// adds them to every pixel whose square holds that row (compile-time row and
+// pixel ranges); elsewhere each pixel sums its own clipped square.
+template <int R>
+__global__ void __launch_bounds__(ST_TILE* ST_TILE) sharpen_kernel(Geo G, double amount) {
+    __shared__ double tile[SH_SPAN * SH_ROWS * 3];
+    const int tx0 = G.ox + blockIdx.x * SH_TW, ty0 = G.oy + blockIdx.y * SH_TH;
+    const int sx0 = tx0 - R, sy0 = ty0 - R;
+    stage_rgb<SH_TW, SH_TH, SH_SPAN>(G, R, R, tile, sx0, sy0);
     __syncthreads();
-    int x, y;
-    if (!my_pixel(G, x, y)) return;
-    const int left = max(G.ix, x - radius), top = max(G.iy, y - radius);
-    const int right = min(G.ix + G.iw - 1, x + radius), bottom = min(G.iy + G.ih - 1, y + radius);
-    const double count = (double)((right - left + 1) * (bottom - top + 1));
-    float* o = G.out + (size_t)(y - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
-    for (int c = 0; c < 3; ++c) {
-        const double center = tile[((y - sy0) * ST_SPAN + (x - sx0)) * 3 + c];
-        const float cf = (float)center;   // exact: the value came from a float
-        double sum = 0.0;
-        for (int yy = top; yy <= bottom; ++yy)
-            for (int xx = left; xx <= right; ++xx)
-                sum = __dadd_rn(sum, __dsub_rn(tile[((yy - sy0) * ST_SPAN + (xx - sx0)) * 3 + c], center));
-        const double detail = -__ddiv_rn(sum, count);
-        if (detail == 0.0) {
-            o[c] = cf;
-            continue;
+    const int x = tx0 + (int)(threadIdx.x % ST_TILE);
+    const int y0 = ty0 + SH_PX * (int)(threadIdx.x / ST_TILE);
+    const int rows = min(SH_PX, G.oy + G.oh - y0);   // this thread's pixels y0 .. y0 + rows - 1
+    if (x >= G.ox + G.ow || rows <= 0) return;
+    float* o = G.out + (size_t)(y0 - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
+    const bool whole = rows == SH_PX && x - R >= G.ix && x + R < G.ix + G.iw && y0 - R >= G.iy &&
+                       y0 + SH_PX - 1 + R < G.iy + G.ih;
+    if (whole) {
+        constexpr int K = 2 * R + 1;
+        const double count = (double)(K * K);
+        for (int c = 0; c < 3; ++c) {
+            double center[SH_PX], sum[SH_PX];
+#pragma unroll
+            for (int p = 0; p < SH_PX; ++p) {
+                center[p] = tile[((y0 + p - sy0) * SH_SPAN + (x - sx0)) * 3 + c];
+                sum[p] = 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < SH_PX + 2 * R; ++j) {   // row y0 - R + j
+                const double* row = tile + ((y0 - R + j - sy0) * SH_SPAN + (x - R - sx0)) * 3 + c;
+                double v[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) v[k] = row[3 * k];
+#pragma unroll
+                for (int p = 0; p < SH_PX; ++p) {
+                    if (j < p || j > p + 2 * R) continue;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) sum[p] = __dadd_rn(sum[p], __dsub_rn(v[k], center[p]));
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < SH_PX; ++p)
+                o[(size_t)p * G.out_stride + c] = sharpen_out(G, center[p], sum[p], count, amount);
         }
-        const double offset = __dmul_rn(amount, detail);
-        o[c] = offset == 0.0 ? cf : to_output(G, __dadd_rn(center, offset));
+        return;
+    }
+    const int left = max(G.ix, x - R), right = min(G.ix + G.iw - 1, x + R);
+    for (int p = 0; p < rows; ++p) {
+        const int y = y0 + p;
+        const int top = max(G.iy, y - R), bottom = min(G.iy + G.ih - 1, y + R);
+        const double count = (double)((right - left + 1) * (bottom - top + 1));
+        for (int c = 0; c < 3; ++c) {
+            const double center = tile[((y - sy0) * SH_SPAN + (x - sx0)) * 3 + c];
+            double sum = 0.0;
+            for (int yy = top; yy <= bottom; ++yy)
+                for (int xx = left; xx <= right; ++xx)
+                    sum = __dadd_rn(sum, __dsub_rn(tile[((yy - sy0) * SH_SPAN + (xx - sx0)) * 3 + c], center));
+            o[(size_t)p * G.out_stride + c] = sharpen_out(G, center, sum, count, amount);
+        }
     }
 }
 
@@ -193,51 +249,60 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) clarity_kernel(Geo G, double
 
 // ---------------------------------------------------------------- texture
 
+// Texture renders 32 x 32 output tiles (its halo of 2 * scale, up to 8, costs
+// less against a larger tile); each thread owns four pixels of one column.
+constexpr int TX_TILE = 32, TX_SPAN = TX_TILE + 2 * ST_MAX_HALO;   // 48
+constexpr int TX_THREADS = 256, TX_ROWS = TX_THREADS / 32, TX_PX = TX_TILE / TX_ROWS;
+
 // One axis pass of SpatialOps.cpp:557-587 over the image rectangle
-// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0; at most ST_SPAN
-// columns, so a warp takes one row per step).  The division by the weight is
-// exact scaling for weights 2 and 4 (the correctly rounded product by 1/2 or
-// 1/4 is the correctly rounded quotient); weight 3 divides.
+// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0): a warp takes a
+// row per step.  The division by the weight is exact scaling for weights 2
+// and 4 (the correctly rounded product by 1/2 or 1/4 is the correctly rounded
+// quotient); weight 3 divides.
 __device__ __forceinline__ void texture_axis(const Geo& G, const double* src, double* dst, int x0, int x1, int y0,
                                              int y1, bool vertical, int sx0, int sy0) {
     const int lower = vertical ? G.iy : G.ix, upper = vertical ? G.iy + G.ih : G.ix + G.iw;
-    const int step = vertical ? ST_SPAN : 1;
-    const int x = x0 + (int)(threadIdx.x & 31u);
-    if (x >= x1) return;
-    for (int y = y0 + (int)(threadIdx.x >> 5); y < y1; y += (int)(blockDim.x >> 5)) {
-        const int k = (y - sy0) * ST_SPAN + (x - sx0), coord = vertical ? y : x;
-        const double center = src[k];
-        double sum = 0.0;
-        unsigned weight = 2;
-        if (coord > lower) {
-            sum = __dadd_rn(sum, __dsub_rn(src[k - step], center));
-            ++weight;
+    const int step = vertical ? TX_SPAN : 1;
+    for (int y = y0 + (int)(threadIdx.x >> 5); y < y1; y += TX_ROWS) {
+        for (int x = x0 + (int)(threadIdx.x & 31u); x < x1; x += 32) {
+            const int k = (y - sy0) * TX_SPAN + (x - sx0), coord = vertical ? y : x;
+            const double center = src[k];
+            double sum = 0.0;
+            unsigned weight = 2;
+            if (coord > lower) {
+                sum = __dadd_rn(sum, __dsub_rn(src[k - step], center));
+                ++weight;
+            }
+            if (coord + 1 < upper) {
+                sum = __dadd_rn(sum, __dsub_rn(src[k + step], center));
+                ++weight;
+            }
+            const double delta = weight == 4 ? __dmul_rn(sum, 0.25)
+                                 : weight == 2 ? __dmul_rn(sum, 0.5)
+                                               : __ddiv_rn(sum, 3.0);
+            dst[k] = delta == 0.0 ? center : __dadd_rn(center, delta);
         }
-        if (coord + 1 < upper) {
-            sum = __dadd_rn(sum, __dsub_rn(src[k + step], center));
-            ++weight;
-        }
-        const double delta = weight == 4 ? __dmul_rn(sum, 0.25)
-                             : weight == 2 ? __dmul_rn(sum, 0.5)
-                                           : __ddiv_rn(sum, 3.0);
-        dst[k] = delta == 0.0 ? center : __dadd_rn(center, delta);
     }
 }
 
 // SpatialOps.cpp:536-620
-__global__ void __launch_bounds__(ST_TILE* ST_TILE) texture_kernel(Geo G, double amount, int scale, double wr,
-                                                                   double wb) {
-    __shared__ double plane[ST_SPAN * ST_SPAN], temp[ST_SPAN * ST_SPAN];
+__global__ void __launch_bounds__(TX_THREADS) texture_kernel(Geo G, double amount, int scale, double wr, double wb) {
+    __shared__ double plane[TX_SPAN * TX_SPAN], temp[TX_SPAN * TX_SPAN];
     const int halo = 2 * scale;
-    const int tx0 = G.ox + blockIdx.x * ST_TILE, ty0 = G.oy + blockIdx.y * ST_TILE;
-    const int tx1 = min(G.ox + G.ow, tx0 + ST_TILE), ty1 = min(G.oy + G.oh, ty0 + ST_TILE);
+    const int tx0 = G.ox + blockIdx.x * TX_TILE, ty0 = G.oy + blockIdx.y * TX_TILE;
+    const int tx1 = min(G.ox + G.ow, tx0 + TX_TILE), ty1 = min(G.oy + G.oh, ty0 + TX_TILE);
     const int sx0 = tx0 - halo, sy0 = ty0 - halo;
-    stage_y(G, halo, wr, wb, plane, sx0, sy0);
+    stage_y<TX_TILE, TX_SPAN>(G, halo, wr, wb, plane, sx0, sy0);
     __syncthreads();
-    int x, y;
-    const bool mine = my_pixel(G, x, y);
-    const double center = mine ? plane[(y - sy0) * ST_SPAN + (x - sx0)] : 0.0;
-    double fine = 0.0;
+    // this thread's pixels: column x, rows y0p + TX_ROWS * k
+    const int x = tx0 + (int)(threadIdx.x & 31u), y0p = ty0 + (int)(threadIdx.x >> 5);
+    double center[TX_PX], fine[TX_PX];
+#pragma unroll
+    for (int k = 0; k < TX_PX; ++k) {
+        const int y = y0p + TX_ROWS * k;
+        center[k] = x < tx1 && y < ty1 ? plane[(y - sy0) * TX_SPAN + (x - sx0)] : 0.0;
+        fine[k] = 0.0;
+    }
     for (int pass = 1; pass <= halo; ++pass) {
         const int r = halo - pass;
         // valid = the tile grown by r; the horizontal pass also covers one row above and below
@@ -247,11 +312,21 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) texture_kernel(Geo G, double
         __syncthreads();
         texture_axis(G, temp, plane, vx0, vx1, vy0, vy1, true, sx0, sy0);
         __syncthreads();
-        if (pass == scale && mine) fine = plane[(y - sy0) * ST_SPAN + (x - sx0)];
+        if (pass == scale) {
+#pragma unroll
+            for (int k = 0; k < TX_PX; ++k) {
+                const int y = y0p + TX_ROWS * k;
+                if (x < tx1 && y < ty1) fine[k] = plane[(y - sy0) * TX_SPAN + (x - sx0)];
+            }
+        }
     }
-    if (!mine) return;
-    const double detail = __dsub_rn(fine, plane[(y - sy0) * ST_SPAN + (x - sx0)]);
-    apply_offset(G, x, y, center, detail, amount);
+#pragma unroll
+    for (int k = 0; k < TX_PX; ++k) {
+        const int y = y0p + TX_ROWS * k;
+        if (x >= tx1 || y >= ty1) continue;
+        const double detail = __dsub_rn(fine[k], plane[(y - sy0) * TX_SPAN + (x - sx0)]);
+        apply_offset(G, x, y, center[k], detail, amount);
+    }
 }
 
 // ------------------------------------------------------------ convolution
@@ -423,7 +498,10 @@ re_status re_sharpen_window(const float* in, size_t in_stride, re_rect window, r
     const uint32_t h = amount == 0 ? 0 : radius;
     return run_stencil(kSharpen, in, in_stride, window, image, output, h, h, amount == 0, out, out_stride, stream,
                        [&](const Geo& G, dim3 grid) {
-                           sharpen_kernel<<<grid, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, amount, (int)radius);
+                           const dim3 tiles((G.ow + SH_TW - 1) / SH_TW, (G.oh + SH_TH - 1) / SH_TH);
+                           (void)grid;
+                           auto kernel = radius == 1 ? sharpen_kernel<1> : radius == 2 ? sharpen_kernel<2> : sharpen_kernel<3>;
+                           kernel<<<tiles, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, amount);
                        });
 }
 
@@ -454,8 +532,9 @@ re_status re_texture_window(const float* in, size_t in_stride, re_rect window, r
     const uint32_t h = amount == 0 ? 0 : 2 * scale;
     return run_stencil(kTexture, in, in_stride, window, image, output, h, h, amount == 0, out, out_stride, stream,
                        [&](const Geo& G, dim3 grid) {
-                           texture_kernel<<<grid, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, amount, (int)scale,
-                                                                                             wr, wb);
+                           const dim3 tiles((G.ow + TX_TILE - 1) / TX_TILE, (G.oh + TX_TILE - 1) / TX_TILE);
+                           (void)grid;
+                           texture_kernel<<<tiles, TX_THREADS, 0, (cudaStream_t)stream>>>(G, amount, (int)scale, wr, wb);
                        });
 }
 
