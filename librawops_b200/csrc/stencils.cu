@@ -89,12 +89,12 @@ __device__ __forceinline__ double working_y(float r, float g, float b, double wr
     return __dadd_rn(__dadd_rn(Gc, __dmul_rn(wr, __dsub_rn(R, Gc))), __dmul_rn(wb, __dsub_rn(B, Gc)));
 }
 
-// Stages working Y (binary64) of the TILE x TILE tile grown by h, clipped like
+// Stages working Y (binary64) of the TILE x TH tile grown by h, clipped like
 // stage_rgb, at plane[(y - sy0) * SPAN + (x - sx0)].
-template <int TILE = ST_TILE, int SPAN = ST_SPAN>
+template <int TILE = ST_TILE, int SPAN = ST_SPAN, int TH = TILE>
 __device__ __forceinline__ void stage_y(const Geo& G, int h, double wr, double wb, double* plane, int sx0, int sy0) {
     const int x0 = max(G.wx, sx0), x1 = min(min(G.wx + G.ww, sx0 + TILE + 2 * h), G.ox + G.ow + h);
-    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + TILE + 2 * h), G.oy + G.oh + h);
+    const int y0 = max(G.wy, sy0), y1 = min(min(G.wy + G.wh, sy0 + TH + 2 * h), G.oy + G.oh + h);
     const int w = x1 - x0;   // a warp stages a row per step
     bool bad = false;
     for (int y = y0 + (int)(threadIdx.x >> 5); w > 0 && y < y1; y += (int)(blockDim.x >> 5)) {
@@ -224,27 +224,72 @@ __device__ __forceinline__ void apply_offset(const Geo& G, int x, int y, double 
     for (int c = 0; c < 3; ++c) o[c] = offset == 0.0 ? src[c] : to_output(G, __dadd_rn((double)src[c], offset));
 }
 
-// SpatialOps.cpp:437-495
-__global__ void __launch_bounds__(ST_TILE* ST_TILE) clarity_kernel(Geo G, double amount, int radius, double wr,
-                                                                   double wb) {
-    __shared__ double plane[ST_SPAN * ST_SPAN];
-    const int sx0 = G.ox + blockIdx.x * ST_TILE - radius, sy0 = G.oy + blockIdx.y * ST_TILE - radius;
-    stage_y(G, radius, wr, wb, plane, sx0, sy0);
+// Clarity renders 16 x 64 output tiles like sharpen: four vertically adjacent
+// pixels per thread (radius <= 8: the staged plane is 32 x 80).
+constexpr int CL_MAX_RADIUS = 8, CL_SPAN = ST_TILE + 2 * CL_MAX_RADIUS, CL_ROWS = SH_TH + 2 * CL_MAX_RADIUS;
+
+// SpatialOps.cpp:437-495, radius R.  A pixel with 0 < Y < 1 sums its clipped
+// square of (neighbour - centre) in row-major order.  Where no square of the
+// thread's four pixels is clipped, the thread walks their rows once with a
+// row's 2R+1 values in registers and adds them to every pixel whose square
+// holds the row (each pixel's sum keeps its own row-major order); elsewhere
+// each pixel sums its own clipped square.
+template <int R>
+__global__ void __launch_bounds__(ST_TILE* ST_TILE) clarity_kernel(Geo G, double amount, double wr, double wb) {
+    __shared__ double plane[CL_SPAN * CL_ROWS];
+    const int tx0 = G.ox + blockIdx.x * SH_TW, ty0 = G.oy + blockIdx.y * SH_TH;
+    const int sx0 = tx0 - R, sy0 = ty0 - R;
+    stage_y<SH_TW, CL_SPAN, SH_TH>(G, R, wr, wb, plane, sx0, sy0);
     __syncthreads();
-    int x, y;
-    if (!my_pixel(G, x, y)) return;
-    const double center = plane[(y - sy0) * ST_SPAN + (x - sx0)];
-    double detail = 0.0;
-    if (center > 0.0 && center < 1.0) {
-        const int left = max(G.ix, x - radius), top = max(G.iy, y - radius);
-        const int right = min(G.ix + G.iw - 1, x + radius), bottom = min(G.iy + G.ih - 1, y + radius);
-        double sum = 0.0;
-        for (int yy = top; yy <= bottom; ++yy)
-            for (int xx = left; xx <= right; ++xx)
-                sum = __dadd_rn(sum, __dsub_rn(plane[(yy - sy0) * ST_SPAN + (xx - sx0)], center));
-        detail = -__ddiv_rn(sum, (double)((right - left + 1) * (bottom - top + 1)));
+    const int x = tx0 + (int)(threadIdx.x % ST_TILE);
+    const int y0 = ty0 + SH_PX * (int)(threadIdx.x / ST_TILE);
+    const int rows = min(SH_PX, G.oy + G.oh - y0);
+    if (x >= G.ox + G.ow || rows <= 0) return;
+    double center[SH_PX], detail[SH_PX];
+#pragma unroll
+    for (int p = 0; p < SH_PX; ++p) {
+        center[p] = p < rows ? plane[(y0 + p - sy0) * CL_SPAN + (x - sx0)] : 0.0;
+        detail[p] = 0.0;
     }
-    apply_offset(G, x, y, center, detail, amount);
+    const bool whole = rows == SH_PX && x - R >= G.ix && x + R < G.ix + G.iw && y0 - R >= G.iy &&
+                       y0 + SH_PX - 1 + R < G.iy + G.ih;
+    if (whole) {
+        constexpr int K = 2 * R + 1;
+        double sum[SH_PX];
+#pragma unroll
+        for (int p = 0; p < SH_PX; ++p) sum[p] = 0.0;
+#pragma unroll
+        for (int j = 0; j < SH_PX + 2 * R; ++j) {   // row y0 - R + j
+            const double* row = plane + (y0 - R + j - sy0) * CL_SPAN + (x - R - sx0);
+            double v[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = row[k];
+#pragma unroll
+            for (int p = 0; p < SH_PX; ++p) {
+                if (j < p || j > p + 2 * R) continue;
+#pragma unroll
+                for (int k = 0; k < K; ++k) sum[p] = __dadd_rn(sum[p], __dsub_rn(v[k], center[p]));
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < SH_PX; ++p)
+            if (center[p] > 0.0 && center[p] < 1.0) detail[p] = -__ddiv_rn(sum[p], (double)(K * K));
+    } else {
+        const int left = max(G.ix, x - R), right = min(G.ix + G.iw - 1, x + R);
+        for (int p = 0; p < rows; ++p) {
+            if (!(center[p] > 0.0 && center[p] < 1.0)) continue;
+            const int y = y0 + p;
+            const int top = max(G.iy, y - R), bottom = min(G.iy + G.ih - 1, y + R);
+            double sum = 0.0;
+            for (int yy = top; yy <= bottom; ++yy)
+                for (int xx = left; xx <= right; ++xx)
+                    sum = __dadd_rn(sum, __dsub_rn(plane[(yy - sy0) * CL_SPAN + (xx - sx0)], center[p]));
+            detail[p] = -__ddiv_rn(sum, (double)((right - left + 1) * (bottom - top + 1)));
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < SH_PX; ++p)
+        if (p < rows) apply_offset(G, x, y0 + p, center[p], detail[p], amount);
 }
 
 // ---------------------------------------------------------------- texture
@@ -363,6 +408,80 @@ __global__ void __launch_bounds__(ST_TILE* ST_TILE) convolution_kernel(Geo G, co
     }
     float* o = G.out + (size_t)(y - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
     for (int c = 0; c < 3; ++c) o[c] = to_output(G, sum[c]);
+}
+
+// SpatialOps.cpp:354-383 for a square KS x KS kernel (3 or 5), on 16 x 64
+// output tiles with four vertically adjacent pixels per thread.  Pixel p's
+// sum runs over kernel rows ky ascending (image rows descending) and columns
+// kx ascending, as in the reference.  Where no tap of the thread's pixels is
+// clamped, the thread walks the image rows once from the bottom, holding a
+// row's KS samples in registers, and adds w * x to every pixel whose kernel
+// reaches that row (the coefficients are compile-time kernel-parameter
+// operands); elsewhere each pixel runs the clamped loop.
+template <int KS>
+__global__ void __launch_bounds__(ST_TILE* ST_TILE) convolution_square_kernel(Geo G,
+                                                                              const __grid_constant__ ConvKernel K) {
+    constexpr int H = KS / 2;
+    static_assert(H <= SH_MAX_RADIUS, "the staged tile holds a halo of at most 3");
+    __shared__ double tile[SH_SPAN * SH_ROWS * 3];
+    const int tx0 = G.ox + blockIdx.x * SH_TW, ty0 = G.oy + blockIdx.y * SH_TH;
+    const int sx0 = tx0 - H, sy0 = ty0 - H;
+    stage_rgb<SH_TW, SH_TH, SH_SPAN>(G, H, H, tile, sx0, sy0);
+    __syncthreads();
+    const int x = tx0 + (int)(threadIdx.x % ST_TILE);
+    const int y0 = ty0 + SH_PX * (int)(threadIdx.x / ST_TILE);
+    const int rows = min(SH_PX, G.oy + G.oh - y0);
+    if (x >= G.ox + G.ow || rows <= 0) return;
+    float* o = G.out + (size_t)(y0 - G.oy) * G.out_stride + (size_t)(x - G.ox) * 3;
+    const int right = G.ix + G.iw - 1, bottom = G.iy + G.ih - 1;
+    const bool whole = rows == SH_PX && x - H >= G.ix && x + H <= right && y0 - H >= G.iy &&
+                       y0 + SH_PX - 1 + H <= bottom;
+    if (whole) {
+        double sum[SH_PX][3];
+#pragma unroll
+        for (int p = 0; p < SH_PX; ++p) sum[p][0] = sum[p][1] = sum[p][2] = 0.0;
+#pragma unroll
+        for (int j = 0; j < SH_PX + 2 * H; ++j) {   // image row y0 + SH_PX - 1 + H - j
+            const double* row = tile + ((y0 + SH_PX - 1 + H - j - sy0) * SH_SPAN + (x + H - sx0)) * 3;
+            double v[KS][3];
+#pragma unroll
+            for (int kx = 0; kx < KS; ++kx)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) v[kx][c] = row[c - 3 * kx];   // column x + H - kx
+#pragma unroll
+            for (int p = 0; p < SH_PX; ++p) {
+                const int ky = j + p - (SH_PX - 1);
+                if (ky < 0 || ky >= KS) continue;
+#pragma unroll
+                for (int kx = 0; kx < KS; ++kx) {
+                    const double wgt = K.k[ky * KS + kx];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) sum[p][c] = __dadd_rn(sum[p][c], __dmul_rn(wgt, v[kx][c]));
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < SH_PX; ++p)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[(size_t)p * G.out_stride + c] = to_output(G, sum[p][c]);
+        return;
+    }
+    for (int p = 0; p < rows; ++p) {
+        const int y = y0 + p;
+        double sum[3] = {0.0, 0.0, 0.0};
+        for (int ky = 0; ky < KS; ++ky) {
+            const int yy = min(max(y + H - ky, G.iy), bottom);
+            for (int kx = 0; kx < KS; ++kx) {
+                const int xx = min(max(x + H - kx, G.ix), right);
+                const double* t = tile + ((yy - sy0) * SH_SPAN + (xx - sx0)) * 3;
+                const double wgt = K.k[ky * KS + kx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sum[c] = __dadd_rn(sum[c], __dmul_rn(wgt, t[c]));
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[(size_t)p * G.out_stride + c] = to_output(G, sum[c]);
+    }
 }
 
 // Input check and copy of the output rectangle (zero amount, identity kernel).
@@ -516,8 +635,12 @@ re_status re_clarity_window(const float* in, size_t in_stride, re_rect window, r
     const uint32_t h = amount == 0 ? 0 : radius;
     return run_stencil(kClarity, in, in_stride, window, image, output, h, h, amount == 0, out, out_stride, stream,
                        [&](const Geo& G, dim3 grid) {
-                           clarity_kernel<<<grid, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, amount, (int)radius,
-                                                                                             wr, wb);
+                           const dim3 tiles((G.ow + SH_TW - 1) / SH_TW, (G.oh + SH_TH - 1) / SH_TH);
+                           (void)grid;
+                           void (*const kernels[])(Geo, double, double, double) = {
+                               clarity_kernel<1>, clarity_kernel<2>, clarity_kernel<3>, clarity_kernel<4>,
+                               clarity_kernel<5>, clarity_kernel<6>, clarity_kernel<7>, clarity_kernel<8>};
+                           kernels[radius - 1]<<<tiles, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, amount, wr, wb);
                        });
 }
 
@@ -558,7 +681,13 @@ re_status re_convolution_window(const float* in, size_t in_stride, re_rect windo
     return run_stencil(kConvolution, in, in_stride, window, image, output, identity ? 0 : kernel_width / 2,
                        identity ? 0 : kernel_height / 2, identity, out, out_stride, stream,
                        [&](const Geo& G, dim3 grid) {
-                           convolution_kernel<<<grid, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, K);
+                           const dim3 tiles((G.ow + SH_TW - 1) / SH_TW, (G.oh + SH_TH - 1) / SH_TH);
+                           if (K.w == K.h && K.w == 3)
+                               convolution_square_kernel<3><<<tiles, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, K);
+                           else if (K.w == K.h && K.w == 5)
+                               convolution_square_kernel<5><<<tiles, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, K);
+                           else
+                               convolution_kernel<<<grid, ST_TILE * ST_TILE, 0, (cudaStream_t)stream>>>(G, K);
                        });
 }
 

@@ -30,6 +30,9 @@ CASES = [
     ("convolution", dict(kernel=RNG.normal(size=(5, 7)) / 8)),
     ("convolution", dict(kernel=RNG.normal(size=(17, 17)) / 40)),
     ("convolution", dict(kernel=np.pad([[1.0]], 1))),
+    ("sharpen", dict(amount=1.3, radius=2)),
+    ("clarity", dict(amount=0.8, radius=5)),
+    ("convolution", dict(kernel=RNG.normal(size=(5, 5)) / 5)),
 ]
 
 
@@ -123,3 +126,22 @@ def test_stencil_results_beyond_float32(reference):
             render.stencil(kind, torch.from_numpy(img).cuda(), (0, 0, 9, 9), (0, 0, 9, 9), (0, 0, 9, 9), **p)
         assert got.value.kind == want.value.kind == "invalid_argument"
         assert str(got.value) == str(want.value), (str(got.value), str(want.value))
+
+
+@pytest.mark.parametrize("kind,params", [("sharpen", dict(amount=1.0, radius=2)), ("clarity", dict(amount=0.7, radius=8)),
+                                         ("texture", dict(amount=0.9, radius=4)),
+                                         ("convolution", dict(kernel=np.random.default_rng(9).normal(size=(5, 5)) / 5))])
+def test_stencil_600x400_against_reference(reference, kind, params):
+    """A frame large enough that most threads of the register-blocked tiles
+    (16 x 64 for sharpen, clarity and square convolutions, 32 x 32 for
+    texture) take the unclipped path, and partial tiles sit on both edges."""
+    from librawops_b200 import render
+    rng = np.random.default_rng(21)
+    h, w = 400, 600
+    y, x = np.mgrid[0:h, 0:w]
+    img = np.stack([0.5 + 0.4 * np.sin(x / 17.0), 0.5 + 0.4 * np.cos(y / 11.0), 0.3 + 0.2 * np.sin((x + y) / 7.0)], -1)
+    img = (img + 0.05 * rng.normal(size=img.shape)).astype(np.float32)
+    vp = (5, 3, w - 11, h - 7)
+    want = reference.stencil(kind, img, vp, **params)
+    got = render.stencil(kind, torch.from_numpy(img).cuda(), (0, 0, w, h), (0, 0, w, h), vp, **params)
+    assert bits_equal(got.cpu().numpy(), want)
