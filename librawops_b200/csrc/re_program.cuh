@@ -417,25 +417,22 @@ __device__ __forceinline__ bool try_chain(Chain<KINDS...>, const DevProgram& P, 
 
 // The stage program over N pixels held by one thread: the stage loop is
 // outside, so each stage's constants are read once and its arithmetic runs
-// over N independent pixels.  Common chains run as straight-line code, which
-// the compiler schedules across stages: the reference renderer's usual node
-// orders (white balance, exposure, camera matrix, curves or tone curve,
-// output matrix, sRGB encode) and their prefixes up to the mip anchor.  Any
-// other program goes through the per-stage dispatch.  Either way each pixel
-// sees apply_stages' operations.
+// over N independent pixels.  Two chains of the reference renderer's usual
+// node order run as straight-line code, which the compiler schedules across
+// stages: white balance, camera matrix, curves, output matrix, sRGB encode
+// (a finished sRGB render), and white balance, camera matrix (scene-linear
+// output).  Any other program goes through the per-stage dispatch (each more
+// specialised chain multiplies the code of every render kernel).  Either way
+// each pixel sees apply_stages' operations.
 // sc / sc_stage: the master curve of stage sc_stage staged in shared memory
 // by stage_curve_smem (nullptr / -1: none).
 template <int N, int CHUNK = 3>
 __device__ __forceinline__ void apply_stages_n(const DevProgram& P, int begin, int end, float (&r)[N],
                                                float (&g)[N], float (&b)[N], uint32_t& err,
                                                const SmemCurve* sc = nullptr, int sc_stage = -1) {
-    constexpr int G = RE_STAGE_GAIN3, X = RE_STAGE_SCALE, M = RE_STAGE_MATRIX, T = RE_STAGE_TONE,
-                  C = RE_STAGE_CURVES, S = RE_STAGE_SRGB;
+    constexpr int G = RE_STAGE_GAIN3, M = RE_STAGE_MATRIX, C = RE_STAGE_CURVES, S = RE_STAGE_SRGB;
     if (try_chain<N, CHUNK>(Chain<G, M, C, M, S>{}, P, begin, end, r, g, b, err, sc, sc_stage) ||
-        try_chain<N, CHUNK>(Chain<G, M>{}, P, begin, end, r, g, b, err, sc, sc_stage) ||
-        try_chain<N, CHUNK>(Chain<G, X, M>{}, P, begin, end, r, g, b, err, sc, sc_stage) ||
-        try_chain<N, CHUNK>(Chain<G, X, M, M, T, S>{}, P, begin, end, r, g, b, err, sc, sc_stage) ||
-        try_chain<N, CHUNK>(Chain<G, M, X, C, M, S>{}, P, begin, end, r, g, b, err, sc, sc_stage))
+        try_chain<N, CHUNK>(Chain<G, M>{}, P, begin, end, r, g, b, err, sc, sc_stage))
         return;
     for (int s = begin; s < end; ++s) {
         switch (P.st[s].kind) {
