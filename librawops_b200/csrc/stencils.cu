@@ -300,16 +300,25 @@ constexpr int TX_TILE = 32, TX_SPAN = TX_TILE + 2 * ST_MAX_HALO;   // 48
 constexpr int TX_THREADS = 256, TX_ROWS = TX_THREADS / 32, TX_PX = TX_TILE / TX_ROWS;
 
 // One axis pass of SpatialOps.cpp:557-587 over the image rectangle
-// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0): a warp takes a
-// row per step.  The division by the weight is exact scaling for weights 2
+// [x0, x1) x [y0, y1) (smem coordinates relative to sx0, sy0), its cells dealt
+// to the threads in row-major order.  The division by the weight is exact
+// scaling for weights 2
 // and 4 (the correctly rounded product by 1/2 or 1/4 is the correctly rounded
 // quotient); weight 3 divides.
 __device__ __forceinline__ void texture_axis(const Geo& G, const double* src, double* dst, int x0, int x1, int y0,
                                              int y1, bool vertical, int sx0, int sy0) {
     const int lower = vertical ? G.iy : G.ix, upper = vertical ? G.iy + G.ih : G.ix + G.iw;
     const int step = vertical ? TX_SPAN : 1;
-    for (int y = y0 + (int)(threadIdx.x >> 5); y < y1; y += TX_ROWS) {
-        for (int x = x0 + (int)(threadIdx.x & 31u); x < x1; x += 32) {
+    const int w = x1 - x0, n = w > 0 && y1 > y0 ? w * (y1 - y0) : 0;
+    // element i of the rectangle is row i / w, found as the truncated product
+    // (i + 1/2) * (1 / w): exact here, since the product's fractional part
+    // stays at least 1/(2w) >= 1/96 away from an integer while its rounding
+    // error is below n * 2^-23 < 1/3000
+    const float inv_w = 1.0f / (float)max(w, 1);
+    for (int i = (int)threadIdx.x; i < n; i += TX_THREADS) {
+        {
+            const int r = __float2int_rz(((float)i + 0.5f) * inv_w);
+            const int y = y0 + r, x = x0 + (i - r * w);
             const int k = (y - sy0) * TX_SPAN + (x - sx0), coord = vertical ? y : x;
             const double center = src[k];
             double sum = 0.0;
