@@ -109,7 +109,21 @@ __global__ void __launch_bounds__(HIST_THREADS) histogram_kernel(HistParams P) {
         for (uint32_t i = threadIdx.x; i < 3 * P.bins; i += HIST_THREADS) sbins[i] = 0;
         __syncthreads();
     }
-    unsigned long long kmin[3] = {~0ull, ~0ull, ~0ull}, kmax[3] = {0ull, 0ull, 0ull};
+    // Each thread's extrema as (order code, position, sign); the 64-bit keys
+    // (order code, traversal index, sign) are formed only where two samples
+    // share a code and at the end, so the common path carries no index
+    // arithmetic (a divergent branch costs the whole warp).  Sentinels: no
+    // finite sample has order code 0xffffffff or 0.
+    uint32_t mn_code[3] = {~0u, ~0u, ~0u}, mx_code[3] = {0u, 0u, 0u};
+    uint32_t mn_x[3], mn_y[3], mn_s[3], mx_x[3], mx_y[3], mx_s[3];
+    auto min_key = [&](uint32_t code, uint32_t x, uint32_t y, uint32_t sign) {
+        const uint64_t idx = min(traversal(P, x, y), (uint64_t)0x7fffffffu);
+        return ((unsigned long long)code << 32) | (idx << 1) | sign;
+    };
+    auto max_key = [&](uint32_t code, uint32_t x, uint32_t y, uint32_t sign) {
+        const uint64_t idx = min(traversal(P, x, y), (uint64_t)0x7fffffffu);
+        return ((unsigned long long)code << 32) | ((0x7fffffffull - idx) << 1) | sign;
+    };
     uint32_t tally[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     // rows are dealt to CTAs, a row's pixels to the CTA's threads (coalesced)
     for (uint32_t y = blockIdx.x; y < P.height; y += gridDim.x) {
@@ -124,15 +138,22 @@ __global__ void __launch_bounds__(HIST_THREADS) histogram_kernel(HistParams P) {
                     ++tally[6 + c];
                     continue;
                 }
-                // the traversal index only decides between equal values, so it
-                // is formed only when this sample ties or beats an extremum
+                // the traversal index only decides between equal codes
                 const uint32_t code = order_code(s);
-                if (code <= (uint32_t)(kmin[c] >> 32) || code >= (uint32_t)(kmax[c] >> 32)) {
-                    const unsigned long long hi = (unsigned long long)code << 32;
-                    const unsigned long long sign = __float_as_uint(s) >> 31;
-                    const uint64_t idx = min(traversal(P, x, y), (uint64_t)0x7fffffffu);
-                    kmin[c] = min(kmin[c], hi | (idx << 1) | sign);
-                    kmax[c] = max(kmax[c], hi | ((0x7fffffffull - idx) << 1) | sign);
+                const uint32_t sign = __float_as_uint(s) >> 31;
+                if (code < mn_code[c] ||
+                    (code == mn_code[c] && min_key(code, x, y, sign) < min_key(code, mn_x[c], mn_y[c], mn_s[c]))) {
+                    mn_code[c] = code;
+                    mn_x[c] = x;
+                    mn_y[c] = y;
+                    mn_s[c] = sign;
+                }
+                if (code > mx_code[c] ||
+                    (code == mx_code[c] && max_key(code, x, y, sign) > max_key(code, mx_x[c], mx_y[c], mx_s[c]))) {
+                    mx_code[c] = code;
+                    mx_x[c] = x;
+                    mx_y[c] = y;
+                    mx_s[c] = sign;
                 }
                 const double d = (double)s;
                 if (d < P.lower) {
@@ -150,6 +171,12 @@ __global__ void __launch_bounds__(HIST_THREADS) histogram_kernel(HistParams P) {
                     atomicAdd(&P.counts[(size_t)c * P.bins + bin], 1ull);
             }
         }
+    }
+    unsigned long long kmin[3], kmax[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        kmin[c] = mn_code[c] == ~0u ? ~0ull : min_key(mn_code[c], mn_x[c], mn_y[c], mn_s[c]);
+        kmax[c] = mx_code[c] == 0u ? 0ull : max_key(mx_code[c], mx_x[c], mx_y[c], mx_s[c]);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
