@@ -190,7 +190,9 @@ __device__ __forceinline__ void bilinear_cta(float (*tile)[BL_SW], const DevRaw&
     }
 }
 
-__global__ void __launch_bounds__(BL_THREADS, 4)
+// Six CTAs per SM (40 registers, no spills): the tile's load, barrier and
+// stores overlap across more CTAs than at four (24 MP demosaic 0.146 -> 0.116 ms).
+__global__ void __launch_bounds__(BL_THREADS, 6)
 bilinear_kernel(const __grid_constant__ DevRaw raw, int ox, int oy, int ow, int oh, int layout, int stage_end,
                 const __grid_constant__ DevProgram P, float* __restrict__ out,
                 size_t out_stride, uint32_t* status) {
